@@ -1,0 +1,359 @@
+"""Benchmark of the multi-sphere T-matrix GMRES solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload medium|small]
+
+One step = one complete solve (GMRES to the workload's tolerance) of the seeded synthetic
+scene.  The default workload is the 2000-sphere lognormal cluster (40 um cube, per-sphere
+Wiscombe truncation, GMRES(50) to 1e-8, FP64, one x-polarised plane wave along +z).  With N > 1
+(torchrun, one process per GPU) every rank solves its own replica: the path has no exchange
+step, so there is no collective on the data path ("scaling": "weak").
+
+Printed JSON line (rank 0):
+  value      solves/s of the whole job with the scene resident in HBM (device-timed, max over
+             ranks), e2e the same through the public API with host buffers (scene upload,
+             solve, solution download inside the timed region);
+  roofline   the operator kernel k_direct (>95% of the solve): achieved FP64 FLOP/s from the
+             algorithmic flop count per launch and its CUDA-event time, against the FP64
+             cuBLAS DGEMM rate measured in the same run;
+  cpu_baseline  the FP64 oracle (restated reference algorithm, exact Xu translation
+             coefficients recomputed for every pair as the reference does) timed on this
+             host's cores on a bounded random sample of sphere pairs, extrapolated to solves/s.
+--impl reference prints the same line for that CPU implementation alone.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLFMM-GMRES solves/s, p50/p99 latency at 1e-6 rel err vs plain FP64 on 1 B200"
+
+# Operator applications one solve of the default workload takes (GMRES(50) to 1e-8 with the
+# initial residual and one explicit residual per restart), measured by the GPU arm; the CPU
+# reference arm scales its per-matvec time by it.
+MATVECS_PER_SOLVE = {"medium": None, "small": None}
+
+
+def workload_scene(name):
+    from itofoggysim_b200 import scene as S
+    if name == "small":
+        return S.small_cluster()
+    return S.medium_cluster()
+
+
+def algorithmic_flops(sc):
+    """FP64 flops of one direct-operator application, as written: per ordered pair (j <- l)
+    two rotations (source degrees nu <= p_l, target degrees n <= p_j; a and b parts; a real
+    d-matrix times a complex vector = 4 flops per term) and the axial step (4 complex MACs per
+    (k, n, nu), 8 flops each); plus the T-matrix scaling 2 P_j complex multiplies per sphere."""
+    p = sc.p_of_sphere().astype(np.int64)
+    N = len(p)
+    pv = np.arange(0, int(p.max()) + 1)
+    rot = np.cumsum((2 * pv + 1) ** 2) - 1          # sum_{n=1..p} (2n+1)^2
+    # axial terms: sum over k = -min..min of (#n >= max(1,|k|), n <= pj) (#nu >= max(1,|k|), nu <= pl)
+    ps = np.unique(p)
+    ax = {}
+    for a in ps:
+        for b in ps:
+            mn = min(a, b)
+            s = 0
+            for k in range(-mn, mn + 1):
+                lo = max(1, abs(k))
+                s += (a - lo + 1) * (b - lo + 1)
+            ax[(a, b)] = s
+    cnt = {v: int(np.sum(p == v)) for v in ps}
+    total = 0.0
+    for a in ps:
+        for b in ps:
+            pairs = cnt[a] * cnt[b] - (cnt[a] if a == b else 0)
+            total += pairs * (4.0 * 2 * (rot[b] + rot[a]) + 8.0 * 4 * ax[(a, b)])
+    total += 8.0 * float(np.sum(2 * p * (p + 2)))
+    return total
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(np.max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measure_fp64_peak(torch, dev):
+    """cuBLAS DGEMM 8192^3 (float64 torch.matmul), best of 5, TFLOP/s."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_sample(sc, budget_s=15.0, seed=0):
+    """Time the oracle (reference algorithm, translation blocks recomputed per pair) on random
+    ordered sphere pairs for about budget_s seconds on all host cores; returns seconds per
+    operator application (extrapolated over all N (N - 1) pairs) and the sample size."""
+    from oracle import oracle as O
+    P = O.Problem(sc)
+    rng = np.random.default_rng(seed)
+    x = P.vector_b()
+    N = sc.n_spheres
+    done, elapsed = 0, 0.0
+    batch = max(os.cpu_count() or 1, 1)
+    while elapsed < budget_s and done < N * (N - 1):
+        t = rng.integers(0, N, batch)
+        s = (t + rng.integers(1, N, batch)) % N
+        t0 = time.perf_counter()
+        P.pairs_apply(x, t, s)
+        elapsed += time.perf_counter() - t0
+        done += batch
+    per_pair = elapsed / done
+    return per_pair * N * (N - 1), done, elapsed
+
+
+def percentile(v, q):
+    return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sc = workload_scene(args.workload)
+    matvecs = MATVECS_PER_SOLVE[args.workload] or args.matvecs_per_solve
+    cores = os.cpu_count()
+    times, per_mv = [], []
+    for i in range(args.warmup + args.steps):
+        s_mv, pairs, el = cpu_sample(sc, budget_s=args.cpu_budget / max(1, args.steps), seed=i)
+        if i >= args.warmup:
+            per_mv.append(s_mv)
+            times.append(s_mv * matvecs)
+    sps = 1.0 / float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": sps, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(times)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_of(sc, args),
+        "cpu_baseline": {"value": sps, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": "%d random sphere pairs per step, exact Xu translations recomputed per pair "
+                                   "(reference algorithm), extrapolated x N(N-1) pairs x %d matvecs/solve"
+                                   % (pairs, matvecs)},
+        "e2e": {"value": sps, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(sc, args):
+    p = sc.p_of_sphere()
+    return {"workload": sc.name, "spheres": sc.n_spheres, "p_max": int(p.max()), "p_median": float(np.median(p)),
+            "unknowns_ragged": sc.ragged_unknowns(), "matvec": "direct (all pairs, rotation-axial-rotation)",
+            "z_coupling": "h_n^(1)" if sc.z_coupling == 3 else "j_n", "gmres_restart": sc.gmres_restart,
+            "gmres_tolerance": sc.gmres_tolerance, "rhs": 1, "parallelism": "replicas x%d" % args.gpus,
+            "l2": "Krylov basis (restart+1 vectors) exceeds L2; 256 MB L2 flush between steps"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="medium", choices=["medium", "small"])
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU sampling")
+    ap.add_argument("--matvecs-per-solve", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if not args.matvecs_per_solve and not MATVECS_PER_SOLVE[args.workload]:
+            args.matvecs_per_solve = 1
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from itofoggysim_b200 import solver
+
+    sc = workload_scene(args.workload)
+    s = solver.MultiSphereSolver(sc, device=local)
+    n = s.n
+    xbuf = torch.empty(2 * n, dtype=torch.float64, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def step():
+        return s.solve_device(xbuf.data_ptr())
+
+    for _ in range(args.warmup):
+        st = step()
+    torch.cuda.synchronize()
+
+    lat, mv_ms, mv_count, iters, launches = [], 0.0, 0, [], 0
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e_all0 = torch.cuda.Event(enable_timing=True)
+        e_all1 = torch.cuda.Event(enable_timing=True)
+        total_ms = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            st = step()
+            lat.append(st["ms_total"])
+            total_ms += st["ms_total"]
+            mv_ms += st["ms_matvec"]
+            mv_count += st["matvecs"]
+            iters.append(st["iterations"])
+            launches += st["kernel_launches"] + 1
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * args.steps / (max_ms * 1e-3)
+    x_dev = xbuf.cpu().numpy().view(np.complex128)
+    berr = s.get_backward_error()
+
+    # end to end through the public API: scene from host memory, solution back to host
+    e2e_ms = []
+    h2d = 0
+    for i in range(max(1, min(args.steps, 2))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with solver.MultiSphereSolver(sc, device=local) as s2:
+            xh, st2 = s2.solve()
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    h2d = (sc.centres.nbytes + sc.param_index.nbytes + sc.refractive_index.nbytes + sc.radius.nbytes
+           + sc.n_range_param.nbytes + 6 * 8 * sc.n_waves)
+    d2h = xh.nbytes
+    e2e_t = torch.tensor([float(np.mean(e2e_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world / (float(e2e_t.item()) * 1e-3)
+
+    result = None
+    if rank == 0:
+        peak = measure_fp64_peak(torch, dev)
+        flops = algorithmic_flops(sc)
+        avg_mv = mv_ms / max(mv_count, 1)
+        achieved = flops / (avg_mv * 1e-3) / 1e12
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tf):
+            with open(tf) as f:
+                traffic = json.load(f).get(sc.name)
+        result = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_of(sc, args),
+            "latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99)},
+            "solve": {"iterations": iters, "matvecs_per_solve": mv_count // args.steps,
+                      "backward_error": berr, "ms_operator_per_solve": mv_ms / args.steps},
+            "roofline": {"bound": "tensor", "compute": "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_direct (+k_direct_finish)", "flops_per_launch": flops,
+                         "ms_per_launch": avg_mv,
+                         "peak_source": "cuBLAS FP64 DGEMM 8192^3 measured in this run (no FP64 figure in "
+                                        "MEASURED_PEAKS.json)"},
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu:
+            s_mv, pairs, el = cpu_sample(sc, budget_s=args.cpu_budget)
+            per_solve = s_mv * (mv_count / args.steps)
+            result["cpu_baseline"] = {
+                "value": 1.0 / per_solve, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                "sample": "%d random sphere pairs (%.1f s), exact Xu translations recomputed per pair as the "
+                          "reference does, extrapolated x N(N-1) pairs x %d matvecs/solve"
+                          % (pairs, el, mv_count // args.steps)}
+    s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+/*
+ * foggy_gpu.h -- C ABI of the B200 multi-sphere Mie solver (sm_100a, one GPU).
+ *
+ * This is the drop-in boundary for ItoFoggySim's multi-sphere solve.  Each entry point
+ * replaces one reference interface; the citation beside it is the reference file:line
+ * (paths relative to the reference project root).  A Fortran caller binds these through
+ * iso_c_binding (itofoggysim_b200/fortran/foggy_gpu_f.f90), Python through ctypes
+ * (itofoggysim_b200/_native.py).
+ *
+ * Conventions
+ *   - every call returns FOGGY_OK (0) or a negative status; foggy_last_error() explains it;
+ *   - complex numbers are two interleaved doubles (Fortran complex(8), C double _Complex);
+ *   - coefficient vectors use the reference's flat layout: per sphere i (in input order)
+ *     a block of 2*C complex entries, C = (n2+1)^2 - n1^2 for the global n_range [n1,n2]:
+ *     first a_nm for n = n1..n2, m = -n..n, then b_nm in the same order
+ *     (FoggySim/src/lib/mie_theory/lib_mie_ms_solver_interface_helper_functions.f90:49-163);
+ *     entries above a sphere's own truncation order are zero;
+ *   - pointers flagged FOGGY_MEM_HOST are ordinary host memory, FOGGY_MEM_DEVICE are CUDA
+ *     device pointers on the handle's device; all buffers are caller-owned;
+ *   - lengths are in one unit of the caller's choice (the reference uses metres); the
+ *     wavenumber is k = 2*pi*n_medium/lambda_0.
+ *   - a handle is used by one host thread at a time; it owns one CUDA stream.
+ */
+#ifndef FOGGY_GPU_H
+#define FOGGY_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------------------- */
+#define FOGGY_OK                 0
+#define FOGGY_ERR_ARGUMENT      -1   /* invalid argument or size                        */
+#define FOGGY_ERR_STATE         -2   /* call out of order (e.g. solve before spheres)   */
+#define FOGGY_ERR_CUDA          -3   /* a CUDA runtime call failed                      */
+#define FOGGY_ERR_NOMEM         -4   /* the solve does not fit the device memory budget */
+#define FOGGY_ERR_NOT_CONVERGED -5   /* GMRES stopped at max_iterations above tolerance */
+#define FOGGY_ERR_BREAKDOWN     -6   /* GMRES breakdown (zero Krylov vector)            */
+#define FOGGY_ERR_NAN           -7   /* NaN or Inf met in the residual                  */
+#define FOGGY_ERR_UNSUPPORTED   -8   /* option not built                                */
+
+#define FOGGY_MEM_HOST   0
+#define FOGGY_MEM_DEVICE 1
+
+#define FOGGY_MATVEC_DIRECT 0   /* all sphere pairs (..._without_transposed_all)        */
+#define FOGGY_MATVEC_MLFMM  1   /* multilevel FMM (lib_mie_ms_ml_fmm_calculate_vector_b) */
+
+typedef struct foggy_handle_s* foggy_handle;
+
+/* Solver configuration.  Mirrors the Fortran state the reference keeps in
+ * simulation_data%spherical_harmonics (FoggySim/src/lib/mie_theory/lib_mie_type.f90:43-99),
+ * lib_mie_ms_solver_parameter_type (lib_mie_ms_solver_interface.f90:63-67) and
+ * solver_gmres_parameter_type (lib_solver_GMRES.f90:39-50). */
+typedef struct foggy_params {
+    double  lambda_0;            /* vacuum wavelength                                       */
+    double  n_medium;            /* refractive index of the medium (real)                   */
+    int32_t n_range[2];          /* global degree range [n1, n2], n1 >= 1                   */
+    int32_t z_coupling;          /* radial function of the sphere-sphere translation:
+                                    1 = j_n (the reference's z_selector_incident_wave in all of
+                                    its tests), 3 = h_n^(1) (scattered-wave coupling)       */
+    int32_t reference_row_rule;  /* 1: zero the coupling rows of a sphere whose n_range does
+                                    not cover the global n_range, as the reference does
+                                    (lib_mie_ms_solver_interface.f90:965-978); 0: couple every
+                                    sphere up to its own truncation order                  */
+    int32_t matvec_mode;         /* FOGGY_MATVEC_DIRECT or FOGGY_MATVEC_MLFMM                */
+    int32_t use_initial_guess;   /* 1: x0 = single-sphere solution a_n p, b_n q            */
+    int32_t gmres_restart;       /* Krylov dimension per restart cycle (reference: 10)      */
+    int32_t gmres_max_iterations;/* reference: 1000                                        */
+    double  gmres_tolerance;     /* stop when ||b - A x|| / ||b|| <= tolerance              */
+    int32_t tree_l_max;          /* 0: reference rule from tree_s_opt; > 0: fixed deepest level */
+    int32_t tree_s_opt;          /* elements per leaf for the reference l_max rule (10)     */
+    double  fmm_digits;          /* d0 of the per-level order L = kd + 1.8 d0^(2/3) (kd)^(1/3) */
+    int64_t device_memory_budget;/* bytes the handle may allocate; 0 = 90% of free memory  */
+} foggy_params;
+
+/* Per-solve statistics (the reference prints these; here they are returned). */
+typedef struct foggy_stats {
+    int32_t iterations;          /* Arnoldi steps performed                                 */
+    int32_t restarts;
+    int32_t matvecs;
+    int32_t status;              /* FOGGY_OK or FOGGY_ERR_NOT_CONVERGED / _BREAKDOWN / _NAN */
+    double  backward_error;      /* final true ||b - A x|| / ||b||                         */
+    double  ms_total;            /* device time of the solve                                */
+    double  ms_matvec;           /* device time inside the matvec                           */
+    double  ms_setup;            /* translation tables, Mie coefficients, right-hand side    */
+    int64_t kernel_launches;     /* CUDA kernels this library launched during the solve     */
+} foggy_stats;
+
+/* ---- lifecycle ------------------------------------------------------------------------ */
+
+/* Fills *p with the reference defaults (lib_mie_ms_constructor, lib_mie_multi_sphere.f90:111-150;
+ * lib_mie_ms_solver_gmres_get_parameter_std_values, lib_solver_GMRES.f90:93-106). */
+void foggy_default_params(foggy_params* p);
+
+/* Replaces lib_mie_ms_constructor + lib_mie_ms_solver_constructor
+ * (lib_mie_multi_sphere.f90:111-150, lib_mie_ms_solver_interface.f90:91-129). */
+int32_t foggy_create(const foggy_params* params, int32_t device, foggy_handle* out);
+
+/* Replaces lib_mie_ms_solver_destructor (lib_mie_ms_solver_interface.f90:131-141). */
+int32_t foggy_destroy(foggy_handle h);
+
+/* Message of the last failing call on this handle (or of the last failing foggy_create). */
+const char* foggy_last_error(foggy_handle h);
+
+/* Replaces lib_mie_ms_solver_set_n_range / _set_max_iterations / _use_ml_fmm
+ * (lib_mie_ms_solver_interface.f90:156-201). */
+int32_t foggy_set_params(foggy_handle h, const foggy_params* params);
+
+/* ---- scene ---------------------------------------------------------------------------- */
+
+/* Sphere list and shared sphere parameters; replaces filling simulation_data%sphere_list and
+ * %sphere_parameter_list through lib_mie_type_func_get_sphere_parameter
+ * (FoggySim/src/lib/mie_theory/lib_mie_type_functions.f90:46-86).
+ *   centres[3*n_spheres]         d_0_j, x y z per sphere
+ *   param_index[n_spheres]       0-based index into the parameter arrays
+ *   refractive_index[2*n_param]  complex particle index (re, im)
+ *   radius[n_param]
+ *   n_range[2*n_param]           per-parameter degree range [1, n_max] (n_max <= global n2)
+ * Mie coefficients a_n, b_n are computed on the device in FP64. */
+int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centres,
+                          const int32_t* param_index, int32_t n_param,
+                          const double* refractive_index, const double* radius,
+                          const int32_t* n_range);
+
+/* Plane-wave illumination; replaces lib_mie_type_func_get_plane_wave_illumination
+ * (lib_mie_type_functions.f90:122-167) with the Jones vector and phase of
+ * lib_mie_illumination_get_p_q_j_j_multi_plane_wave (lib_mie_illumination.f90:392-478).
+ *   theta[nw], phi[nw]   propagation direction of wave i
+ *   jones[4*nw]          (re x, im x, re y, im y): x -> TM part, y -> TE part
+ *   g[nw]                amplitude weight, phase[nw] extra phase
+ *   d_0_i[3*nw]          origin of the wave's coordinate system
+ * All waves of one call form ONE right-hand side, as in the reference. */
+int32_t foggy_set_plane_waves(foggy_handle h, int32_t nw, const double* theta, const double* phi,
+                              const double* jones, const double* g, const double* phase,
+                              const double* d_0_i);
+
+/* Number of complex entries of one coefficient vector in the reference layout. */
+int64_t foggy_vector_length(foggy_handle h);
+
+/* ---- parity / building blocks ---------------------------------------------------------- */
+
+/* Mie coefficients a_n, b_n for parameter set ip, n = n1..n2 of that parameter
+ * (lib_mie_ss_helper_functions.f90:628-722).  a, b: complex[n2-n1+1], host memory. */
+int32_t foggy_get_mie_coefficients(foggy_handle h, int32_t ip, double* a, double* b);
+
+/* Right-hand side b = [a_n p_nm ; b_n q_nm] per sphere
+ * (lib_mie_ms_solver_get_vector_b_all, lib_mie_ms_solver_interface.f90:230-315). */
+int32_t foggy_get_vector_b(foggy_handle h, double* b, int32_t mem);
+
+/* y = A x (lib_mie_ms_solver_calculate_vector_b, lib_mie_ms_solver_interface.f90:739-783,
+ * direct form 806-998; ML-FMM form lib_mie_ms_ml_fmm_calculate_vector_b,
+ * lib_mie_ms_ml_fmm_interface.f90:110-176). */
+int32_t foggy_matvec(foggy_handle h, const double* x, double* y, int32_t mem);
+
+/* Solve A x = b by restarted GMRES on the device; replaces lib_mie_ms_solver_run and
+ * lib_mie_ms_solver_gmres_run (lib_mie_ms_solver_interface.f90:143-154,
+ * lib_solver_GMRES.f90:116-316).  x0 may be NULL (then the params' use_initial_guess
+ * decides between 0 and the single-sphere solution).  stats may be NULL. */
+int32_t foggy_solve(foggy_handle h, const double* x0, double* x, int32_t mem, foggy_stats* stats);
+
+/* Backward error of the last solve (lib_mie_ms_solver_get_backward_error, :203-209). */
+double foggy_get_backward_error(foggy_handle h);
+
+/* Extinction, scattering and absorption cross-sections of the whole cluster for the
+ * coefficient vector x (reference layout).  The reference has only the single-sphere form
+ * (lib_mie_ss_helper_functions.f90:1380-1475); the cluster form sums Xu's per-sphere
+ * extinction and absorption terms. out[3] = {C_sca, C_ext, C_abs}. */
+int32_t foggy_cross_sections(foggy_handle h, const double* x, int32_t mem, double* out);
+
+/* Vector translation coefficients A_mn^{mu nu}, B_mn^{mu nu} at kd = x, direction (theta,
+ * phi), computed on the device by rotation + axial translation + rotation back; replaces
+ * lib_math_vector_spherical_harmonics_translation_coeff_r
+ * (libmath/src/math/lib_math_vector_spherical_harmonics.f90:1354-1585).
+ * A, B: host complex[C_n * C_nu], row (n, m) major, C_n = (n2+1)^2-n1^2. */
+int32_t foggy_translation_coefficients(double x, double theta, double phi,
+                                       const int32_t n_range[2], const int32_t nu_range[2],
+                                       int32_t z_selector, double* A, double* B);
+
+/* Wigner 3j symbol (j1 j2 j3; m1 m2 m3) for integer arguments; replaces lib_math_wigner_3j
+ * (libmath/src/math/lib_math_wigner.f90:45-72, which calls wigxjpf).  Host computation by the
+ * three-term recurrence that also builds the device's axial translation tables. */
+double foggy_wigner_3j(int32_t j1, int32_t j2, int32_t j3, int32_t m1, int32_t m2, int32_t m3);
+
+/* ---- octree (libtree) ------------------------------------------------------------------ */
+
+/* Builds the octree of the sphere centres on the device; replaces lib_tree_constructor
+ * (libtree/src/lib/lib_tree.f90:147-270).  Outputs (each may be NULL):
+ *   uindex_out[n_spheres]  universal index of each sphere at level l_max (input order)
+ *   order_out[n_spheres]   sphere indices sorted by their level-21 universal index
+ *   l_min_out, l_max_out   level range (lib_tree_get_level_min/max, lib_tree.f90:1162-1242) */
+int32_t foggy_build_tree(foggy_handle h, int64_t* uindex_out, int32_t* order_out,
+                         int32_t* l_min_out, int32_t* l_max_out);
+
+/* Universal index of points already scaled to [0,1)^3 at level l (1..21); replaces
+ * lib_tree_hf_get_universal_index (libtree/src/lib/lib_tree_helper_functions.f90:202-364).
+ * points[3*n] host memory, out[n]. */
+int32_t foggy_universal_index(int32_t n, const double* points, int32_t l, int64_t* out);
+
+/* Number of boxes at tree level l and their universal indices in ascending order
+ * (lib_ml_fmm_hf_create_hierarchy, libmlfmm/src/lib/lib_ml_fmm_helper_functions.f90:366-457).
+ * Call with boxes == NULL to query the count. */
+int32_t foggy_tree_boxes(foggy_handle h, int32_t l, int64_t* boxes, int32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FOGGY_GPU_H */

@@ -1,0 +1,1046 @@
+// C ABI of libfoggy_b200 (include/foggy_gpu.h).  Host orchestration of the device kernels:
+// scene upload, Mie coefficients, right-hand side, operator, device GMRES, cross-sections and
+// the octree keys.  Every entry point returns a status code; no exception crosses the ABI.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "foggy_kernels.cuh"
+
+using namespace foggy;
+
+namespace {
+const double kPi = 3.14159265358979323846264338327950288;
+std::mutex g_err_mu;
+std::string g_err;   // error of a failing foggy_create / handle-less call
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct foggy_handle_s {
+    foggy_params prm{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::vector<void*> allocs;   // every device allocation, freed in destroy
+    size_t bytes_in_use = 0;
+    size_t budget = 0;
+
+    // scene (host)
+    int N = 0, NP = 0, pmax = 0, pg = 0;
+    std::vector<double> centres;
+    std::vector<int> pidx, p_s, p_param, couple;
+    std::vector<int64_t> off;
+    int64_t n_unk = 0;
+    std::vector<double> mre, mim, radius;
+    std::vector<int> nr;
+    // scene (device)
+    double* d_centres = nullptr;
+    int* d_p = nullptr;
+    int64_t* d_off = nullptr;
+    cplx* d_an = nullptr;
+    cplx* d_bn = nullptr;
+    cplx* d_an_p = nullptr;
+    cplx* d_bn_p = nullptr;
+    int* d_couple = nullptr;
+    double* d_g = nullptr;
+    // translation tables
+    int tab_pmax = -1;
+    int32_t* d_axoff = nullptr;
+    double* d_ga = nullptr;
+    double* d_gb = nullptr;
+    double* d_sqrt_binom = nullptr;
+    double* d_rs = nullptr;
+    int K = 0;
+    // waves and right-hand side
+    std::vector<WaveDev> waves;
+    bool rhs_ready = false;
+    cplx* d_b = nullptr;
+    cplx* d_pq = nullptr;
+    // operator scratch
+    int chunks = 1;
+    cplx* d_partial = nullptr;
+    cplx* d_tmp_in = nullptr;    // ragged work vectors
+    cplx* d_tmp_out = nullptr;
+    cplx* d_ref_a = nullptr;     // reference-layout staging (host-pointer calls)
+    cplx* d_ref_b = nullptr;
+    // GMRES workspace
+    int ws_restart = 0;
+    cplx* d_V = nullptr;
+    cplx* d_w = nullptr;
+    cplx* d_x = nullptr;
+    cplx* d_r = nullptr;
+    cplx* d_H = nullptr;
+    cplx* d_cs = nullptr;
+    double* d_sn = nullptr;
+    cplx* d_gv = nullptr;
+    cplx* d_h = nullptr;
+    cplx* d_c = nullptr;
+    cplx* d_y = nullptr;
+    cplx* d_part = nullptr;
+    double* d_npart = nullptr;
+    double* d_scal = nullptr;    // [0] hn, [1] beta, [2] res_est, [3] bnorm
+    int* d_flags = nullptr;
+    double* h_pin = nullptr;     // pinned: res_est, beta, bnorm
+    int* h_pin_flags = nullptr;
+    double last_berr = -1.0;
+    int64_t launches = 0;        // kernels launched by the current solve
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm0 = nullptr, evm1 = nullptr;
+    // tree
+    unsigned long long* d_keys = nullptr;
+    int* d_idx = nullptr;
+    unsigned long long* d_keys_sorted = nullptr;
+    int* d_idx_sorted = nullptr;
+    int tree_lmax = 0, tree_lmin = 0;
+    bool tree_ready = false;
+};
+
+namespace {
+
+int fail(foggy_handle h, int code, const std::string& msg) {
+    if (h) {
+        h->err = msg;
+    } else {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_err = msg;
+    }
+    return code;
+}
+
+#define CK(h, call)                                                                         \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(h, FOGGY_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CKL(h)                                                                              \
+    do {                                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                                \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(h, FOGGY_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int dalloc(foggy_handle h, T** p, size_t count) {
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = 16;
+    if (h->budget && h->bytes_in_use + bytes > h->budget)
+        return fail(h, FOGGY_ERR_NOMEM, "device memory budget exceeded (" + std::to_string(h->bytes_in_use + bytes) +
+                                            " > " + std::to_string(h->budget) + " bytes)");
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    h->allocs.push_back(*p);
+    h->bytes_in_use += bytes;
+    return FOGGY_OK;
+}
+
+template <class T>
+void dfree(foggy_handle h, T*& p) {
+    if (!p) return;
+    auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)p);
+    if (it != h->allocs.end()) h->allocs.erase(it);
+    cudaFree(p);
+    p = nullptr;
+}
+
+#define TRY(x)                      \
+    do {                            \
+        int r_ = (x);               \
+        if (r_ != FOGGY_OK) return r_; \
+    } while (0)
+
+void to_spherical(const double* c, double* rho, double* theta, double* phi) {
+    double r = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    *rho = r;
+    *theta = (r == 0.0) ? 0.0 : std::acos(c[2] / r);
+    *phi = (c[0] == 0.0 && c[1] == 0.0) ? 0.0 : std::atan2(c[1], c[0]);
+}
+
+double wavenumber(const foggy_params& p) { return 2.0 * kPi * p.n_medium / p.lambda_0; }
+
+SceneView scene_view(foggy_handle h) {
+    SceneView s;
+    s.n = h->N;
+    s.pmax = h->pmax;
+    s.k = wavenumber(h->prm);
+    s.centres = h->d_centres;
+    s.p = h->d_p;
+    s.off = h->d_off;
+    s.an = h->d_an;
+    s.bn = h->d_bn;
+    s.couple = h->d_couple;
+    return s;
+}
+
+// 3j tables, g_nm and d-table helper tables for degrees <= pmax
+int ensure_tables(foggy_handle h, int pmax) {
+    if (h->tab_pmax >= pmax) return FOGGY_OK;
+    dfree(h, h->d_axoff);
+    dfree(h, h->d_ga);
+    dfree(h, h->d_gb);
+    dfree(h, h->d_sqrt_binom);
+    dfree(h, h->d_rs);
+    dfree(h, h->d_g);
+    AxialTables t;
+    build_axial_tables(pmax, t);
+    TRY(dalloc(h, &h->d_axoff, t.offset.size()));
+    TRY(dalloc(h, &h->d_ga, t.ga.size()));
+    TRY(dalloc(h, &h->d_gb, t.gb.size()));
+    CK(h, cudaMemcpy(h->d_axoff, t.offset.data(), t.offset.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_ga, t.ga.data(), t.ga.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_gb, t.gb.data(), t.gb.size() * sizeof(double), cudaMemcpyHostToDevice));
+    int K = pmax;
+    std::vector<double> sb((size_t)(K + 1) * (2 * K + 1), 0.0), rs((size_t)(K + 1) * (K + 1), 0.0);
+    for (int J = 0; J <= K; ++J)
+        for (int m = -J; m <= J; ++m) {
+            long double c = 1.0L;   // C(2J, J+m)
+            int a = J + m, b = J - m;
+            for (int i = 1; i <= b; ++i) c = c * (a + i) / i;
+            sb[(size_t)J * (2 * K + 1) + (m + K)] = (double)std::sqrt(c);
+        }
+    for (int j = 0; j <= K; ++j)
+        for (int m = 0; m <= j; ++m) rs[(size_t)j * (K + 1) + m] = std::sqrt((double)j * j - (double)m * m);
+    TRY(dalloc(h, &h->d_sqrt_binom, sb.size()));
+    TRY(dalloc(h, &h->d_rs, rs.size()));
+    CK(h, cudaMemcpy(h->d_sqrt_binom, sb.data(), sb.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_rs, rs.data(), rs.size() * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<double> g;
+    build_g_table(pmax, g);
+    TRY(dalloc(h, &h->d_g, g.size()));
+    CK(h, cudaMemcpy(h->d_g, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->K = K;
+    h->tab_pmax = pmax;
+    return FOGGY_OK;
+}
+
+DirectArgs direct_args(foggy_handle h, const cplx* x) {
+    DirectArgs a;
+    a.sc = scene_view(h);
+    a.ax.pmax = h->tab_pmax;
+    a.ax.offset = h->d_axoff;
+    a.ax.ga = h->d_ga;
+    a.ax.gb = h->d_gb;
+    a.sqrt_binom = h->d_sqrt_binom;
+    a.rs = h->d_rs;
+    a.K = h->K;
+    a.z = h->prm.z_coupling;
+    a.x = x;
+    a.partial = h->d_partial;
+    a.chunks = h->chunks;
+    a.n_unk = h->n_unk;
+    return a;
+}
+
+// y = A x in the device layout
+int apply_operator(foggy_handle h, const cplx* x, cplx* y) {
+    if (h->prm.matvec_mode != FOGGY_MATVEC_DIRECT)
+        return fail(h, FOGGY_ERR_UNSUPPORTED, "matvec_mode: only FOGGY_MATVEC_DIRECT is built");
+    DirectArgs a = direct_args(h, x);
+    launch_direct(a, h->stream);
+    CKL(h);
+    k_direct_finish<<<h->N, 256, 0, h->stream>>>(a.sc, x, h->d_partial, h->chunks, h->n_unk, y);
+    h->launches += 2;
+    CKL(h);
+    return FOGGY_OK;
+}
+
+int ensure_rhs(foggy_handle h) {
+    if (h->rhs_ready) return FOGGY_OK;
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    if (h->waves.empty()) return fail(h, FOGGY_ERR_STATE, "no plane waves set");
+    int nw = (int)h->waves.size();
+    WaveDev* d_w = nullptr;
+    double *d_pi = nullptr, *d_tau = nullptr;
+    size_t S = (size_t)(h->pmax + 1) * (h->pmax + 1);
+    CK(h, cudaMalloc(&d_w, nw * sizeof(WaveDev)));
+    CK(h, cudaMalloc(&d_pi, nw * S * sizeof(double)));
+    CK(h, cudaMalloc(&d_tau, nw * S * sizeof(double)));
+    CK(h, cudaMemcpyAsync(d_w, h->waves.data(), nw * sizeof(WaveDev), cudaMemcpyHostToDevice, h->stream));
+    k_pitau<<<nw, h->pmax + 1, 0, h->stream>>>(nw, d_w, h->pmax, d_pi, d_tau);
+    k_rhs<<<h->N, 128, 0, h->stream>>>(scene_view(h), nw, d_w, h->pmax, d_pi, d_tau, h->d_b, h->d_pq);
+    h->launches += 2;
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_w);
+    cudaFree(d_pi);
+    cudaFree(d_tau);
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("rhs: ") + cudaGetErrorString(e));
+    CKL(h);
+    h->rhs_ready = true;
+    return FOGGY_OK;
+}
+
+void free_scene(foggy_handle h) {
+    dfree(h, h->d_centres);
+    dfree(h, h->d_p);
+    dfree(h, h->d_off);
+    dfree(h, h->d_an);
+    dfree(h, h->d_bn);
+    dfree(h, h->d_an_p);
+    dfree(h, h->d_bn_p);
+    dfree(h, h->d_couple);
+    dfree(h, h->d_b);
+    dfree(h, h->d_pq);
+    dfree(h, h->d_partial);
+    dfree(h, h->d_tmp_in);
+    dfree(h, h->d_tmp_out);
+    dfree(h, h->d_ref_a);
+    dfree(h, h->d_ref_b);
+    dfree(h, h->d_V);
+    dfree(h, h->d_w);
+    dfree(h, h->d_x);
+    dfree(h, h->d_r);
+    dfree(h, h->d_keys);
+    dfree(h, h->d_idx);
+    dfree(h, h->d_keys_sorted);
+    dfree(h, h->d_idx_sorted);
+    h->ws_restart = 0;
+    h->tree_ready = false;
+    h->rhs_ready = false;
+}
+
+int ensure_workspace(foggy_handle h, int restart) {
+    if (h->ws_restart >= restart && h->d_V) return FOGGY_OK;
+    dfree(h, h->d_V);
+    dfree(h, h->d_H);
+    dfree(h, h->d_cs);
+    dfree(h, h->d_sn);
+    dfree(h, h->d_gv);
+    dfree(h, h->d_h);
+    dfree(h, h->d_c);
+    dfree(h, h->d_y);
+    dfree(h, h->d_part);
+    TRY(dalloc(h, &h->d_V, (size_t)(restart + 1) * h->n_unk));
+    if (!h->d_w) TRY(dalloc(h, &h->d_w, h->n_unk));
+    if (!h->d_x) TRY(dalloc(h, &h->d_x, h->n_unk));
+    if (!h->d_r) TRY(dalloc(h, &h->d_r, h->n_unk));
+    TRY(dalloc(h, &h->d_H, (size_t)(restart + 1) * restart));
+    TRY(dalloc(h, &h->d_cs, restart));
+    TRY(dalloc(h, &h->d_sn, restart));
+    TRY(dalloc(h, &h->d_gv, restart + 1));
+    TRY(dalloc(h, &h->d_h, restart + 1));
+    TRY(dalloc(h, &h->d_c, restart + 1));
+    TRY(dalloc(h, &h->d_y, restart + 1));
+    TRY(dalloc(h, &h->d_part, (size_t)kRedBlocks * (restart + 1)));
+    if (!h->d_npart) TRY(dalloc(h, &h->d_npart, kRedBlocks));
+    if (!h->d_scal) TRY(dalloc(h, &h->d_scal, 8));
+    if (!h->d_flags) TRY(dalloc(h, &h->d_flags, 4));
+    h->ws_restart = restart;
+    return FOGGY_OK;
+}
+
+int norm_dev(foggy_handle h, const cplx* v, double* out_dev) {
+    k_norm_partial<<<kRedBlocks, 256, 0, h->stream>>>(v, h->n_unk, h->d_npart);
+    k_norm_reduce<<<1, 256, 0, h->stream>>>(h->d_npart, out_dev);
+    h->launches += 2;
+    CKL(h);
+    return FOGGY_OK;
+}
+
+int grid_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 8); }
+
+// GMRES(m) with classical Gram-Schmidt and one reorthogonalisation (CGS2), Givens rotations
+// and the explicit residual at each restart.
+int gmres(foggy_handle h, foggy_stats* st) {
+    const int m = h->prm.gmres_restart;
+    const int maxit = h->prm.gmres_max_iterations;
+    const double tol = h->prm.gmres_tolerance;
+    const int64_t n = h->n_unk;
+    const int G = grid_for(n);
+    double* d_hn = h->d_scal + 0;
+    double* d_beta = h->d_scal + 1;
+    double* d_res = h->d_scal + 2;
+    double* d_bn = h->d_scal + 3;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> mv_events;
+    auto matvec = [&](const cplx* x, cplx* y) -> int {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, h->stream);
+        int r = apply_operator(h, x, y);
+        cudaEventRecord(b, h->stream);
+        mv_events.push_back({a, b});
+        st->matvecs++;
+        return r;
+    };
+    auto cleanup = [&]() {
+        for (auto& e : mv_events) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e.first, e.second);
+            st->ms_matvec += ms;
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        mv_events.clear();
+    };
+    TRY(norm_dev(h, h->d_b, d_bn));
+    TRY(matvec(h->d_x, h->d_w));
+    k_sub<<<G, 256, 0, h->stream>>>(h->d_b, h->d_w, h->d_r, n);
+    h->launches += 1;
+    TRY(norm_dev(h, h->d_r, d_beta));
+    CK(h, cudaMemcpyAsync(h->h_pin, h->d_scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    double bnorm = h->h_pin[3];
+    double beta = h->h_pin[1];
+    if (bnorm == 0.0) {
+        CK(h, cudaMemsetAsync(h->d_x, 0, n * sizeof(cplx), h->stream));
+        st->backward_error = 0.0;
+        cleanup();
+        return FOGGY_OK;
+    }
+    double berr = beta / bnorm;
+    int status = FOGGY_OK;
+    if (!std::isfinite(berr)) {
+        cleanup();
+        st->backward_error = berr;
+        return FOGGY_ERR_NAN;
+    }
+    while (berr > tol && st->iterations < maxit) {
+        k_scale_copy<<<G, 256, 0, h->stream>>>(h->d_r, d_beta, h->d_V, n);
+        k_init_cycle<<<1, 64, 0, h->stream>>>(h->d_gv, m + 1, d_beta, h->d_flags);
+        h->launches += 2;
+        int k = 0;
+        for (; k < m && st->iterations < maxit; ++k) {
+            cplx* vk = h->d_V + (size_t)k * n;
+            cplx* vk1 = h->d_V + (size_t)(k + 1) * n;
+            TRY(matvec(vk, h->d_w));
+            k_dots_partial<<<kRedBlocks, 256, 0, h->stream>>>(h->d_V, n, k + 1, h->d_w, n, h->d_part);
+            k_dots_reduce<<<k + 1, 256, 0, h->stream>>>(h->d_part, k + 1, h->d_h, 0);
+            k_axpy_multi<<<G, 256, 0, h->stream>>>(h->d_V, n, k + 1, h->d_h, h->d_w, n);
+            k_dots_partial<<<kRedBlocks, 256, 0, h->stream>>>(h->d_V, n, k + 1, h->d_w, n, h->d_part);
+            k_dots_reduce<<<k + 1, 256, 0, h->stream>>>(h->d_part, k + 1, h->d_c, 0);
+            k_axpy_multi<<<G, 256, 0, h->stream>>>(h->d_V, n, k + 1, h->d_c, h->d_w, n);
+            TRY(norm_dev(h, h->d_w, d_hn));
+            k_scale_copy<<<G, 256, 0, h->stream>>>(h->d_w, d_hn, vk1, n);
+            k_givens<<<1, 1, 0, h->stream>>>(h->d_H, m, h->d_cs, h->d_sn, h->d_gv, h->d_h, h->d_c, d_hn, k, d_res,
+                                             h->d_flags);
+            CKL(h);
+            h->launches += 8;
+            CK(h, cudaMemcpyAsync(h->h_pin, h->d_scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaMemcpyAsync(h->h_pin_flags, h->d_flags, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+            st->iterations++;
+            if (h->h_pin_flags[0] == 2) { status = FOGGY_ERR_NAN; break; }
+            if (h->h_pin_flags[0] == 1) { status = FOGGY_ERR_BREAKDOWN; break; }
+            if (h->h_pin[2] / bnorm <= tol || h->h_pin[0] == 0.0) { ++k; break; }
+        }
+        if (status == FOGGY_ERR_NAN) break;
+        if (status == FOGGY_ERR_BREAKDOWN) {
+            if (k == 0) break;
+            status = FOGGY_OK;   // solve with the columns built so far
+        }
+        if (k > 0) {
+            k_trisolve<<<1, 1, 0, h->stream>>>(h->d_H, m, h->d_gv, k, h->d_y);
+            k_update_x<<<G, 256, 0, h->stream>>>(h->d_x, h->d_V, n, h->d_y, k, n);
+            h->launches += 2;
+        }
+        st->restarts++;
+        TRY(matvec(h->d_x, h->d_w));
+        k_sub<<<G, 256, 0, h->stream>>>(h->d_b, h->d_w, h->d_r, n);
+        h->launches += 1;
+    h->launches += 1;
+        TRY(norm_dev(h, h->d_r, d_beta));
+        CK(h, cudaMemcpyAsync(h->h_pin, h->d_scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        beta = h->h_pin[1];
+        berr = beta / bnorm;
+        if (!std::isfinite(berr)) { status = FOGGY_ERR_NAN; break; }
+    }
+    cleanup();
+    st->backward_error = berr;
+    if (status == FOGGY_OK && berr > tol) status = FOGGY_ERR_NOT_CONVERGED;
+    return status;
+}
+
+}  // namespace
+
+// =====================================================================================
+extern "C" {
+
+void foggy_default_params(foggy_params* p) {
+    std::memset(p, 0, sizeof(*p));
+    p->lambda_0 = 0.55;
+    p->n_medium = 1.0;
+    p->n_range[0] = 1;
+    p->n_range[1] = 1;
+    p->z_coupling = 1;
+    p->reference_row_rule = 1;
+    p->matvec_mode = FOGGY_MATVEC_DIRECT;
+    p->use_initial_guess = 0;
+    p->gmres_restart = 10;
+    p->gmres_max_iterations = 1000;
+    p->gmres_tolerance = 1e-6;
+    p->tree_l_max = 0;
+    p->tree_s_opt = 10;
+    p->fmm_digits = 3.0;
+    p->device_memory_budget = 0;
+}
+
+static int check_params(foggy_handle h, const foggy_params* p) {
+    if (!p) return fail(h, FOGGY_ERR_ARGUMENT, "params is NULL");
+    if (!(p->lambda_0 > 0) || !(p->n_medium > 0)) return fail(h, FOGGY_ERR_ARGUMENT, "lambda_0 and n_medium must be > 0");
+    if (p->n_range[0] != 1) return fail(h, FOGGY_ERR_UNSUPPORTED, "n_range(1) must be 1");
+    if (p->n_range[1] < 1 || p->n_range[1] > kMaxDegree)
+        return fail(h, FOGGY_ERR_ARGUMENT, "n_range(2) must be in [1, 45]");
+    if (p->z_coupling < 1 || p->z_coupling > 4) return fail(h, FOGGY_ERR_ARGUMENT, "z_coupling must be 1..4");
+    if (p->gmres_restart < 1 || p->gmres_restart > 60) return fail(h, FOGGY_ERR_ARGUMENT, "gmres_restart must be 1..60");
+    if (p->gmres_max_iterations < 1) return fail(h, FOGGY_ERR_ARGUMENT, "gmres_max_iterations must be >= 1");
+    if (!(p->gmres_tolerance > 0)) return fail(h, FOGGY_ERR_ARGUMENT, "gmres_tolerance must be > 0");
+    if (p->matvec_mode != FOGGY_MATVEC_DIRECT && p->matvec_mode != FOGGY_MATVEC_MLFMM)
+        return fail(h, FOGGY_ERR_ARGUMENT, "matvec_mode");
+    return FOGGY_OK;
+}
+
+int32_t foggy_create(const foggy_params* params, int32_t device, foggy_handle* out) {
+    if (!out) return fail(nullptr, FOGGY_ERR_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int rc = check_params(nullptr, params);
+    if (rc) return rc;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(nullptr, FOGGY_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return fail(nullptr, FOGGY_ERR_ARGUMENT, "device index out of range");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, FOGGY_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    foggy_handle h = new (std::nothrow) foggy_handle_s();
+    if (!h) return fail(nullptr, FOGGY_ERR_NOMEM, "host allocation");
+    h->prm = *params;
+    h->device = device;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&h->h_pin, 8 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&h->h_pin_flags, 4 * sizeof(int)) != cudaSuccess) {
+        delete h;
+        return fail(nullptr, FOGGY_ERR_CUDA, "stream or pinned allocation failed");
+    }
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    h->budget = params->device_memory_budget > 0 ? (size_t)params->device_memory_budget : (size_t)(0.9 * fr);
+    *out = h;
+    return FOGGY_OK;
+}
+
+int32_t foggy_destroy(foggy_handle h) {
+    if (!h) return FOGGY_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    if (h->h_pin) cudaFreeHost(h->h_pin);
+    if (h->h_pin_flags) cudaFreeHost(h->h_pin_flags);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return FOGGY_OK;
+}
+
+const char* foggy_last_error(foggy_handle h) {
+    if (h) return h->err.c_str();
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_err.c_str();
+}
+
+int32_t foggy_set_params(foggy_handle h, const foggy_params* params) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    TRY(check_params(h, params));
+    bool scene_change = params->n_range[1] != h->prm.n_range[1] || params->lambda_0 != h->prm.lambda_0 ||
+                        params->n_medium != h->prm.n_medium ||
+                        params->reference_row_rule != h->prm.reference_row_rule;
+    foggy_params old = h->prm;
+    h->prm = *params;
+    if (scene_change && h->N > 0) {
+        // rebuild the scene with the new global settings
+        std::vector<double> c = h->centres, mr, rad = h->radius;
+        std::vector<int> pi = h->pidx, nr = h->nr;
+        for (int i = 0; i < h->NP; ++i) {
+            mr.push_back(h->mre[i]);
+            mr.push_back(h->mim[i]);
+        }
+        int rc = foggy_set_spheres(h, h->N, c.data(), pi.data(), h->NP, mr.data(), rad.data(), nr.data());
+        if (rc) {
+            h->prm = old;
+            return rc;
+        }
+    }
+    return FOGGY_OK;
+}
+
+int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centres, const int32_t* param_index,
+                          int32_t n_param, const double* refractive_index, const double* radius,
+                          const int32_t* n_range) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (n_spheres < 1 || n_param < 1 || !centres || !param_index || !refractive_index || !radius || !n_range)
+        return fail(h, FOGGY_ERR_ARGUMENT, "empty or NULL sphere input");
+    CK(h, cudaSetDevice(h->device));
+    free_scene(h);
+    const int pg = h->prm.n_range[1];
+    h->N = n_spheres;
+    h->NP = n_param;
+    h->pg = pg;
+    h->centres.assign(centres, centres + 3 * (size_t)n_spheres);
+    h->pidx.assign(param_index, param_index + n_spheres);
+    h->mre.resize(n_param);
+    h->mim.resize(n_param);
+    h->radius.assign(radius, radius + n_param);
+    h->nr.assign(n_range, n_range + 2 * n_param);
+    h->p_param.resize(n_param);
+    for (int i = 0; i < n_param; ++i) {
+        h->mre[i] = refractive_index[2 * i] / h->prm.n_medium;
+        h->mim[i] = refractive_index[2 * i + 1] / h->prm.n_medium;
+        if (n_range[2 * i] != 1 || n_range[2 * i + 1] < 1)
+            return fail(h, FOGGY_ERR_ARGUMENT, "parameter n_range must be [1, n_max], n_max >= 1");
+        if (!(radius[i] > 0)) return fail(h, FOGGY_ERR_ARGUMENT, "radius must be > 0");
+        h->p_param[i] = std::min(n_range[2 * i + 1], pg);
+    }
+    h->p_s.resize(n_spheres);
+    h->couple.resize(n_spheres);
+    h->off.resize(n_spheres + 1);
+    h->pmax = 0;
+    int64_t o = 0;
+    for (int j = 0; j < n_spheres; ++j) {
+        int ip = param_index[j];
+        if (ip < 0 || ip >= n_param) return fail(h, FOGGY_ERR_ARGUMENT, "param_index out of range");
+        for (int d = 0; d < 3; ++d)
+            if (!std::isfinite(centres[3 * (size_t)j + d])) return fail(h, FOGGY_ERR_ARGUMENT, "non-finite centre");
+        int p = h->p_param[ip];
+        h->p_s[j] = p;
+        h->pmax = std::max(h->pmax, p);
+        // rows of spheres whose range does not cover the global one carry no coupling
+        // (lib_mie_ms_solver_interface.f90:965-978)
+        h->couple[j] = (h->prm.reference_row_rule && n_range[2 * ip + 1] < pg) ? 0 : 1;
+        h->off[j] = o;
+        o += 2 * (int64_t)p * (p + 2);
+    }
+    h->off[n_spheres] = o;
+    h->n_unk = o;
+    if (h->pmax > 32)
+        return fail(h, FOGGY_ERR_UNSUPPORTED, "the direct operator supports truncation orders up to 32");
+    TRY(ensure_tables(h, std::max(h->pmax, 1)));
+    // device scene
+    TRY(dalloc(h, &h->d_centres, 3 * (size_t)n_spheres));
+    TRY(dalloc(h, &h->d_p, n_spheres));
+    TRY(dalloc(h, &h->d_off, n_spheres + 1));
+    TRY(dalloc(h, &h->d_couple, n_spheres));
+    TRY(dalloc(h, &h->d_an, (size_t)n_spheres * h->pmax));
+    TRY(dalloc(h, &h->d_bn, (size_t)n_spheres * h->pmax));
+    TRY(dalloc(h, &h->d_an_p, (size_t)n_param * h->pmax));
+    TRY(dalloc(h, &h->d_bn_p, (size_t)n_param * h->pmax));
+    TRY(dalloc(h, &h->d_b, h->n_unk));
+    TRY(dalloc(h, &h->d_pq, h->n_unk));
+    TRY(dalloc(h, &h->d_tmp_in, h->n_unk));
+    TRY(dalloc(h, &h->d_tmp_out, h->n_unk));
+    h->chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, (4 * 148 + n_spheres - 1) / n_spheres));
+    h->chunks = std::min(h->chunks, std::max(1, n_spheres - 1));
+    TRY(dalloc(h, &h->d_partial, (size_t)h->chunks * h->n_unk));
+    CK(h, cudaMemcpy(h->d_centres, centres, 3 * (size_t)n_spheres * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_p, h->p_s.data(), n_spheres * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_off, h->off.data(), (n_spheres + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_couple, h->couple.data(), n_spheres * sizeof(int), cudaMemcpyHostToDevice));
+    // Mie coefficients per parameter (FP64, device) then gathered per sphere
+    std::vector<double> xs(n_param);
+    for (int i = 0; i < n_param; ++i) xs[i] = 2.0 * kPi * h->prm.n_medium * radius[i] / h->prm.lambda_0;
+    double *d_x = nullptr, *d_mr = nullptr, *d_mi = nullptr;
+    int* d_pp = nullptr;
+    int* d_pidx = nullptr;
+    CK(h, cudaMalloc(&d_x, n_param * sizeof(double)));
+    CK(h, cudaMalloc(&d_mr, n_param * sizeof(double)));
+    CK(h, cudaMalloc(&d_mi, n_param * sizeof(double)));
+    CK(h, cudaMalloc(&d_pp, n_param * sizeof(int)));
+    CK(h, cudaMalloc(&d_pidx, n_spheres * sizeof(int)));
+    CK(h, cudaMemcpy(d_x, xs.data(), n_param * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(d_mr, h->mre.data(), n_param * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(d_mi, h->mim.data(), n_param * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(d_pp, h->p_param.data(), n_param * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(d_pidx, param_index, n_spheres * sizeof(int), cudaMemcpyHostToDevice));
+    k_mie_ab<<<(n_param + 63) / 64, 64, 0, h->stream>>>(n_param, d_x, d_mr, d_mi, d_pp, h->pmax, h->d_an_p, h->d_bn_p);
+    k_gather_an<<<n_spheres, 64, 0, h->stream>>>(n_spheres, d_pidx, h->pmax, h->d_an_p, h->d_bn_p, h->d_an, h->d_bn);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_x);
+    cudaFree(d_mr);
+    cudaFree(d_mi);
+    cudaFree(d_pp);
+    cudaFree(d_pidx);
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("mie: ") + cudaGetErrorString(e));
+    CKL(h);
+    h->rhs_ready = false;
+    return FOGGY_OK;
+}
+
+int32_t foggy_set_plane_waves(foggy_handle h, int32_t nw, const double* theta, const double* phi,
+                              const double* jones, const double* g, const double* phase, const double* d_0_i) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (nw < 1 || !theta || !phi || !jones || !g) return fail(h, FOGGY_ERR_ARGUMENT, "empty or NULL wave input");
+    h->waves.clear();
+    double k = wavenumber(h->prm);
+    for (int i = 0; i < nw; ++i) {
+        WaveDev w{};
+        // the reference stores the direction as a cartesian vector and converts it back
+        // (lib_mie_illumination.f90:421-425, 330-333)
+        double rs = k * std::sin(theta[i]);
+        w.kc[0] = rs * std::cos(phi[i]);
+        w.kc[1] = rs * std::sin(phi[i]);
+        w.kc[2] = k * std::cos(theta[i]);
+        double rho;
+        to_spherical(w.kc, &rho, &w.alpha, &w.beta);
+        double ph = phase ? phase[i] : 0.0;
+        w.ax = std::hypot(jones[4 * i], jones[4 * i + 1]);
+        w.phx = std::atan2(jones[4 * i + 1], jones[4 * i]) + ph;
+        w.ay = std::hypot(jones[4 * i + 2], jones[4 * i + 3]);
+        w.phy = std::atan2(jones[4 * i + 3], jones[4 * i + 2]) + ph;
+        w.g = g[i];
+        for (int d = 0; d < 3; ++d) w.d0[d] = d_0_i ? d_0_i[3 * i + d] : 0.0;
+        h->waves.push_back(w);
+    }
+    h->rhs_ready = false;
+    return FOGGY_OK;
+}
+
+int64_t foggy_vector_length(foggy_handle h) {
+    if (!h || h->N == 0) return 0;
+    int C = (h->pg + 1) * (h->pg + 1) - 1;
+    return (int64_t)2 * C * h->N;
+}
+
+int32_t foggy_get_mie_coefficients(foggy_handle h, int32_t ip, double* a, double* b) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (ip < 0 || ip >= h->NP || !a || !b) return fail(h, FOGGY_ERR_ARGUMENT, "parameter index");
+    int p = h->p_param[ip];
+    CK(h, cudaMemcpy(a, h->d_an_p + (size_t)ip * h->pmax, p * sizeof(cplx), cudaMemcpyDeviceToHost));
+    CK(h, cudaMemcpy(b, h->d_bn_p + (size_t)ip * h->pmax, p * sizeof(cplx), cudaMemcpyDeviceToHost));
+    return FOGGY_OK;
+}
+
+static int stage_ref_buffers(foggy_handle h) {
+    size_t len = (size_t)foggy_vector_length(h);
+    if (!h->d_ref_a) TRY(dalloc(h, &h->d_ref_a, len));
+    if (!h->d_ref_b) TRY(dalloc(h, &h->d_ref_b, len));
+    return FOGGY_OK;
+}
+
+int32_t foggy_get_vector_b(foggy_handle h, double* b, int32_t mem) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!b) return fail(h, FOGGY_ERR_ARGUMENT, "b is NULL");
+    CK(h, cudaSetDevice(h->device));
+    TRY(ensure_rhs(h));
+    size_t len = (size_t)foggy_vector_length(h);
+    cplx* dst = reinterpret_cast<cplx*>(b);
+    if (mem == FOGGY_MEM_HOST) {
+        TRY(stage_ref_buffers(h));
+        dst = h->d_ref_b;
+    }
+    k_pack<<<h->N, 128, 0, h->stream>>>(scene_view(h), h->pg, h->d_g, h->d_b, nullptr, dst);
+    CKL(h);
+    if (mem == FOGGY_MEM_HOST)
+        CK(h, cudaMemcpyAsync(b, dst, len * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return FOGGY_OK;
+}
+
+int32_t foggy_matvec(foggy_handle h, const double* x, double* y, int32_t mem) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!x || !y) return fail(h, FOGGY_ERR_ARGUMENT, "x or y is NULL");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    CK(h, cudaSetDevice(h->device));
+    size_t len = (size_t)foggy_vector_length(h);
+    const cplx* xr = reinterpret_cast<const cplx*>(x);
+    cplx* yr = reinterpret_cast<cplx*>(y);
+    if (mem == FOGGY_MEM_HOST) {
+        TRY(stage_ref_buffers(h));
+        CK(h, cudaMemcpyAsync(h->d_ref_a, x, len * sizeof(cplx), cudaMemcpyHostToDevice, h->stream));
+        xr = h->d_ref_a;
+        yr = h->d_ref_b;
+    }
+    SceneView sv = scene_view(h);
+    k_unpack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, xr, h->d_tmp_in);
+    TRY(apply_operator(h, h->d_tmp_in, h->d_tmp_out));
+    k_pack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, h->d_tmp_out, xr, yr);
+    CKL(h);
+    if (mem == FOGGY_MEM_HOST)
+        CK(h, cudaMemcpyAsync(y, yr, len * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return FOGGY_OK;
+}
+
+int32_t foggy_solve(foggy_handle h, const double* x0, double* x, int32_t mem, foggy_stats* stats) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!x) return fail(h, FOGGY_ERR_ARGUMENT, "x is NULL");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    CK(h, cudaSetDevice(h->device));
+    foggy_stats st{};
+    h->launches = 0;
+    if (!h->ev0) {
+        cudaEventCreate(&h->ev0);
+        cudaEventCreate(&h->ev1);
+    }
+    CK(h, cudaEventRecord(h->ev0, h->stream));
+    TRY(ensure_rhs(h));
+    TRY(ensure_workspace(h, h->prm.gmres_restart));
+    size_t len = (size_t)foggy_vector_length(h);
+    SceneView sv = scene_view(h);
+    if (x0) {
+        const cplx* src = reinterpret_cast<const cplx*>(x0);
+        if (mem == FOGGY_MEM_HOST) {
+            TRY(stage_ref_buffers(h));
+            CK(h, cudaMemcpyAsync(h->d_ref_a, x0, len * sizeof(cplx), cudaMemcpyHostToDevice, h->stream));
+            src = h->d_ref_a;
+        }
+        k_unpack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, src, h->d_x);
+        h->launches += 1;
+    } else if (h->prm.use_initial_guess) {
+        // x0 = single-sphere solution a_n p, b_n q (lib_mie_single_sphere.f90:1312-1395)
+        CK(h, cudaMemcpyAsync(h->d_x, h->d_b, h->n_unk * sizeof(cplx), cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        CK(h, cudaMemsetAsync(h->d_x, 0, h->n_unk * sizeof(cplx), h->stream));
+    }
+    CKL(h);
+    int status = gmres(h, &st);
+    if (status == FOGGY_ERR_CUDA || status == FOGGY_ERR_UNSUPPORTED || status == FOGGY_ERR_NOMEM) return status;
+    cplx* dst = reinterpret_cast<cplx*>(x);
+    if (mem == FOGGY_MEM_HOST) {
+        TRY(stage_ref_buffers(h));
+        dst = h->d_ref_b;
+    }
+    k_pack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, h->d_x, nullptr, dst);
+    h->launches += 1;
+    CKL(h);
+    if (mem == FOGGY_MEM_HOST)
+        CK(h, cudaMemcpyAsync(x, dst, len * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaEventRecord(h->ev1, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    st.ms_total = ms;
+    st.kernel_launches = h->launches;
+    st.status = status;
+    h->last_berr = st.backward_error;
+    if (stats) *stats = st;
+    if (status != FOGGY_OK) {
+        const char* what = status == FOGGY_ERR_NOT_CONVERGED ? "GMRES did not reach the tolerance"
+                           : status == FOGGY_ERR_BREAKDOWN   ? "GMRES breakdown"
+                                                             : "NaN or Inf in the residual";
+        fail(h, status, what);
+    }
+    return status;
+}
+
+double foggy_get_backward_error(foggy_handle h) { return h ? h->last_berr : -1.0; }
+
+int32_t foggy_cross_sections(foggy_handle h, const double* x, int32_t mem, double* out) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!x || !out) return fail(h, FOGGY_ERR_ARGUMENT, "x or out is NULL");
+    CK(h, cudaSetDevice(h->device));
+    TRY(ensure_rhs(h));
+    size_t len = (size_t)foggy_vector_length(h);
+    const cplx* src = reinterpret_cast<const cplx*>(x);
+    if (mem == FOGGY_MEM_HOST) {
+        TRY(stage_ref_buffers(h));
+        CK(h, cudaMemcpyAsync(h->d_ref_a, x, len * sizeof(cplx), cudaMemcpyHostToDevice, h->stream));
+        src = h->d_ref_a;
+    }
+    SceneView sv = scene_view(h);
+    k_unpack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, src, h->d_tmp_in);
+    double* d_part = nullptr;
+    CK(h, cudaMalloc(&d_part, 2 * (size_t)h->N * sizeof(double)));
+    k_cross_sections<<<h->N, 256, 0, h->stream>>>(sv, h->d_tmp_in, h->d_pq, d_part);
+    std::vector<double> part(2 * (size_t)h->N);
+    cudaError_t e = cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_part);
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("cross sections: ") + cudaGetErrorString(e));
+    double se = 0, sa = 0;
+    for (int j = 0; j < h->N; ++j) {
+        se += part[2 * j];
+        sa += part[2 * j + 1];
+    }
+    double k = wavenumber(h->prm);
+    double f = 4.0 * kPi / (k * k);
+    out[1] = f * se;
+    out[2] = f * sa;
+    out[0] = out[1] - out[2];
+    return FOGGY_OK;
+}
+
+double foggy_wigner_3j(int32_t j1, int32_t j2, int32_t j3, int32_t m1, int32_t m2, int32_t m3) {
+    return wigner3j(j1, j2, j3, m1, m2, m3);
+}
+
+int32_t foggy_translation_coefficients(double x, double theta, double phi, const int32_t n_range[2],
+                                       const int32_t nu_range[2], int32_t z_selector, double* A, double* B) {
+    if (!n_range || !nu_range || !A || !B) return fail(nullptr, FOGGY_ERR_ARGUMENT, "NULL argument");
+    if (n_range[0] < 1 || nu_range[0] < 1 || n_range[1] < n_range[0] || nu_range[1] < nu_range[0] ||
+        n_range[1] > 32 || nu_range[1] > 32)
+        return fail(nullptr, FOGGY_ERR_ARGUMENT, "degree ranges must lie in [1, 32]");
+    if (z_selector < 1 || z_selector > 4) return fail(nullptr, FOGGY_ERR_ARGUMENT, "z_selector must be 1..4");
+    if (!(x > 0)) return fail(nullptr, FOGGY_ERR_ARGUMENT, "x must be > 0");
+    foggy_params p;
+    foggy_default_params(&p);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    foggy_handle h = nullptr;
+    int rc = foggy_create(&p, dev, &h);
+    if (rc) return rc;
+    int pn = n_range[1], pnu = nu_range[1];
+    int pmax = std::max(pn, pnu);
+    rc = ensure_tables(h, pmax);
+    if (rc) {
+        fail(nullptr, rc, h->err);
+        foggy_destroy(h);
+        return rc;
+    }
+    AxialView ax{h->tab_pmax, h->d_axoff, h->d_ga, h->d_gb};
+    int Pn = pn * (pn + 2), Pnu = pnu * (pnu + 2);
+    cplx *dA = nullptr, *dB = nullptr;
+    cudaMalloc(&dA, (size_t)Pn * Pnu * sizeof(cplx));
+    cudaMalloc(&dB, (size_t)Pn * Pnu * sizeof(cplx));
+    size_t smem = direct_smem_bytes(pmax);
+    cudaFuncSetAttribute(k_translation_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_translation_pair<<<1, 256, smem, h->stream>>>(ax, h->d_sqrt_binom, h->d_rs, h->K, x, theta, phi, pn, pnu,
+                                                    z_selector, dA, dB);
+    std::vector<cplx> hA((size_t)Pn * Pnu), hB((size_t)Pn * Pnu);
+    cudaError_t e = cudaMemcpyAsync(hA.data(), dA, hA.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hB.data(), dB, hB.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dA);
+    cudaFree(dB);
+    std::vector<double> g;
+    build_g_table(pmax, g);
+    foggy_destroy(h);
+    if (e != cudaSuccess) return fail(nullptr, FOGGY_ERR_CUDA, std::string("translation: ") + cudaGetErrorString(e));
+    // back to the reference basis and the requested ranges
+    int n1 = n_range[0], nu1 = nu_range[0];
+    int cnu = (nu_range[1] + 1) * (nu_range[1] + 1) - nu1 * nu1;
+    cplx* Ao = reinterpret_cast<cplx*>(A);
+    cplx* Bo = reinterpret_cast<cplx*>(B);
+    for (int n = n1; n <= pn; ++n)
+        for (int m = -n; m <= n; ++m)
+            for (int nu = nu1; nu <= pnu; ++nu)
+                for (int mu = -nu; mu <= nu; ++mu) {
+                    int r = n * n - 1 + n + m, c = nu * nu - 1 + nu + mu;
+                    double sc = g[n * (n + 1) + m] / g[nu * (nu + 1) + mu];
+                    size_t o = (size_t)(n * n - n1 * n1 + n + m) * cnu + (nu * nu - nu1 * nu1 + nu + mu);
+                    Ao[o] = sc * hA[(size_t)r * Pnu + c];
+                    Bo[o] = sc * hB[(size_t)r * Pnu + c];
+                }
+    return FOGGY_OK;
+}
+
+// ---- octree -------------------------------------------------------------------------------
+static int build_tree_dev(foggy_handle h) {
+    if (h->tree_ready) return FOGGY_OK;
+    int n = h->N;
+    if (!h->d_keys) {
+        TRY(dalloc(h, &h->d_keys, n));
+        TRY(dalloc(h, &h->d_idx, n));
+        TRY(dalloc(h, &h->d_keys_sorted, n));
+        TRY(dalloc(h, &h->d_idx_sorted, n));
+    }
+    double* d_mm = nullptr;
+    int* d_lmax = nullptr;
+    CK(h, cudaMalloc(&d_mm, 6 * sizeof(double)));
+    CK(h, cudaMalloc(&d_lmax, sizeof(int)));
+    k_minmax<<<1, 256, 0, h->stream>>>(n, h->d_centres, d_mm);
+    k_morton<<<(n + 255) / 256, 256, 0, h->stream>>>(n, h->d_centres, d_mm, h->d_keys, h->d_idx);
+    size_t tmp_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, h->d_keys, h->d_keys_sorted, h->d_idx, h->d_idx_sorted, n, 0,
+                                    63, h->stream);
+    void* d_tmp = nullptr;
+    CK(h, cudaMalloc(&d_tmp, tmp_bytes));
+    cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, h->d_keys, h->d_keys_sorted, h->d_idx, h->d_idx_sorted, n, 0,
+                                    63, h->stream);
+    int one = 1;
+    CK(h, cudaMemcpyAsync(d_lmax, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    int s = std::max(1, h->prm.tree_s_opt);
+    if (n > s) k_level_max<<<(n + 255) / 256, 256, 0, h->stream>>>(n, s, h->d_keys_sorted, d_lmax);
+    int lmax = 1;
+    cudaError_t e = cudaMemcpyAsync(&lmax, d_lmax, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_tmp);
+    cudaFree(d_mm);
+    cudaFree(d_lmax);
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("tree: ") + cudaGetErrorString(e));
+    CKL(h);
+    // l_min = 1 + floor(log(k + 1) / log(2)) for k = 1 (lib_tree.f90:1162-1170)
+    h->tree_lmin = (int)(1 + std::floor(std::log(2.0f) / std::log(2.0f)));
+    h->tree_lmax = h->prm.tree_l_max > 0 ? h->prm.tree_l_max : lmax;
+    h->tree_ready = true;
+    return FOGGY_OK;
+}
+
+int32_t foggy_build_tree(foggy_handle h, int64_t* uindex_out, int32_t* order_out, int32_t* l_min_out,
+                         int32_t* l_max_out) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    CK(h, cudaSetDevice(h->device));
+    h->tree_ready = false;
+    TRY(build_tree_dev(h));
+    int n = h->N;
+    if (uindex_out || order_out) {
+        std::vector<unsigned long long> ks(n);
+        std::vector<int> is(n);
+        CK(h, cudaMemcpy(ks.data(), h->d_keys_sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        CK(h, cudaMemcpy(is.data(), h->d_idx_sorted, n * sizeof(int), cudaMemcpyDeviceToHost));
+        int sh = 3 * (21 - h->tree_lmax);
+        for (int i = 0; i < n; ++i) {
+            if (order_out) order_out[i] = is[i];
+            if (uindex_out) uindex_out[is[i]] = (int64_t)(ks[i] >> sh);
+        }
+    }
+    if (l_min_out) *l_min_out = h->tree_lmin;
+    if (l_max_out) *l_max_out = h->tree_lmax;
+    return FOGGY_OK;
+}
+
+int32_t foggy_universal_index(int32_t n, const double* points, int32_t l, int64_t* out) {
+    if (n < 1 || !points || !out) return fail(nullptr, FOGGY_ERR_ARGUMENT, "empty or NULL input");
+    if (l < 1 || l > 21) return fail(nullptr, FOGGY_ERR_ARGUMENT, "level must be 1..21");
+    double* dp = nullptr;
+    long long* dout = nullptr;
+    cudaError_t e = cudaMalloc(&dp, 3 * (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&dout, (size_t)n * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMemcpy(dp, points, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_uindex_points<<<(n + 255) / 256, 256>>>(n, dp, l, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, (size_t)n * sizeof(long long), cudaMemcpyDeviceToHost);
+    cudaFree(dp);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(nullptr, FOGGY_ERR_CUDA, std::string("universal index: ") + cudaGetErrorString(e));
+    return FOGGY_OK;
+}
+
+int32_t foggy_tree_boxes(foggy_handle h, int32_t l, int64_t* boxes, int32_t* count) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!count) return fail(h, FOGGY_ERR_ARGUMENT, "count is NULL");
+    if (l < 0 || l > 21) return fail(h, FOGGY_ERR_ARGUMENT, "level must be 0..21");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    CK(h, cudaSetDevice(h->device));
+    TRY(build_tree_dev(h));
+    int n = h->N;
+    std::vector<unsigned long long> ks(n);
+    CK(h, cudaMemcpy(ks.data(), h->d_keys_sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    int sh = 3 * (21 - l);
+    std::vector<int64_t> u;
+    for (int i = 0; i < n; ++i) {
+        int64_t v = (int64_t)(ks[i] >> sh);
+        if (u.empty() || u.back() != v) u.push_back(v);
+    }
+    if (boxes) {
+        if (*count < (int)u.size()) return fail(h, FOGGY_ERR_ARGUMENT, "boxes buffer too small");
+        std::copy(u.begin(), u.end(), boxes);
+    }
+    *count = (int)u.size();
+    return FOGGY_OK;
+}
+
+}  // extern "C"

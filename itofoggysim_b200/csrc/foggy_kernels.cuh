@@ -1,0 +1,77 @@
+// Kernel declarations of libfoggy_b200 (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "foggy_internal.h"
+
+namespace foggy {
+
+// Plane wave on the device (lib_mie_illumination.f90:392-478): propagation direction after
+// the reference's cartesian round trip, Jones weights and phases, origin.
+struct WaveDev {
+    double kc[3];        // wave vector (cartesian)
+    double alpha, beta;  // its polar and azimuthal angle
+    double ax, phx;      // |J_x|, arg(J_x) + phase   (TM)
+    double ay, phy;      // |J_y|, arg(J_y) + phase   (TE)
+    double g;            // amplitude weight
+    double d0[3];        // origin of the wave's coordinate system
+};
+
+// k_scene.cu
+__global__ void k_mie_ab(int n_param, const double* size_param, const double* m_re, const double* m_im,
+                         const int* p_of_param, int pstride, cplx* an_out, cplx* bn_out);
+__global__ void k_gather_an(int n, const int* pidx, int pstride, const cplx* an_p, const cplx* bn_p,
+                            cplx* an_s, cplx* bn_s);
+__global__ void k_pitau(int nw, const WaveDev* waves, int pmax, double* pi_out, double* tau_out);
+__global__ void k_rhs(SceneView sc, int nw, const WaveDev* waves, int pmax, const double* pi_tab,
+                      const double* tau_tab, cplx* b, cplx* pq);
+__global__ void k_unpack(SceneView sc, int pg, const double* g, const cplx* xref, cplx* xdev);
+__global__ void k_pack(SceneView sc, int pg, const double* g, const cplx* ydev, const cplx* identity_ref,
+                       cplx* yref);
+__global__ void k_cross_sections(SceneView sc, const cplx* x, const cplx* pq, double* part);
+
+// k_direct.cu -- all-pairs sphere coupling (the direct operator)
+struct DirectArgs {
+    SceneView sc;
+    AxialView ax;
+    const double* sqrt_binom;  // d-table start values
+    const double* rs;          // sqrt(j^2 - m^2)
+    int K;                     // width of those tables (>= pmax)
+    int z;                     // radial function selector (1 j_n, 2 y_n, 3 h1, 4 h2)
+    const cplx* x;             // ragged scaled input
+    cplx* partial;             // [chunks][n_unk] partial sums
+    int chunks;
+    int64_t n_unk;
+};
+size_t direct_smem_bytes(int pmax);
+void launch_direct(const DirectArgs& a, cudaStream_t s);
+// y = x + T (sum of chunk partials) for coupled spheres, y = x otherwise
+__global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial, int chunks, int64_t n_unk,
+                                cplx* y);
+// single-pair translation for the parity entry point: A, B blocks in the scaled basis
+__global__ void k_translation_pair(AxialView ax, const double* sqrt_binom, const double* rs, int K, double x,
+                                   double theta, double phi, int pn, int pnu, int z, cplx* A, cplx* B);
+
+// k_gmres.cu -- Krylov kernels (deterministic fixed-order reductions)
+constexpr int kRedBlocks = 296;
+__global__ void k_dots_partial(const cplx* V, int64_t ld, int nv, const cplx* w, int64_t n, cplx* part);
+__global__ void k_dots_reduce(const cplx* part, int nv, cplx* out, int accumulate);
+__global__ void k_axpy_multi(const cplx* V, int64_t ld, int nv, const cplx* h, cplx* w, int64_t n);
+__global__ void k_norm_partial(const cplx* w, int64_t n, double* part);
+__global__ void k_norm_reduce(const double* part, double* out);
+__global__ void k_scale_copy(const cplx* w, const double* nrm, cplx* v, int64_t n);
+__global__ void k_sub(const cplx* b, const cplx* ax, cplx* r, int64_t n);
+__global__ void k_givens(cplx* H, int ldh, cplx* cs, double* sn, cplx* g, const cplx* h, const cplx* c,
+                         const double* hn, int k, double* res_est, int* flags);
+__global__ void k_trisolve(const cplx* H, int ldh, const cplx* g, int k, cplx* y);
+__global__ void k_update_x(cplx* x, const cplx* V, int64_t ld, const cplx* y, int k, int64_t n);
+__global__ void k_init_cycle(cplx* g, int m1, const double* beta, int* flags);
+
+// k_tree.cu -- octree keys (libtree)
+__global__ void k_minmax(int n, const double* c, double* out);
+__global__ void k_morton(int n, const double* c, const double* mm, unsigned long long* key, int* idx);
+__global__ void k_level_max(int n, int s, const unsigned long long* key, int* lmax);
+__global__ void k_uindex_points(int n, const double* pts, int l, long long* out);
+
+}  // namespace foggy

@@ -1,0 +1,278 @@
+// Scene-level kernels: Mie coefficients, plane-wave right-hand side, layout conversion between
+// the reference's flat coefficient vector and the device's ragged scaled layout, and the
+// cluster cross-sections.
+#include "foggy_kernels.cuh"
+#include "k_special.cuh"
+
+namespace foggy {
+
+// ---- Mie coefficients a_n, b_n (lib_mie_ss_helper_functions.f90:628-722; logarithmic
+// derivative by downward recurrence 751-924; start n_c from 937-951) -----------------------
+__global__ void k_mie_ab(int n_param, const double* size_param, const double* m_re, const double* m_im,
+                         const int* p_of_param, int pstride, cplx* an_out, cplx* bn_out) {
+    int ip = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ip >= n_param) return;
+    double x = size_param[ip];
+    cplx m = mk(m_re[ip], m_im[ip]);
+    int p = p_of_param[ip];
+    cplx mx = mk(m.x * x, m.y * x);
+    double amx = sqrt(mx.x * mx.x + mx.y * mx.y);
+    int n_c = (int)ceil(x + 4.05 * cbrt(x) + 2.0);
+    int n_mx = max(n_c, (int)amx) + 15;
+    cplx* an = an_out + (size_t)ip * pstride;
+    cplx* bn = bn_out + (size_t)ip * pstride;
+    // downward: A_{i-1} = i/(mx) - 1/(A_i + i/(mx)); keep A_n for n = 1..p in an[] temporarily
+    cplx A = mk(0, 0);
+    for (int i = n_mx; i >= 2; --i) {
+        cplx ndm = cdiv(mk((double)i, 0), mx);
+        A = ndm - cdiv(mk(1, 0), A + ndm);
+        if (i - 1 <= p) an[i - 2] = A;
+    }
+    double jb[kMaxDegree + 2], yb[kMaxDegree + 2];
+    dev_sph_jn(x, p, jb);
+    dev_sph_yn(x, p, yb);
+    for (int n = 1; n <= p; ++n) {
+        cplx An = an[n - 1];
+        double ndx = (double)n / x;
+        cplx jn = mk(jb[n], 0), jnm = mk(jb[n - 1], 0), hn = mk(jb[n], yb[n]), hnm = mk(jb[n - 1], yb[n - 1]);
+        cplx bufa = cdiv(An, m) + mk(ndx, 0);
+        cplx bufb = m * An + mk(ndx, 0);
+        an[n - 1] = cdiv(bufa * jn - jnm, bufa * hn - hnm);
+        bn[n - 1] = cdiv(bufb * jn - jnm, bufb * hn - hnm);
+    }
+}
+
+__global__ void k_gather_an(int n, const int* pidx, int pstride, const cplx* an_p, const cplx* bn_p,
+                            cplx* an_s, cplx* bn_s) {
+    int j = blockIdx.x;
+    int ip = pidx[j];
+    for (int t = threadIdx.x; t < pstride; t += blockDim.x) {
+        an_s[(size_t)j * pstride + t] = an_p[(size_t)ip * pstride + t];
+        bn_s[(size_t)j * pstride + t] = bn_p[(size_t)ip * pstride + t];
+    }
+}
+
+// ---- scaled pi_nm, tau_nm of each wave (lib_math_legendre.f90:834-982; values divided by
+// g_nm = (-1)^m sqrt((n+m)!/(n-m)!), which turns the recurrence into the stable normalised
+// one).  Table pt[w][n(n+1)+m] (pi) and tt[...] (tau).  One thread per m >= 0. -------------
+__global__ void k_pitau(int nw, const WaveDev* waves, int pmax, double* pi_out, double* tau_out) {
+    int w = blockIdx.x;
+    int m = threadIdx.x;
+    if (m > pmax) return;
+    double alpha = waves[w].alpha;
+    double x = cos(alpha), s = sin(alpha);
+    int S = (pmax + 1) * (pmax + 1);
+    double* pi = pi_out + (size_t)w * S;
+    double* tau = tau_out + (size_t)w * S;
+    double sgm = (m & 1) ? -1.0 : 1.0;
+    if (x == 1.0 || x == -1.0) {
+        // The reference's pole table (lib_math_legendre.f90:854-920), phase removed, then
+        // scaled by 1/g_{n,+-1} = -1/sqrt(n(n+1)), -sqrt(n(n+1)).  At x = -1 it sets
+        // tau_n^{+-1} = -pi_n^{+-1} for odd n, which flips the sign of tau_n^{-1} there
+        // relative to the limit of the general formula; kept as the reference has it.
+        for (int n = max(m, 1); n <= pmax; ++n) {
+            pi[n * (n + 1) + m] = 0.0;
+            tau[n * (n + 1) + m] = 0.0;
+            pi[n * (n + 1) - m] = 0.0;
+            tau[n * (n + 1) - m] = 0.0;
+        }
+        if (m == 1) {
+            for (int n = 1; n <= pmax; ++n) {
+                double h = (double)(n * (n + 1) / 2);
+                double pim = -0.5, pip = -h, taum = 0.5, taup = -h;   // with phase, x = +1
+                if (x == -1.0) {
+                    if (!(n & 1)) { pim = -pim; pip = -pip; }
+                    else { taum = -pim; taup = -pip; }
+                }
+                double r = sqrt((double)n * (n + 1));
+                // phase removed (odd |m|): negate; scaled by 1/g
+                pi[n * (n + 1) - 1] = -pim * (-r);
+                tau[n * (n + 1) - 1] = -taum * (-r);
+                pi[n * (n + 1) + 1] = -pip / (-r);
+                tau[n * (n + 1) + 1] = -taup / (-r);
+            }
+        }
+        if (m == 0) { pi[0] = 0.0; tau[0] = 0.0; }
+        return;
+    }
+    if (m == 0) {
+        // tau_n^0 = -P_n^1 (no phase) -> scaled: -sqrt(n(n+1)) * Phat_n^1
+        // Phat_n^1 by the normalised recurrence from Phat_1^1 = sqrt(1/2) s
+        double pm2 = 0.0, pm1 = 0.0;
+        for (int n = 1; n <= pmax; ++n) {
+            double pn;
+            if (n == 1) pn = sqrt(0.5) * s;
+            else if (n == 2) pn = sqrt(3.0) * x * pm1;
+            else pn = ((2.0 * n - 1.0) * x * pm1 - sqrt((n - 1.0) * (n - 1.0) - 1.0) * pm2) / sqrt((double)n * n - 1.0);
+            pm2 = pm1;
+            pm1 = pn;
+            pi[n * (n + 1)] = 0.0;
+            tau[n * (n + 1)] = -sqrt((double)n * (n + 1)) * pn;
+        }
+        pi[0] = 0.0;
+        tau[0] = 0.0;
+        return;
+    }
+    // Qhat_n^m = Phat_n^m / sin(alpha), Phat = sqrt((n-m)!/(n+m)!) P_n^m (no phase)
+    double qmm = 1.0;
+    for (int k = 1; k <= m; ++k) qmm *= sqrt((2.0 * k - 1.0) / (2.0 * k));
+    for (int k = 1; k < m; ++k) qmm *= s;
+    double qm2 = 0.0, qm1 = 0.0;   // Qhat_{n-2}, Qhat_{n-1}
+    for (int n = m; n <= pmax; ++n) {
+        double qn;
+        if (n == m) qn = qmm;
+        else if (n == m + 1) qn = sqrt(2.0 * m + 1.0) * x * qm1;
+        else qn = ((2.0 * n - 1.0) * x * qm1 - sqrt((n - 1.0 - m) * (n - 1.0 + m)) * qm2) / sqrt((double)(n - m) * (n + m));
+        double qprev = qm1;
+        qm2 = qm1;
+        qm1 = qn;
+        double pv = m * qn;                                           // pi-hat_n^m
+        double tv = n * x * qn - sqrt((double)(n + m) * (n - m)) * qprev;   // tau-hat_n^m
+        pi[n * (n + 1) + m] = sgm * pv;
+        tau[n * (n + 1) + m] = sgm * tv;
+        // negative orders: pi_{n,-m} = -(-1)^m pi_{n,m}, tau_{n,-m} = (-1)^m tau_{n,m} (scaled)
+        pi[n * (n + 1) - m] = -sgm * sgm * pv;
+        tau[n * (n + 1) - m] = sgm * sgm * tv;
+    }
+}
+
+// ---- right-hand side b = [a_n p ; b_n q] (lib_mie_ms_solver_interface.f90:230-315) with the
+// plane-wave coefficients of lib_mie_illumination.f90:392-478 (several waves, Jones vector,
+// TE swaps p and q) and :636-763 (p = tau e^{-i m beta}/(n(n+1)) e^{i(k.d + phase)}).
+// One block per sphere; pq keeps the incident coefficients for the cross-sections. --------
+__global__ void k_rhs(SceneView sc, int nw, const WaveDev* waves, int pmax, const double* pi_tab,
+                      const double* tau_tab, cplx* b, cplx* pq) {
+    int j = blockIdx.x;
+    int pj = sc.p[j];
+    int Pj = pj * (pj + 2);
+    int64_t o = sc.off[j];
+    int S = (pmax + 1) * (pmax + 1);
+    const double* cj = sc.centres + 3 * (size_t)j;
+    for (int t = threadIdx.x; t < Pj; t += blockDim.x) {
+        int n = (int)sqrt((double)(t + 1));
+        if ((n + 1) * (n + 1) <= t + 1) ++n;
+        if (n * n > t + 1) --n;
+        int m = t + 1 - n * n - n;
+        cplx pv = mk(0, 0), qv = mk(0, 0);
+        double rn = 1.0 / (double)(n * (n + 1));
+        for (int w = 0; w < nw; ++w) {
+            const WaveDev& W = waves[w];
+            double d0 = cj[0] - W.d0[0], d1 = cj[1] - W.d0[1], d2 = cj[2] - W.d0[2];
+            double dn = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+            double kd = W.kc[0] * d0 + W.kc[1] * d1 + W.kc[2] * d2;
+            double pi_s = pi_tab[(size_t)w * S + n * (n + 1) + m];
+            double tau_s = tau_tab[(size_t)w * S + n * (n + 1) + m];
+            if (W.alpha == 0.0 && m != 1 && m != -1) { pi_s = 0.0; tau_s = 0.0; }
+            double sb, cbv;
+            sincos(-m * W.beta, &sb, &cbv);
+            cplx base = mk(rn * cbv, rn * sb);
+            cplx tp = mk(0, 0), tq = mk(0, 0);
+            if (W.ax > 0) {
+                cplx e = mk(1, 0);
+                if (dn > 0.0 || W.phx != 0.0) { double ss, cc; sincos(kd + W.phx, &ss, &cc); e = mk(cc, ss); }
+                tp = tp + W.ax * (e * (tau_s * base));
+                tq = tq + W.ax * (e * (pi_s * base));
+            }
+            if (W.ay > 0) {
+                cplx e = mk(1, 0);
+                if (dn > 0.0 || W.phy != 0.0) { double ss, cc; sincos(kd + W.phy, &ss, &cc); e = mk(cc, ss); }
+                tp = tp + W.ay * (e * (pi_s * base));    // TE: p and q swap
+                tq = tq + W.ay * (e * (tau_s * base));
+            }
+            pv = pv + W.g * tp;
+            qv = qv + W.g * tq;
+        }
+        pq[o + t] = pv;
+        pq[o + Pj + t] = qv;
+        b[o + t] = sc.an[(size_t)j * sc.pmax + n - 1] * pv;
+        b[o + Pj + t] = sc.bn[(size_t)j * sc.pmax + n - 1] * qv;
+    }
+}
+
+// ---- layout conversion ---------------------------------------------------------------------
+// reference flat layout (per sphere 2C entries, C = (pg+1)^2 - 1) <-> ragged scaled layout
+__global__ void k_unpack(SceneView sc, int pg, const double* g, const cplx* xref, cplx* xdev) {
+    int j = blockIdx.x;
+    int pj = sc.p[j];
+    int Pj = pj * (pj + 2);
+    int C = (pg + 1) * (pg + 1) - 1;
+    int64_t o = sc.off[j];
+    for (int t = threadIdx.x; t < Pj; t += blockDim.x) {
+        int n = (int)sqrt((double)(t + 1));
+        if ((n + 1) * (n + 1) <= t + 1) ++n;
+        if (n * n > t + 1) --n;
+        int m = t + 1 - n * n - n;
+        double rg = 1.0 / g[n * (n + 1) + m];
+        xdev[o + t] = rg * xref[(size_t)2 * C * j + t];
+        xdev[o + Pj + t] = rg * xref[(size_t)2 * C * j + C + t];
+    }
+}
+
+// identity_ref != nullptr: entries above the sphere's own degree are copied from it (the
+// identity rows of the reference operator); otherwise they are set to zero.
+__global__ void k_pack(SceneView sc, int pg, const double* g, const cplx* ydev, const cplx* identity_ref,
+                       cplx* yref) {
+    int j = blockIdx.x;
+    int pj = sc.p[j];
+    int Pj = pj * (pj + 2);
+    int C = (pg + 1) * (pg + 1) - 1;
+    int64_t o = sc.off[j];
+    for (int t = threadIdx.x; t < C; t += blockDim.x) {
+        size_t ra = (size_t)2 * C * j + t, rb = ra + C;
+        if (t < Pj) {
+            int n = (int)sqrt((double)(t + 1));
+            if ((n + 1) * (n + 1) <= t + 1) ++n;
+            if (n * n > t + 1) --n;
+            int m = t + 1 - n * n - n;
+            double gv = g[n * (n + 1) + m];
+            yref[ra] = gv * ydev[o + t];
+            yref[rb] = gv * ydev[o + Pj + t];
+        } else if (identity_ref) {
+            yref[ra] = identity_ref[ra];
+            yref[rb] = identity_ref[rb];
+        } else {
+            yref[ra] = mk(0, 0);
+            yref[rb] = mk(0, 0);
+        }
+    }
+}
+
+// ---- cluster cross-sections, per sphere partial sums {ext, abs} ----------------------------
+// In the scaled basis the reference weights n(n+1)(2n+1)(n-m)!/(n+m)! reduce to n(n+1)(2n+1).
+__global__ void k_cross_sections(SceneView sc, const cplx* x, const cplx* pq, double* part) {
+    int j = blockIdx.x;
+    int pj = sc.p[j];
+    int Pj = pj * (pj + 2);
+    int64_t o = sc.off[j];
+    double se = 0.0, sa = 0.0;
+    for (int t = threadIdx.x; t < Pj; t += blockDim.x) {
+        int n = (int)sqrt((double)(t + 1));
+        if ((n + 1) * (n + 1) <= t + 1) ++n;
+        if (n * n > t + 1) --n;
+        double E = (double)(n * (n + 1) * (2 * n + 1));
+        cplx a = x[o + t], bb = x[o + Pj + t];
+        cplx p = pq[o + t], q = pq[o + Pj + t];
+        cplx an = sc.an[(size_t)j * sc.pmax + n - 1], bn = sc.bn[(size_t)j * sc.pmax + n - 1];
+        double ra = (an.x != 0.0 || an.y != 0.0) ? cdiv(mk(1, 0), an).x - 1.0 : 0.0;
+        double rb = (bn.x != 0.0 || bn.y != 0.0) ? cdiv(mk(1, 0), bn).x - 1.0 : 0.0;
+        se += E * ((conjg(p) * a).x + (conjg(q) * bb).x);
+        sa += E * ((a.x * a.x + a.y * a.y) * ra + (bb.x * bb.x + bb.y * bb.y) * rb);
+    }
+    __shared__ double red[2][256];
+    red[0][threadIdx.x] = se;
+    red[1][threadIdx.x] = sa;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * j] = red[0][0];
+        part[2 * j + 1] = red[1][0];
+    }
+}
+
+}  // namespace foggy

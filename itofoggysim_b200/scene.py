@@ -1,0 +1,168 @@
+"""Seeded synthetic scenes of the multi-sphere solve.
+
+A Scene carries exactly the data the reference keeps in its module-global simulation_data
+(FoggySim/src/lib/mie_theory/lib_mie_type.f90:43-99): the sphere list (centres, parameter index),
+the shared sphere parameters (refractive index, radius, degree range), the global degree range,
+the z-selector of the coupling and the plane waves; plus the GMRES settings.
+
+Workloads (all lengths in micrometres, n_medium = 1, m = 1.33 + 1e-8 i, lambda = 0.55):
+  small_cluster   64 spheres r = 0.5 in a 10 um cube, p = 15, GMRES(30) to 1e-8, 3 tree levels
+  medium_cluster  2000 spheres, lognormal r (median 0.6, sigma_ln 0.3, clipped to 0.2..1.5) in a
+                  40 um cube, per-sphere p by the Wiscombe rule, GMRES(50) to 1e-8, 5 levels
+Centres are uniform in the cube with rejection of overlapping spheres.
+"""
+import dataclasses
+import math
+
+import numpy as np
+
+M_WATER = complex(1.33, 1e-8)
+
+
+def wiscombe_n_max(x):
+    """n_max = ceil(x + 4 x^(1/3) + 2) (Wiscombe; the reference rounds up the same way,
+    lib_mie_ss_helper_functions.f90:937-951, with 4.05 in place of 4)."""
+    return int(math.ceil(x + 4.0 * x ** (1.0 / 3.0) + 2.0))
+
+
+@dataclasses.dataclass
+class Scene:
+    lambda_0: float
+    n_medium: float
+    centres: np.ndarray          # (N, 3)
+    param_index: np.ndarray      # (N,) int32, 0-based
+    refractive_index: np.ndarray  # (NP,) complex
+    radius: np.ndarray           # (NP,)
+    n_range_param: np.ndarray    # (NP, 2) int32
+    n_range: tuple               # global (1, n_max)
+    wave_theta: np.ndarray
+    wave_phi: np.ndarray
+    jones: np.ndarray            # (nw, 4): re x, im x, re y, im y
+    wave_g: np.ndarray
+    wave_phase: np.ndarray
+    wave_d0: np.ndarray          # (nw, 3)
+    z_coupling: int = 3
+    reference_row_rule: bool = False
+    gmres_restart: int = 30
+    gmres_tolerance: float = 1e-8
+    gmres_max_iterations: int = 1000
+    tree_l_max: int = 0
+    name: str = "scene"
+
+    @property
+    def n_spheres(self):
+        return int(self.centres.shape[0])
+
+    @property
+    def n_param(self):
+        return int(self.radius.shape[0])
+
+    @property
+    def n_waves(self):
+        return int(self.wave_theta.shape[0])
+
+    @property
+    def wavenumber(self):
+        return 2.0 * math.pi * self.n_medium / self.lambda_0
+
+    def p_of_sphere(self):
+        p = np.minimum(self.n_range_param[:, 1], self.n_range[1])
+        return p[self.param_index]
+
+    def ragged_unknowns(self):
+        p = self.p_of_sphere().astype(np.int64)
+        return int(np.sum(2 * p * (p + 2)))
+
+    def vector_length(self):
+        c = (self.n_range[1] + 1) ** 2 - 1
+        return 2 * c * self.n_spheres
+
+
+def place_spheres(rng, radii, box):
+    """Uniform centres in [0, box)^3, rejecting overlaps |c_i - c_j| < r_i + r_j."""
+    n = len(radii)
+    cell = 2.0 * float(np.max(radii))
+    grid = {}
+    centres = np.zeros((n, 3))
+    for i in range(n):
+        for _ in range(100000):
+            c = rng.uniform(0.0, box, 3)
+            key = tuple((c // cell).astype(int))
+            ok = True
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        for j in grid.get((key[0] + dx, key[1] + dy, key[2] + dz), ()):
+                            if np.sum((centres[j] - c) ** 2) < (radii[i] + radii[j]) ** 2:
+                                ok = False
+                                break
+                        if not ok:
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                centres[i] = c
+                grid.setdefault(key, []).append(i)
+                break
+        else:
+            raise RuntimeError("could not place sphere %d" % i)
+    return centres
+
+
+def single_wave(theta=0.0, phi=0.0, jones=(1.0, 0.0, 0.0, 0.0)):
+    """One plane wave; Jones (1, 0) along +z is the reference's x-polarised TM wave
+    (lib_mie_type_functions.f90:156-158)."""
+    return dict(wave_theta=np.array([theta]), wave_phi=np.array([phi]),
+                jones=np.array([list(jones)], dtype=np.float64), wave_g=np.array([1.0]),
+                wave_phase=np.array([0.0]), wave_d0=np.zeros((1, 3)))
+
+
+def make_scene(radii, box, seed, lambda_0=0.55, n_medium=1.0, m=M_WATER, n_max=None, **kw):
+    rng = np.random.default_rng(seed)
+    radii = np.asarray(radii, dtype=np.float64)
+    centres = place_spheres(rng, radii, box)
+    k = 2.0 * math.pi * n_medium / lambda_0
+    uniq, inv = np.unique(radii, return_inverse=True)
+    p = np.array([wiscombe_n_max(k * r) if n_max is None else n_max for r in uniq], dtype=np.int32)
+    nrp = np.stack([np.ones_like(p), p], axis=1).astype(np.int32)
+    waves = kw.pop("waves", single_wave())
+    return Scene(lambda_0=lambda_0, n_medium=n_medium, centres=centres,
+                 param_index=inv.astype(np.int32), refractive_index=np.full(len(uniq), m, np.complex128),
+                 radius=uniq, n_range_param=nrp, n_range=(1, int(p.max())), **waves, **kw)
+
+
+def small_cluster(seed=1, z_coupling=3):
+    """64 monodisperse water spheres, r = 0.5 um, 10 um cube, p = 15, GMRES(30) to 1e-8."""
+    return make_scene(np.full(64, 0.5), 10.0, seed, z_coupling=z_coupling, reference_row_rule=True,
+                      gmres_restart=30, gmres_tolerance=1e-8, tree_l_max=3, name="small_cluster_64")
+
+
+def lognormal_radii(rng, n, median=0.6, sigma=0.3, lo=0.2, hi=1.5):
+    return np.clip(median * np.exp(sigma * rng.standard_normal(n)), lo, hi)
+
+
+def medium_cluster(seed=2, n=2000, box=40.0, z_coupling=3):
+    """2000 lognormal water spheres in a 40 um cube, per-sphere Wiscombe p, GMRES(50) to 1e-8."""
+    rng = np.random.default_rng(1000 + seed)
+    radii = lognormal_radii(rng, n)
+    return make_scene(radii, box, seed, z_coupling=z_coupling, reference_row_rule=False,
+                      gmres_restart=50, gmres_tolerance=1e-8, tree_l_max=5,
+                      name="medium_cluster_%d" % n)
+
+
+def random_cluster(n, seed, p=None, box=None, radii=None, z_coupling=3, reference_row_rule=None,
+                   waves=None, m=M_WATER):
+    """Small polydisperse clusters for parity tests."""
+    rng = np.random.default_rng(500 + seed)
+    if radii is None:
+        radii = rng.uniform(0.15, 0.45, n)
+    if box is None:
+        box = max(2.0, (n * 60.0) ** (1.0 / 3.0))
+    kw = {}
+    if waves is not None:
+        kw["waves"] = waves
+    sc = make_scene(radii, box, seed, n_max=p, m=m, z_coupling=z_coupling,
+                    reference_row_rule=bool(reference_row_rule), **kw)
+    return sc

@@ -1,0 +1,218 @@
+"""Host-side mirror of the reference's multi-sphere solver interface.
+
+The reference drives the solve through module-global Fortran state and these routines:
+  lib_mie_ms_constructor                           FoggySim/src/lib/mie_theory/lib_mie_multi_sphere.f90:111-150
+  lib_mie_ms_calculate_scattering_coefficients_ab_nm                             :162-371
+  lib_mie_ms_solver_run / _use_ml_fmm / _set_n_range / _set_max_iterations /
+  _get_backward_error                       lib_mie_ms_solver_interface.f90:143-209
+  lib_mie_ms_solver_calculate_vector_b (the matvec)                              :739-783
+  lib_mie_ms_solver_get_vector_b_all (the right-hand side)                       :230-315
+  lib_math_vector_spherical_harmonics_translation_coefficient
+                                   libmath/src/math/lib_math_vector_spherical_harmonics.f90:48-52
+  lib_math_wigner_3j                                    libmath/src/math/lib_math_wigner.f90:45-72
+  lib_tree_constructor / lib_tree_hf_get_universal_index            libtree/src/lib/lib_tree.f90:147-270
+Here one MultiSphereSolver object holds that state and calls the C ABI of libfoggy_b200.so; all
+arithmetic runs on the GPU.  Vectors use the reference's flat layout (complex128, per sphere
+[a_nm | b_nm], n = 1..n_max, m = -n..n).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+def _params(scene, use_ml_fmm=False, init_with_single_sphere=False, memory_budget=0):
+    L = N.load()
+    p = N.FoggyParams()
+    L.foggy_default_params(C.byref(p))
+    p.lambda_0 = scene.lambda_0
+    p.n_medium = scene.n_medium
+    p.n_range[0] = int(scene.n_range[0])
+    p.n_range[1] = int(scene.n_range[1])
+    p.z_coupling = int(scene.z_coupling)
+    p.reference_row_rule = int(bool(scene.reference_row_rule))
+    p.matvec_mode = N.FOGGY_MATVEC_MLFMM if use_ml_fmm else N.FOGGY_MATVEC_DIRECT
+    p.use_initial_guess = int(bool(init_with_single_sphere))
+    p.gmres_restart = int(scene.gmres_restart)
+    p.gmres_max_iterations = int(scene.gmres_max_iterations)
+    p.gmres_tolerance = float(scene.gmres_tolerance)
+    p.tree_l_max = int(scene.tree_l_max)
+    p.device_memory_budget = int(memory_budget)
+    return p
+
+
+class MultiSphereSolver:
+    """lib_mie_ms_constructor + the solver interface, on one GPU."""
+
+    def __init__(self, scene, use_ml_fmm=False, init_with_single_sphere=False, device=0, memory_budget=0):
+        self.L = N.load()
+        self.scene = scene
+        self.params = _params(scene, use_ml_fmm, init_with_single_sphere, memory_budget)
+        h = C.c_void_p()
+        N.check(self.L.foggy_create(C.byref(self.params), int(device), C.byref(h)))
+        self.h = h
+        s = scene
+        self._keep = [N.as_f64(s.centres).reshape(-1), N.as_i32(s.param_index),
+                      N.as_c128(s.refractive_index), N.as_f64(s.radius),
+                      N.as_i32(s.n_range_param).reshape(-1)]
+        c, pi, m, r, nr = self._keep
+        N.check(self.L.foggy_set_spheres(self.h, s.n_spheres, N.ptr(c), N.ptr(pi, C.c_int32), s.n_param,
+                                         N.ptr(m), N.ptr(r), N.ptr(nr, C.c_int32)), self.h)
+        w = [N.as_f64(s.wave_theta), N.as_f64(s.wave_phi), N.as_f64(s.jones).reshape(-1),
+             N.as_f64(s.wave_g), N.as_f64(s.wave_phase), N.as_f64(s.wave_d0).reshape(-1)]
+        N.check(self.L.foggy_set_plane_waves(self.h, s.n_waves, *[N.ptr(a) for a in w]), self.h)
+        self.n = int(self.L.foggy_vector_length(self.h))
+        self.last_stats = None
+
+    # ---- lifecycle --------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.foggy_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _set(self):
+        N.check(self.L.foggy_set_params(self.h, C.byref(self.params)), self.h)
+
+    # ---- lib_mie_ms_solver_* setters ------------------------------------------------------
+    def use_ml_fmm(self, flag):
+        self.params.matvec_mode = N.FOGGY_MATVEC_MLFMM if flag else N.FOGGY_MATVEC_DIRECT
+        self._set()
+
+    def set_max_iterations(self, it):
+        self.params.gmres_max_iterations = int(it)
+        self._set()
+
+    def set_tolerance(self, tol):
+        self.params.gmres_tolerance = float(tol)
+        self._set()
+
+    def set_restart(self, m):
+        self.params.gmres_restart = int(m)
+        self._set()
+
+    def get_backward_error(self):
+        return float(self.L.foggy_get_backward_error(self.h))
+
+    # ---- building blocks ----------------------------------------------------------------
+    def mie_coefficients(self, ip):
+        p = int(min(self.scene.n_range_param[ip][1], self.scene.n_range[1]))
+        a = np.zeros(p, np.complex128)
+        b = np.zeros(p, np.complex128)
+        N.check(self.L.foggy_get_mie_coefficients(self.h, int(ip), N.ptr(a), N.ptr(b)), self.h)
+        return a, b
+
+    def get_vector_b(self):
+        b = np.zeros(self.n, np.complex128)
+        N.check(self.L.foggy_get_vector_b(self.h, b.ctypes.data, N.FOGGY_MEM_HOST), self.h)
+        return b
+
+    def calculate_vector_b(self, x):
+        """The operator y = A x (lib_mie_ms_solver_calculate_vector_b)."""
+        x = N.as_c128(x)
+        if x.size != self.n:
+            raise ValueError("x has %d entries, expected %d" % (x.size, self.n))
+        y = np.zeros(self.n, np.complex128)
+        N.check(self.L.foggy_matvec(self.h, x.ctypes.data, y.ctypes.data, N.FOGGY_MEM_HOST), self.h)
+        return y
+
+    def matvec_device(self, x_ptr, y_ptr):
+        """Operator on device buffers (reference layout) given as raw CUDA pointers."""
+        N.check(self.L.foggy_matvec(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), N.FOGGY_MEM_DEVICE), self.h)
+
+    # ---- the solve ------------------------------------------------------------------------
+    def solve(self, x0=None, raise_on_error=True):
+        """lib_mie_ms_solver_run: GMRES on the device; returns (x, stats)."""
+        x = np.zeros(self.n, np.complex128)
+        st = N.FoggyStats()
+        x0p = None
+        if x0 is not None:
+            x0 = N.as_c128(x0)
+            x0p = x0.ctypes.data
+        rc = self.L.foggy_solve(self.h, x0p, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st))
+        self.last_stats = st.as_dict()
+        if raise_on_error:
+            N.check(rc, self.h)
+        return x, self.last_stats
+
+    def solve_device(self, x_ptr, x0_ptr=None):
+        st = N.FoggyStats()
+        rc = self.L.foggy_solve(self.h, C.c_void_p(x0_ptr) if x0_ptr else None, C.c_void_p(x_ptr),
+                                N.FOGGY_MEM_DEVICE, C.byref(st))
+        self.last_stats = st.as_dict()
+        N.check(rc, self.h)
+        return self.last_stats
+
+    def calculate_scattering_coefficients_ab_nm(self):
+        """lib_mie_ms_calculate_scattering_coefficients_ab_nm: solve and split the solution into
+        per-sphere a_nm, b_nm arrays (n = 1..n_max, m = -n..n flattened)."""
+        x, st = self.solve()
+        return self.split(x), st
+
+    def split(self, x):
+        c = (self.scene.n_range[1] + 1) ** 2 - 1
+        x = np.asarray(x).reshape(self.scene.n_spheres, 2, c)
+        return x[:, 0, :], x[:, 1, :]
+
+    def cross_sections(self, x):
+        """{C_sca, C_ext, C_abs} of the whole cluster for coefficient vector x."""
+        x = N.as_c128(x)
+        out = np.zeros(3)
+        N.check(self.L.foggy_cross_sections(self.h, x.ctypes.data, N.FOGGY_MEM_HOST, N.ptr(out)), self.h)
+        return out
+
+    # ---- libtree -----------------------------------------------------------------------
+    def build_tree(self):
+        n = self.scene.n_spheres
+        u = np.zeros(n, np.int64)
+        order = np.zeros(n, np.int32)
+        lmin = C.c_int32()
+        lmax = C.c_int32()
+        N.check(self.L.foggy_build_tree(self.h, N.ptr(u, C.c_int64), N.ptr(order, C.c_int32), C.byref(lmin),
+                                        C.byref(lmax)), self.h)
+        return u, order, lmin.value, lmax.value
+
+    def tree_boxes(self, level):
+        cnt = C.c_int32(0)
+        N.check(self.L.foggy_tree_boxes(self.h, int(level), None, C.byref(cnt)), self.h)
+        out = np.zeros(cnt.value, np.int64)
+        N.check(self.L.foggy_tree_boxes(self.h, int(level), N.ptr(out, C.c_int64), C.byref(cnt)), self.h)
+        return out
+
+
+# ---- libmath / libtree free functions ---------------------------------------------------------
+def translation_coefficient(x, theta, phi, n_range, nu_range, z_selector):
+    """A_mn^{mu nu}, B_mn^{mu nu} (reference layout, rows (n, m), columns (nu, mu))."""
+    L = N.load()
+    cn = (n_range[1] + 1) ** 2 - n_range[0] ** 2
+    cnu = (nu_range[1] + 1) ** 2 - nu_range[0] ** 2
+    A = np.zeros((cn, cnu), np.complex128)
+    B = np.zeros((cn, cnu), np.complex128)
+    nr = (C.c_int32 * 2)(*n_range)
+    nur = (C.c_int32 * 2)(*nu_range)
+    N.check(L.foggy_translation_coefficients(float(x), float(theta), float(phi), nr, nur, int(z_selector),
+                                             N.ptr(A), N.ptr(B)))
+    return A, B
+
+
+def wigner_3j(j1, j2, j3, m1, m2, m3):
+    return float(N.load().foggy_wigner_3j(j1, j2, j3, m1, m2, m3))
+
+
+def universal_index(points, level):
+    pts = N.as_f64(points).reshape(-1)
+    out = np.zeros(len(pts) // 3, np.int64)
+    N.check(N.load().foggy_universal_index(len(out), N.ptr(pts), int(level), N.ptr(out, C.c_int64)))
+    return out

@@ -1,0 +1,260 @@
+"""ctypes wrapper of the FP64 CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py import this module.
+It loads oracle/liboracle.so, which restates the reference algorithms (see oracle.cpp) and
+links the reference's own wigxjpf library built into oracle/_ref/.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+
+
+def build():
+    """Compile liboracle.so (and, where the reference checkout exists, _ref/libwigxjpf.a)."""
+    ref = os.environ.get("FOGGY_REFERENCE", "/root/reference")
+    args = ["make", "-s", "-C", HERE]
+    if os.path.isdir(ref):
+        args.append("REF=" + ref)
+    subprocess.run(args, check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = os.path.join(HERE, "liboracle.so")
+    if not os.path.exists(path):
+        build()
+    L = C.CDLL(path)
+    L.orc_init.argtypes = [C.c_int]
+    L.orc_sph_jn.argtypes = [C.c_double, C.c_int, dp]
+    L.orc_sph_yn.argtypes = [C.c_double, C.c_int, dp]
+    L.orc_legendre_table.argtypes = [C.c_double, C.c_int, dp]
+    L.orc_pi_tau.argtypes = [C.c_double, C.c_int, C.c_int, dp, dp]
+    L.orc_wigner_3j.argtypes = [C.c_int] * 6
+    L.orc_wigner_3j.restype = C.c_double
+    L.orc_ab_xu_cruzan.argtypes = [C.c_int] * 5 + [dp]
+    L.orc_n_c.argtypes = [C.c_double]
+    L.orc_mie_ab.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, dp, dp]
+    L.orc_translation_xu.argtypes = [C.c_double] * 3 + [C.c_int] * 5 + [dp, dp]
+    L.orc_universal_index.argtypes = [dp, C.c_int]
+    L.orc_universal_index.restype = C.c_int64
+    L.orc_coordinate_binary.argtypes = [C.c_double]
+    L.orc_coordinate_binary.restype = C.c_uint64
+    L.orc_scale_points.argtypes = [C.c_int, dp, dp]
+    L.orc_build_tree.argtypes = [C.c_int, dp, C.c_int, C.c_int, lp, ip,
+                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.orc_problem_create.restype = C.c_void_p
+    L.orc_problem_create.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     C.c_int, dp, ip, C.c_int, dp, dp, ip, C.c_int,
+                                     dp, dp, dp, dp, dp, dp]
+    L.orc_problem_destroy.argtypes = [C.c_void_p]
+    L.orc_vector_length.argtypes = [C.c_void_p]
+    L.orc_vector_length.restype = C.c_int64
+    L.orc_mie_of_param.argtypes = [C.c_void_p, C.c_int, dp, dp]
+    L.orc_vector_b.argtypes = [C.c_void_p, dp, dp]
+    L.orc_matvec.argtypes = [C.c_void_p, dp, dp]
+    L.orc_solve.argtypes = [C.c_void_p, dp, dp, C.c_int, C.c_double, C.c_int, C.c_void_p,
+                            ip, C.POINTER(C.c_double)]
+    L.orc_cross_sections.argtypes = [C.c_void_p, dp, dp]
+    L.orc_init(64)
+    _LIB = L
+    return L
+
+
+def _c(a):
+    """complex128 array -> interleaved float64 view."""
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    return a.view(np.float64)
+
+
+def sph_jn(x, nmax):
+    out = np.zeros(nmax + 1)
+    lib().orc_sph_jn(x, nmax, out)
+    return out
+
+
+def sph_yn(x, nmax):
+    out = np.zeros(nmax + 1)
+    lib().orc_sph_yn(x, nmax, out)
+    return out
+
+
+def legendre_table(x, nmax):
+    out = np.zeros((nmax + 1) ** 2)
+    lib().orc_legendre_table(x, nmax, out)
+    return out
+
+
+def pi_tau(theta, nmax, cs_phase=False):
+    pi = np.zeros((nmax + 1) ** 2)
+    tau = np.zeros((nmax + 1) ** 2)
+    lib().orc_pi_tau(theta, nmax, int(cs_phase), pi, tau)
+    return pi, tau
+
+
+def wigner_3j(j1, j2, j3, m1, m2, m3):
+    return lib().orc_wigner_3j(j1, j2, j3, m1, m2, m3)
+
+
+def ab_xu_cruzan(m, n, mu, nu, p):
+    out = np.zeros(2)
+    lib().orc_ab_xu_cruzan(m, n, mu, nu, p, out)
+    return out[0], out[1]
+
+
+def n_c(x):
+    return lib().orc_n_c(x)
+
+
+def mie_ab(x, m, n1, n2):
+    a = np.zeros(2 * (n2 - n1 + 1))
+    b = np.zeros(2 * (n2 - n1 + 1))
+    lib().orc_mie_ab(x, complex(m).real, complex(m).imag, n1, n2, a, b)
+    return a.view(np.complex128), b.view(np.complex128)
+
+
+def translation_xu(x, theta, phi, n_range, nu_range, z):
+    cn = (n_range[1] + 1) ** 2 - n_range[0] ** 2
+    cnu = (nu_range[1] + 1) ** 2 - nu_range[0] ** 2
+    A = np.zeros(2 * cn * cnu)
+    B = np.zeros(2 * cn * cnu)
+    lib().orc_translation_xu(x, theta, phi, n_range[0], n_range[1], nu_range[0], nu_range[1],
+                             z, A, B)
+    return A.view(np.complex128).reshape(cn, cnu), B.view(np.complex128).reshape(cn, cnu)
+
+
+def universal_index(point, l):
+    return lib().orc_universal_index(np.ascontiguousarray(point, dtype=np.float64), l)
+
+
+def coordinate_binary(f):
+    return lib().orc_coordinate_binary(f)
+
+
+def scale_points(centres):
+    c = np.ascontiguousarray(centres, dtype=np.float64).reshape(-1)
+    out = np.zeros_like(c)
+    lib().orc_scale_points(len(c) // 3, c, out)
+    return out.reshape(-1, 3)
+
+
+def build_tree(centres, s=10, l_max=0):
+    c = np.ascontiguousarray(centres, dtype=np.float64).reshape(-1)
+    n = len(c) // 3
+    u = np.zeros(n, np.int64)
+    order = np.zeros(n, np.int32)
+    lmin = C.c_int(0)
+    lmax = C.c_int(0)
+    lib().orc_build_tree(n, c, s, l_max, u, order, C.byref(lmin), C.byref(lmax))
+    return u, order, lmin.value, lmax.value
+
+
+class Problem:
+    """The multi-sphere problem in the reference's data model (lib_mie_type.f90:43-99)."""
+
+    def __init__(self, scene):
+        L = lib()
+        s = scene
+        self.scene = s
+        self.h = L.orc_problem_create(
+            s.lambda_0, s.n_medium, s.n_range[0], s.n_range[1], s.z_coupling,
+            int(s.reference_row_rule), s.n_spheres,
+            np.ascontiguousarray(s.centres, np.float64).reshape(-1),
+            np.ascontiguousarray(s.param_index, np.int32), s.n_param,
+            _c(s.refractive_index), np.ascontiguousarray(s.radius, np.float64),
+            np.ascontiguousarray(s.n_range_param, np.int32).reshape(-1), s.n_waves,
+            np.ascontiguousarray(s.wave_theta, np.float64),
+            np.ascontiguousarray(s.wave_phi, np.float64),
+            np.ascontiguousarray(s.jones, np.float64).reshape(-1),
+            np.ascontiguousarray(s.wave_g, np.float64),
+            np.ascontiguousarray(s.wave_phase, np.float64),
+            np.ascontiguousarray(s.wave_d0, np.float64).reshape(-1))
+        self.n = L.orc_vector_length(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_problem_destroy(self.h)
+            self.h = None
+
+    def mie(self, ip):
+        a0, a1 = self.scene.n_range_param[ip]
+        a = np.zeros(2 * (a1 - a0 + 1))
+        b = np.zeros(2 * (a1 - a0 + 1))
+        lib().orc_mie_of_param(self.h, ip, a, b)
+        return a.view(np.complex128), b.view(np.complex128)
+
+    def vector_b(self, with_pq=False):
+        b = np.zeros(2 * self.n)
+        pq = np.zeros(2 * self.n)
+        lib().orc_vector_b(self.h, b, pq)
+        if with_pq:
+            return b.view(np.complex128), pq.view(np.complex128)
+        return b.view(np.complex128)
+
+    def matvec(self, x):
+        y = np.zeros(2 * self.n)
+        lib().orc_matvec(self.h, _c(x), y)
+        return y.view(np.complex128)
+
+    def solve(self, b=None, x0=None, restart=30, tol=1e-8, maxit=1000, weights=None):
+        if b is None:
+            b = self.vector_b()
+        x = np.array(x0 if x0 is not None else np.zeros(self.n), dtype=np.complex128)
+        xf = _c(x).copy()
+        info = np.zeros(4, np.int32)
+        berr = C.c_double(0.0)
+        w = None
+        if weights is not None:
+            w = np.ascontiguousarray(weights, np.float64)
+        lib().orc_solve(self.h, _c(b), xf, restart, tol, maxit,
+                        w.ctypes.data_as(C.c_void_p) if w is not None else None,
+                        info, C.byref(berr))
+        return xf.view(np.complex128), dict(iterations=int(info[0]), restarts=int(info[1]),
+                                            matvecs=int(info[2]), status=int(info[3]),
+                                            backward_error=berr.value)
+
+    def cross_sections(self, x):
+        out = np.zeros(3)
+        lib().orc_cross_sections(self.h, _c(x), out)
+        return out
+
+
+def _matvec_rows(self, x, j0, j1, cache=True):
+    """Operator rows of target spheres j0 <= j < j1 (other entries zero)."""
+    L = lib()
+    if not getattr(L, "_rows_sig", False):
+        L.orc_matvec_rows.argtypes = [C.c_void_p, dp, C.c_int, C.c_int, C.c_int, dp]
+        L._rows_sig = True
+    y = np.zeros(2 * self.n)
+    L.orc_matvec_rows(self.h, _c(x), int(j0), int(j1), int(bool(cache)), y)
+    return y.view(np.complex128)
+
+
+Problem.matvec_rows = _matvec_rows
+
+
+def _pairs_apply(self, x, targets, sources):
+    """Contributions of ordered pairs (targets[i] <- sources[i]) to the operator, every
+    translation block recomputed as in the reference."""
+    L = lib()
+    if not getattr(L, "_pairs_sig", False):
+        L.orc_pairs_apply.argtypes = [C.c_void_p, dp, C.c_int, ip, ip, dp]
+        L._pairs_sig = True
+    y = np.zeros(2 * self.n)
+    t = np.ascontiguousarray(targets, np.int32)
+    s = np.ascontiguousarray(sources, np.int32)
+    L.orc_pairs_apply(self.h, _c(x), len(t), t, s, y)
+    return y.view(np.complex128)
+
+
+Problem.pairs_apply = _pairs_apply
