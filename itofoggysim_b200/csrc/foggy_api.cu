@@ -60,16 +60,24 @@ struct foggy_handle_s {
     int32_t* d_axoff = nullptr;
     double* d_ga = nullptr;
     double* d_gb = nullptr;
+    int64_t* d_koff = nullptr;
+    double* d_gab = nullptr;
     double* d_sqrt_binom = nullptr;
     double* d_rs = nullptr;
+    double* d_irs = nullptr;
+    double* d_rj = nullptr;
     int K = 0;
+    // operator launches: (target bucket, source bucket) pairs of truncation-order buckets
+    std::vector<DirectBucket> launches_direct;
+    int* d_bucket_lists = nullptr;
+    int nbuckets = 0, cmax = 1;
     // waves and right-hand side
     std::vector<WaveDev> waves;
     bool rhs_ready = false;
     cplx* d_b = nullptr;
     cplx* d_pq = nullptr;
     // operator scratch
-    int chunks = 1;
+    int chunks_unused = 0;
     cplx* d_partial = nullptr;
     cplx* d_tmp_in = nullptr;    // ragged work vectors
     cplx* d_tmp_out = nullptr;
@@ -190,14 +198,27 @@ int ensure_tables(foggy_handle h, int pmax) {
     dfree(h, h->d_axoff);
     dfree(h, h->d_ga);
     dfree(h, h->d_gb);
+    dfree(h, h->d_koff);
+    dfree(h, h->d_gab);
     dfree(h, h->d_sqrt_binom);
     dfree(h, h->d_rs);
+    dfree(h, h->d_irs);
+    dfree(h, h->d_rj);
     dfree(h, h->d_g);
     AxialTables t;
     build_axial_tables(pmax, t);
     TRY(dalloc(h, &h->d_axoff, t.offset.size()));
     TRY(dalloc(h, &h->d_ga, t.ga.size()));
     TRY(dalloc(h, &h->d_gb, t.gb.size()));
+    {
+        std::vector<int64_t> koff;
+        std::vector<double> gab;
+        build_axial_tables_qmajor(t, koff, gab);
+        TRY(dalloc(h, &h->d_koff, koff.size()));
+        TRY(dalloc(h, &h->d_gab, gab.size()));
+        CK(h, cudaMemcpy(h->d_koff, koff.data(), koff.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+        CK(h, cudaMemcpy(h->d_gab, gab.data(), gab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     CK(h, cudaMemcpy(h->d_axoff, t.offset.data(), t.offset.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->d_ga, t.ga.data(), t.ga.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->d_gb, t.gb.data(), t.gb.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -210,12 +231,25 @@ int ensure_tables(foggy_handle h, int pmax) {
             for (int i = 1; i <= b; ++i) c = c * (a + i) / i;
             sb[(size_t)J * (2 * K + 1) + (m + K)] = (double)std::sqrt(c);
         }
+    std::vector<double> irs((size_t)(K + 1) * (K + 1), 0.0), rj(2 * (size_t)(K + 2), 0.0);
     for (int j = 0; j <= K; ++j)
-        for (int m = 0; m <= j; ++m) rs[(size_t)j * (K + 1) + m] = std::sqrt((double)j * j - (double)m * m);
+        for (int m = 0; m <= j; ++m) {
+            double v = std::sqrt((double)j * j - (double)m * m);
+            rs[(size_t)j * (K + 1) + m] = v;
+            irs[(size_t)j * (K + 1) + m] = (v > 0) ? 1.0 / v : 0.0;
+        }
+    for (int j = 2; j <= K; ++j) {
+        rj[2 * j] = 1.0 / ((double)j * (j - 1));
+        rj[2 * j + 1] = 1.0 / ((double)(j - 1) * (2.0 * j - 1.0));
+    }
     TRY(dalloc(h, &h->d_sqrt_binom, sb.size()));
     TRY(dalloc(h, &h->d_rs, rs.size()));
+    TRY(dalloc(h, &h->d_irs, irs.size()));
+    TRY(dalloc(h, &h->d_rj, rj.size()));
     CK(h, cudaMemcpy(h->d_sqrt_binom, sb.data(), sb.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->d_rs, rs.data(), rs.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_irs, irs.data(), irs.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_rj, rj.data(), rj.size() * sizeof(double), cudaMemcpyHostToDevice));
     std::vector<double> g;
     build_g_table(pmax, g);
     TRY(dalloc(h, &h->d_g, g.size()));
@@ -225,6 +259,16 @@ int ensure_tables(foggy_handle h, int pmax) {
     return FOGGY_OK;
 }
 
+DTabs dtabs(foggy_handle h) {
+    DTabs t;
+    t.sqrt_binom = h->d_sqrt_binom;
+    t.rs = h->d_rs;
+    t.irs = h->d_irs;
+    t.rj = h->d_rj;
+    t.K = h->K;
+    return t;
+}
+
 DirectArgs direct_args(foggy_handle h, const cplx* x) {
     DirectArgs a;
     a.sc = scene_view(h);
@@ -232,15 +276,68 @@ DirectArgs direct_args(foggy_handle h, const cplx* x) {
     a.ax.offset = h->d_axoff;
     a.ax.ga = h->d_ga;
     a.ax.gb = h->d_gb;
-    a.sqrt_binom = h->d_sqrt_binom;
-    a.rs = h->d_rs;
-    a.K = h->K;
+    a.ax.koff = h->d_koff;
+    a.ax.gab = reinterpret_cast<const double2*>(h->d_gab);
+    a.dt = dtabs(h);
     a.z = h->prm.z_coupling;
     a.x = x;
     a.partial = h->d_partial;
-    a.chunks = h->chunks;
+    a.cmax = h->cmax;
     a.n_unk = h->n_unk;
     return a;
+}
+
+// Truncation-order buckets of the spheres and the (target bucket, source bucket) launches of
+// the direct operator.  Bucket upper bounds grow in steps of 4 degrees; each launch gets enough
+// CTAs per target to fill the GPU.
+int plan_direct(foggy_handle h) {
+    const int bounds[] = {0, 4, 8, 12, 16, 20, 24, 28, 32};
+    std::vector<std::vector<int>> members;
+    std::vector<int> bp;
+    for (int bi = 1; bi < (int)(sizeof(bounds) / sizeof(bounds[0])); ++bi) {
+        std::vector<int> v;
+        for (int j = 0; j < h->N; ++j)
+            if (h->p_s[j] > bounds[bi - 1] && h->p_s[j] <= bounds[bi]) v.push_back(j);
+        if (!v.empty()) {
+            int pm = 0;
+            for (int j : v) pm = std::max(pm, h->p_s[j]);
+            members.push_back(v);
+            bp.push_back(pm);
+        }
+    }
+    h->nbuckets = (int)members.size();
+    const int want = 148 * 6;
+    h->cmax = 1;
+    std::vector<int> chunks(h->nbuckets);
+    for (int t = 0; t < h->nbuckets; ++t) {
+        int nt = (int)members[t].size();
+        int c = std::max(1, std::min(32, (want + nt - 1) / nt));
+        chunks[t] = c;
+        h->cmax = std::max(h->cmax, c);
+    }
+    std::vector<int> flat;
+    std::vector<int> start;
+    for (auto& v : members) {
+        start.push_back((int)flat.size());
+        flat.insert(flat.end(), v.begin(), v.end());
+    }
+    dfree(h, h->d_bucket_lists);
+    TRY(dalloc(h, &h->d_bucket_lists, flat.size()));
+    CK(h, cudaMemcpy(h->d_bucket_lists, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice));
+    h->launches_direct.clear();
+    for (int t = 0; t < h->nbuckets; ++t)
+        for (int s = 0; s < h->nbuckets; ++s) {
+            DirectBucket b;
+            b.targets = h->d_bucket_lists + start[t];
+            b.ntargets = (int)members[t].size();
+            b.sources = h->d_bucket_lists + start[s];
+            b.nsources = (int)members[s].size();
+            b.slab = s * h->cmax;
+            b.chunks = std::min(chunks[t], std::max(1, b.nsources));
+            b.pp = std::max(bp[t], bp[s]);
+            h->launches_direct.push_back(b);
+        }
+    return FOGGY_OK;
 }
 
 // y = A x in the device layout
@@ -248,10 +345,13 @@ int apply_operator(foggy_handle h, const cplx* x, cplx* y) {
     if (h->prm.matvec_mode != FOGGY_MATVEC_DIRECT)
         return fail(h, FOGGY_ERR_UNSUPPORTED, "matvec_mode: only FOGGY_MATVEC_DIRECT is built");
     DirectArgs a = direct_args(h, x);
-    launch_direct(a, h->stream);
+    for (const DirectBucket& b : h->launches_direct) {
+        launch_direct(a, b, h->stream);
+        h->launches += 1;
+    }
     CKL(h);
-    k_direct_finish<<<h->N, 256, 0, h->stream>>>(a.sc, x, h->d_partial, h->chunks, h->n_unk, y);
-    h->launches += 2;
+    k_direct_finish<<<h->N, 256, 0, h->stream>>>(a.sc, x, h->d_partial, h->nbuckets * h->cmax, h->n_unk, y);
+    h->launches += 1;
     CKL(h);
     return FOGGY_OK;
 }
@@ -639,9 +739,8 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
     TRY(dalloc(h, &h->d_pq, h->n_unk));
     TRY(dalloc(h, &h->d_tmp_in, h->n_unk));
     TRY(dalloc(h, &h->d_tmp_out, h->n_unk));
-    h->chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, (4 * 148 + n_spheres - 1) / n_spheres));
-    h->chunks = std::min(h->chunks, std::max(1, n_spheres - 1));
-    TRY(dalloc(h, &h->d_partial, (size_t)h->chunks * h->n_unk));
+    TRY(plan_direct(h));
+    TRY(dalloc(h, &h->d_partial, (size_t)h->nbuckets * h->cmax * h->n_unk));
     CK(h, cudaMemcpy(h->d_centres, centres, 3 * (size_t)n_spheres * sizeof(double), cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->d_p, h->p_s.data(), n_spheres * sizeof(int), cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->d_off, h->off.data(), (n_spheres + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
@@ -897,15 +996,14 @@ int32_t foggy_translation_coefficients(double x, double theta, double phi, const
         foggy_destroy(h);
         return rc;
     }
-    AxialView ax{h->tab_pmax, h->d_axoff, h->d_ga, h->d_gb};
+    AxialView ax{h->tab_pmax, h->d_axoff, h->d_ga, h->d_gb, h->d_koff, reinterpret_cast<const double2*>(h->d_gab)};
     int Pn = pn * (pn + 2), Pnu = pnu * (pnu + 2);
     cplx *dA = nullptr, *dB = nullptr;
     cudaMalloc(&dA, (size_t)Pn * Pnu * sizeof(cplx));
     cudaMalloc(&dB, (size_t)Pn * Pnu * sizeof(cplx));
-    size_t smem = direct_smem_bytes(pmax);
+    size_t smem = translation_pair_smem_bytes(pmax);
     cudaFuncSetAttribute(k_translation_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_translation_pair<<<1, 256, smem, h->stream>>>(ax, h->d_sqrt_binom, h->d_rs, h->K, x, theta, phi, pn, pnu,
-                                                    z_selector, dA, dB);
+    k_translation_pair<<<1, 256, smem, h->stream>>>(ax, dtabs(h), x, theta, phi, pn, pnu, z_selector, dA, dB);
     std::vector<cplx> hA((size_t)Pn * Pnu), hB((size_t)Pn * Pnu);
     cudaError_t e = cudaMemcpyAsync(hA.data(), dA, hA.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hB.data(), dB, hB.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);

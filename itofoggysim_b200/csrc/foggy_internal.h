@@ -24,6 +24,7 @@ struct AxialTables {
 int wigner3j_family(int j1, int j2, int m1, int m2, std::vector<double>& f);
 double wigner3j(int j1, int j2, int j3, int m1, int m2, int m3);
 void build_axial_tables(int pmax, AxialTables& t);
+void build_axial_tables_qmajor(const AxialTables& t, std::vector<int64_t>& koff, std::vector<double>& gab);
 void build_g_table(int pmax, std::vector<double>& g);
 
 // Maximum truncation order of a sphere (the reference caps single spheres at 45,
@@ -78,6 +79,8 @@ struct AxialView {
     const int32_t* offset;
     const double* ga;
     const double* gb;
+    const int64_t* koff;   // q-major layout (build_axial_tables_qmajor)
+    const double2* gab;
 };
 
 }  // namespace foggy

@@ -32,26 +32,43 @@ __global__ void k_pack(SceneView sc, int pg, const double* g, const cplx* ydev, 
 __global__ void k_cross_sections(SceneView sc, const cplx* x, const cplx* pq, double* part);
 
 // k_direct.cu -- all-pairs sphere coupling (the direct operator)
+// Tables of the Wigner small-d recurrence (degrees <= K).
+struct DTabs {
+    const double* sqrt_binom;  // [J][m + K]: sqrt((2J)!/((J+m)!(J-m)!))
+    const double* rs;          // [j][m]: sqrt(j^2 - m^2)
+    const double* irs;         // [j][m]: 1/sqrt(j^2 - m^2) (0 for m = j)
+    const double* rj;          // [2j] = 1/(j(j-1)), [2j+1] = 1/((j-1)(2j-1))
+    int K;
+};
 struct DirectArgs {
     SceneView sc;
     AxialView ax;
-    const double* sqrt_binom;  // d-table start values
-    const double* rs;          // sqrt(j^2 - m^2)
-    int K;                     // width of those tables (>= pmax)
+    DTabs dt;
     int z;                     // radial function selector (1 j_n, 2 y_n, 3 h1, 4 h2)
     const cplx* x;             // ragged scaled input
-    cplx* partial;             // [chunks][n_unk] partial sums
-    int chunks;
+    cplx* partial;             // [slabs][n_unk] partial sums
+    int cmax;                  // slabs per source bucket
     int64_t n_unk;
 };
-size_t direct_smem_bytes(int pmax);
-void launch_direct(const DirectArgs& a, cudaStream_t s);
-// y = x + T (sum of chunk partials) for coupled spheres, y = x otherwise
-__global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial, int chunks, int64_t n_unk,
+// One launch: targets of one degree bucket against the sources of one degree bucket.
+struct DirectBucket {
+    const int* targets;
+    int ntargets;
+    const int* sources;
+    int nsources;
+    int slab;                  // first partial slab of this launch (slab + blockIdx.y)
+    int chunks;                // CTAs per target (<= cmax)
+    int pp;                    // largest degree of the launch (sizes shared memory)
+};
+size_t direct_smem_bytes(int pp);
+size_t translation_pair_smem_bytes(int pmax);
+void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s);
+// y = x + T (sum of the slab partials) for coupled spheres, y = x otherwise
+__global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial, int slabs, int64_t n_unk,
                                 cplx* y);
 // single-pair translation for the parity entry point: A, B blocks in the scaled basis
-__global__ void k_translation_pair(AxialView ax, const double* sqrt_binom, const double* rs, int K, double x,
-                                   double theta, double phi, int pn, int pnu, int z, cplx* A, cplx* B);
+__global__ void k_translation_pair(AxialView ax, DTabs dt, double x, double theta, double phi, int pn, int pnu,
+                                   int z, cplx* A, cplx* B);
 
 // k_gmres.cu -- Krylov kernels (deterministic fixed-order reductions)
 constexpr int kRedBlocks = 296;

@@ -185,6 +185,39 @@ void build_axial_tables(int pmax, AxialTables& t) {
     }
 }
 
+// The same coefficients laid out for coalesced device reads: for each k a block of
+// (pmax + 1) q-planes, each a dense W x W grid over (n, nu) in [lo, pmax]^2 (lo = max(1, k),
+// W = pmax - lo + 1) of (GA, GB) pairs, zero where q > min(n, nu).  koff[k] is the block start
+// in units of pairs.
+void build_axial_tables_qmajor(const AxialTables& t, std::vector<int64_t>& koff, std::vector<double>& gab) {
+    int pmax = t.pmax;
+    int S = pmax + 1;
+    koff.assign(S + 1, 0);
+    int64_t tot = 0;
+    for (int k = 0; k <= pmax; ++k) {
+        koff[k] = tot;
+        int lo = std::max(1, k);
+        int W = pmax - lo + 1;
+        tot += (int64_t)(pmax + 1) * W * W;
+    }
+    koff[S] = tot;
+    gab.assign(2 * (size_t)tot, 0.0);
+    for (int k = 0; k <= pmax; ++k) {
+        int lo = std::max(1, k);
+        int W = pmax - lo + 1;
+        for (int n = lo; n <= pmax; ++n)
+            for (int nu = lo; nu <= pmax; ++nu) {
+                int o = t.offset[((size_t)k * S + n) * S + nu];
+                int qm = std::min(n, nu);
+                for (int q = 0; q <= qm; ++q) {
+                    size_t d = (size_t)koff[k] + ((size_t)q * W + (n - lo)) * W + (nu - lo);
+                    gab[2 * d] = t.ga[o + q];
+                    gab[2 * d + 1] = t.gb[o + q];
+                }
+            }
+    }
+}
+
 // g_nm = (-1)^m sqrt((n+m)!/(n-m)!) for n = 0..pmax, m = -n..n, index n(n+1)+m
 void build_g_table(int pmax, std::vector<double>& g) {
     g.assign((size_t)(pmax + 1) * (pmax + 1), 1.0);

@@ -14,16 +14,33 @@
 // exactly (rotations do not mix degrees).  A_ax/B_ax come from the precomputed 3j tables
 // (gaunt.cpp) and z_p(kd); the Wigner small-d table is built per pair in shared memory.
 //
-// One CTA owns one target sphere j and a strided subset of the sources (blockIdx.y); its
-// partial sum goes to a per-chunk slab that k_direct_finish adds in a fixed order, so results
-// are bit-reproducible.
+// The a and b parts stay separate throughout: combining them as a +- b would diagonalise the
+// axial block but loses the relative precision of the smaller part when |A| >> |B| (large
+// Hankel values at small kd), which the FP64 parity with the reference does not allow.
+//
+// Work decomposition.  Spheres are grouped into buckets of similar truncation order; one launch
+// per (target bucket, source bucket) sizes its shared memory for the larger order of the two.
+// One CTA owns one target sphere and a strided subset of one source bucket.  Per source pair:
+//   1. geometry; warp 0 runs the Bessel recurrences and the phases, the other warps build the
+//      d-table columns; every thread prefetches its part of the source vector;
+//   2. the source with the phase e^{i mu phi}; zeta_p = i^p z_p;
+//   3. rotation, one thread per (degree, |k|, a|b);
+//   4. axial step in chunks of k: the coefficients A, B of the chunk are built in parallel
+//      over (k, n, nu) into shared memory, then applied, one thread per (n, |k|, a|b);
+//   5. rotation back into the target accumulator, one thread per (n, |m|, a|b).
+// The CTA's partial sum goes to its own slab that k_direct_finish adds in a fixed order, so
+// results are bit-reproducible.
 #include "foggy_kernels.cuh"
 #include "k_special.cuh"
+
+#include <cstdlib>
 
 namespace foggy {
 
 namespace {
 constexpr int kThreads = 256;
+constexpr int kTab = 1024;       // axial coefficient pairs per chunk (A+B, A-B)
+constexpr int kMaxPrefetch = 4;  // source entries a thread keeps in registers
 
 __device__ __forceinline__ cplx ipow_mul(int p, cplx c) {
     switch (p & 3) {
@@ -34,158 +51,194 @@ __device__ __forceinline__ cplx ipow_mul(int p, cplx c) {
     }
 }
 __device__ __forceinline__ void decode_nm(int t, int& n, int& m) {
-    int nn = (int)sqrt((double)(t + 1));
+    int nn = (int)__fsqrt_rn((float)(t + 1));
     if ((nn + 1) * (nn + 1) <= t + 1) ++nn;
     if (nn * nn > t + 1) --nn;
     n = nn;
     m = t + 1 - nn * nn - nn;
 }
+// u = 0.. over (n >= 1, 0 <= k <= n) in order
 __device__ __forceinline__ void decode_nk(int u, int& n, int& k) {
-    int nn = (int)((-1.0 + sqrt(9.0 + 8.0 * u)) * 0.5);
-    while ((nn - 1) * (nn + 2) / 2 > u) --nn;
+    int nn = (int)((-1.0f + __fsqrt_rn(9.0f + 8.0f * (float)u)) * 0.5f);
+    if (nn < 1) nn = 1;
+    while (nn > 1 && (nn - 1) * (nn + 2) / 2 > u) --nn;
     while (nn * (nn + 3) / 2 <= u) ++nn;
     n = nn;
     k = u - (nn - 1) * (nn + 2) / 2;
 }
-
-struct Smem {
-    double* dq;
-    double* jb;
-    double* yb;
-    cplx* zeta;
-    cplx* eph;
-    cplx* xr;
-    cplx* yr;
-    cplx* acc;
-    double* geom;
-};
+__device__ __forceinline__ double sgn(int e) { return (e & 1) ? -1.0 : 1.0; }
+// one (m', m) column index c < (pp+1)^2 -> (m', m)
+__device__ __forceinline__ void decode_col(int c, int& mp, int& m) {
+    int q = (int)__fsqrt_rn((float)c);
+    if ((q + 1) * (q + 1) <= c) ++q;
+    if (q * q > c) --q;
+    mp = q;
+    m = c - q * q - q;
+}
 
 __host__ __device__ inline size_t align2(size_t v) { return (v + 1) & ~(size_t)1; }
 
-__device__ inline Smem carve(double* base, int pmax) {
+struct Smem {
+    double* dq;    // quarter Wigner-d table, degrees <= pp
+    double* jb;    // j_p(rho)
+    double* yb;    // y_p(rho)
+    cplx* zeta;    // i^p z_p(rho)
+    cplx* eph;     // e^{i mu phi}, |mu| <= pp
+    cplx* x1;      // phase-multiplied source (a | b), then the axially translated field (a | b)
+    cplx* xr;      // rotated source (a | b)
+    cplx* tab;     // axial coefficients of one k-chunk: (A, B) pairs
+    cplx* acc;     // target accumulator (a | b)
+    double* geom;  // rho, theta, phi
+};
+
+__host__ __device__ inline size_t smem_doubles(int pp) {
+    size_t P = (size_t)pp * (pp + 2);
+    return align2(dq_size(pp)) + 2 * align2(2 * pp + 3) + 2 * (2 * pp + 3) + 2 * (2 * pp + 1) + 3 * 2 * (2 * P) +
+           2 * 2 * kTab + 4;
+}
+
+__device__ inline Smem carve(double* base, int pp) {
     Smem s;
     size_t o = 0;
-    int P = pmax * (pmax + 2);
-    s.dq = base + o;   o += align2(dq_size(pmax));
-    s.jb = base + o;   o += align2(2 * pmax + 3);
-    s.yb = base + o;   o += align2(2 * pmax + 3);
-    s.zeta = reinterpret_cast<cplx*>(base + o); o += 2 * (2 * pmax + 3);
-    s.eph = reinterpret_cast<cplx*>(base + o);  o += 2 * (2 * pmax + 1);
+    int P = pp * (pp + 2);
+    s.dq = base + o;   o += align2(dq_size(pp));
+    s.jb = base + o;   o += align2(2 * pp + 3);
+    s.yb = base + o;   o += align2(2 * pp + 3);
+    s.zeta = reinterpret_cast<cplx*>(base + o); o += 2 * (2 * pp + 3);
+    s.eph = reinterpret_cast<cplx*>(base + o);  o += 2 * (2 * pp + 1);
+    s.x1 = reinterpret_cast<cplx*>(base + o);   o += 2 * (2 * P);
     s.xr = reinterpret_cast<cplx*>(base + o);   o += 2 * (2 * P);
-    s.yr = reinterpret_cast<cplx*>(base + o);   o += 2 * (2 * P);
     s.acc = reinterpret_cast<cplx*>(base + o);  o += 2 * (2 * P);
+    s.tab = reinterpret_cast<cplx*>(base + o);  o += 2 * 2 * kTab;
     s.geom = base + o;
     return s;
 }
 
-// Fills zeta[p] = i^p z_p(rho) for p <= P, e^{i mu phi} for |mu| <= pp and the d-table for
-// degrees <= pp.  Warp 0 runs the Bessel recurrences and the phases, the other warps the
-// d-table columns; ends with a barrier.
-__device__ inline void pair_tables(const Smem& s, double rho, double theta, double phi, int P, int pp, int z,
-                                   const double* sqrt_binom, const double* rs, int K) {
-    int tid = threadIdx.x;
-    int warp = tid >> 5, lane = tid & 31;
-    if (warp == 0) {
-        if (lane == 0) dev_sph_jn(rho, P, s.jb);
-        else if (lane == 1 && z != 1) dev_sph_yn(rho, P, s.yb);
-        for (int mu = -pp + lane; mu <= pp; mu += 32) {
-            double sn, cs;
-            sincos((double)mu * phi, &sn, &cs);
-            s.eph[mu + pp] = mk(cs, sn);
-        }
-    } else {
-        // The reference evaluates its Legendre functions at x = cos(theta) with
-        // sqrt(|1 - x^2|) as the sine (LPMNS, lib_math_legendre.f90:68-126); the half angles
-        // are taken from that same (x, s) so that the rotation sees the angle the reference
-        // sees, also where cos(theta) rounds to +-1.
-        double cb = cos(theta);
-        double sbf = sqrt(fabs(1.0 - cb * cb));
-        double sb2, cb2;
-        if (cb >= 0.0) {
-            cb2 = sqrt(0.5 * (1.0 + cb));
-            sb2 = 0.5 * sbf / cb2;
+// Column (m', m), m' >= |m|, of the quarter d-table for j = m'..jmax by the upward three-term
+// recurrence of the Jacobi polynomials behind d^j_{m'm}; division-free with the tables
+//   rs[j][m] = sqrt(j^2 - m^2), irs[j][m] = 1/sqrt(j^2 - m^2), rj[j] = {1/(j(j-1)), 1/((j-1)(2j-1))}.
+__device__ inline void dq_column2(double* dq, int mp, int m, int jmax, double cb, double ch, double sh,
+                                  const DTabs& t) {
+    int J = mp;
+    int am = m < 0 ? -m : m;
+    double v = sgn(J - m) * t.sqrt_binom[J * (2 * t.K + 1) + (m + t.K)] * ipow_d(ch, J + m) * ipow_d(sh, J - m);
+    dq[dq_index(J, mp, m)] = v;
+    double prev2 = 0.0, prev1 = v;
+    const int W = t.K + 1;
+    double mmp = (double)(m * mp);
+    for (int j = J + 1; j <= jmax; ++j) {
+        double val;
+        if (j == 1) {
+            val = cb * prev1;
         } else {
-            sb2 = sqrt(0.5 * (1.0 - cb));
-            cb2 = 0.5 * sbf / sb2;
+            double jj = (double)j;
+            double c1 = jj * (2.0 * jj - 1.0) * t.irs[j * W + am] * t.irs[j * W + mp];
+            double c2 = c1 * t.rs[(j - 1) * W + am] * t.rs[(j - 1) * W + mp] * t.rj[2 * j + 1];
+            val = c1 * (cb - mmp * t.rj[2 * j]) * prev1 - c2 * prev2;
         }
-        int ncol = (pp + 1) * (pp + 1);
-        for (int t = tid - 32; t < ncol; t += blockDim.x - 32) {
-            int mp = (int)sqrt((double)t);
-            if ((mp + 1) * (mp + 1) <= t) ++mp;
-            if (mp * mp > t) --mp;
-            int m = t - mp * mp - mp;
-            dq_column(s.dq, mp, m, pp, cb, cb2, sb2, sqrt_binom, rs, K);
-        }
-    }
-    __syncthreads();
-    for (int p = tid; p <= P; p += blockDim.x) {
-        cplx zc;
-        switch (z) {
-            case 1: zc = mk(s.jb[p], 0.0); break;
-            case 2: zc = mk(s.yb[p], 0.0); break;
-            case 3: zc = mk(s.jb[p], s.yb[p]); break;
-            default: zc = mk(s.jb[p], -s.yb[p]); break;
-        }
-        s.zeta[p] = ipow_mul(p, zc);
+        dq[dq_index(j, mp, m)] = val;
+        prev2 = prev1;
+        prev1 = val;
     }
 }
 
-// axial A_ax(k; n, nu), B_ax(k; n, nu) for k >= 0 from the 3j tables and zeta
+// The reference evaluates its Legendre functions at x = cos(theta) with sqrt(|1 - x^2|) as
+// the sine (LPMNS, lib_math_legendre.f90:68-126); the half angles are taken from that same
+// (x, s) so that the rotation sees the angle the reference sees, also where cos(theta) rounds
+// to +-1.
+__device__ __forceinline__ void half_angles(double theta, double& cb, double& cb2, double& sb2) {
+    cb = cos(theta);
+    double sbf = sqrt(fabs(1.0 - cb * cb));
+    if (cb >= 0.0) {
+        cb2 = sqrt(0.5 * (1.0 + cb));
+        sb2 = 0.5 * sbf / cb2;
+    } else {
+        sb2 = sqrt(0.5 * (1.0 - cb));
+        cb2 = 0.5 * sbf / sb2;
+    }
+}
+
+__device__ __forceinline__ cplx zeta_of(int z, int p, const double* jb, const double* yb) {
+    cplx zc;
+    switch (z) {
+        case 1: zc = mk(jb[p], 0.0); break;
+        case 2: zc = mk(yb[p], 0.0); break;
+        case 3: zc = mk(jb[p], yb[p]); break;
+        default: zc = mk(jb[p], -yb[p]); break;
+    }
+    return ipow_mul(p, zc);
+}
+
+// A_ax(k; n, nu), B_ax(k; n, nu) for k >= 0 from the 3j tables and zeta
 __device__ __forceinline__ void axial_coeff(const AxialView& ax, const cplx* zeta, int k, int n, int nu, cplx& A,
                                             cplx& B) {
     int S = ax.pmax + 1;
     int o = ax.offset[((size_t)k * S + n) * S + nu];
     int qm = min(n, nu);
-    cplx a = mk(0, 0), b = mk(0, 0);
     const double* ga = ax.ga + o;
     const double* gb = ax.gb + o;
-    for (int q = 0; q <= qm; ++q) {
-        int p = n + nu - 2 * q;
-        double g1 = __ldg(ga + q);
-        a.x += g1 * zeta[p].x;
-        a.y += g1 * zeta[p].y;
-        if (q >= 1) {
-            double g2 = __ldg(gb + q);
-            b.x += g2 * zeta[p + 1].x;
-            b.y += g2 * zeta[p + 1].y;
-        }
+    int p = n + nu;
+    double g1 = __ldg(ga);
+    double ax_ = g1 * zeta[p].x, ay_ = g1 * zeta[p].y, bx_ = 0, by_ = 0;
+    for (int q = 1; q <= qm; ++q) {
+        p -= 2;
+        double g1q = __ldg(ga + q);
+        double g2q = __ldg(gb + q);
+        cplx z0 = zeta[p], z1 = zeta[p + 1];
+        ax_ += g1q * z0.x;
+        ay_ += g1q * z0.y;
+        bx_ += g2q * z1.x;
+        by_ += g2q * z1.y;
     }
-    A = a;
-    B = b;
+    A = mk(ax_, ay_);
+    B = mk(bx_, by_);
+}
+
+// entry d^j_{mu k} of a full matrix from the quarter table, k >= 0, without branches:
+//   |mu| <= k : (-1)^{k-mu} dq(k, mu);  mu > k : dq(mu, k);  mu < -k : (-1)^{k-mu} dq(-mu, -k)
+__device__ __forceinline__ double d_col(const double* dq, int db, int mu, int k) {
+    int amu = mu < 0 ? -mu : mu;
+    int mp = max(k, amu);
+    int m = (amu <= k) ? mu : (mu > 0 ? k : -k);
+    double s = (mu > k) ? 1.0 : sgn(k - mu);
+    return s * dq[db + mp * (mp + 1) + m];
+}
+// entry d^n_{m k} of a full matrix from the quarter table, m >= 0:
+//   |k| <= m : dq(m, k);  k > m : (-1)^{k-m} dq(k, m);  k < -m : dq(-k, -m)
+__device__ __forceinline__ double d_row(const double* dq, int db, int m, int k) {
+    int ak = k < 0 ? -k : k;
+    int mp = max(m, ak);
+    int mm = (ak <= m) ? k : (k > 0 ? m : -m);
+    double s = (k > m) ? sgn(k - m) : 1.0;
+    return s * dq[db + mp * (mp + 1) + mm];
 }
 
 }  // namespace
 
-size_t direct_smem_bytes(int pmax) {
-    int P = pmax * (pmax + 2);
-    size_t o = 0;
-    o += align2(dq_size(pmax));
-    o += align2(2 * pmax + 3) * 2;
-    o += 2 * (2 * pmax + 3) + 2 * (2 * pmax + 1);
-    o += 3 * 2 * (2 * (size_t)P);
-    o += 4;
-    return o * sizeof(double);
-}
-
-__global__ void __launch_bounds__(kThreads) k_direct(DirectArgs a) {
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBucket bk) {
     extern __shared__ double smem_d[];
     const SceneView& sc = a.sc;
-    Smem s = carve(smem_d, sc.pmax);
-    int j = blockIdx.x;
-    int c = blockIdx.y;
+    const int pp = bk.pp;
+    Smem s = carve(smem_d, pp);
+    const int j = bk.targets[blockIdx.x];
+    const int c = blockIdx.y;
     if (!sc.couple[j]) return;
-    int tid = threadIdx.x;
-    int pj = sc.p[j];
-    int Pj = pj * (pj + 2);
-    for (int t = tid; t < 2 * Pj; t += blockDim.x) s.acc[t] = mk(0, 0);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nthr = blockDim.x;
+    const int pj = sc.p[j];
+    const int Pj = pj * (pj + 2);
+    for (int t = tid; t < 2 * Pj; t += nthr) s.acc[t] = mk(0, 0);
     const double* cj = sc.centres + 3 * (size_t)j;
 
-    for (int l = c; l < sc.n; l += a.chunks) {
+    for (int i = c; i < bk.nsources; i += bk.chunks) {
+        const int l = bk.sources[i];
         if (l == j) continue;
-        int pl = sc.p[l];
-        int Pl = pl * (pl + 2);
-        int pp = max(pj, pl);
-        int P = pj + pl + 1;
+        const int pl = sc.p[l];
+        const int Pl = pl * (pl + 2);
+        const int pq = max(pj, pl);
+        const int P = pj + pl + 1;
+        // ---- 1. geometry, then tables; source entries prefetched into registers --------------
         if (tid == 0) {
             const double* cl = sc.centres + 3 * (size_t)l;
             double d0 = sc.k * (cl[0] - cj[0]);
@@ -196,89 +249,229 @@ __global__ void __launch_bounds__(kThreads) k_direct(DirectArgs a) {
             s.geom[1] = (r == 0.0) ? 0.0 : acos(d2 / r);
             s.geom[2] = (d0 == 0.0 && d1 == 0.0) ? 0.0 : atan2(d1, d0);
         }
-        __syncthreads();
-        double rho = s.geom[0], theta = s.geom[1], phi = s.geom[2];
-        pair_tables(s, rho, theta, phi, P, pp, a.z, a.sqrt_binom, a.rs, a.K);
-
-        // rotate the source: x'_nu[k] = sum_mu d^nu_{mu k} e^{i mu phi} x_nu[mu]
+        cplx pa[kMaxPrefetch], pb[kMaxPrefetch];
         const cplx* xl = a.x + sc.off[l];
-        for (int t = tid; t < Pl; t += blockDim.x) {
-            int nu, k;
-            decode_nm(t, nu, k);
-            cplx sa = mk(0, 0), sb = mk(0, 0);
-            int base = nu * nu - 1 + nu;
-            for (int mu = -nu; mu <= nu; ++mu) {
-                double dv = dq_get(s.dq, nu, mu, k);
-                cplx e = s.eph[mu + pp];
-                cplx xa = xl[base + mu], xb = xl[Pl + base + mu];
-                sa = sa + dv * (e * xa);
-                sb = sb + dv * (e * xb);
+#pragma unroll
+        for (int q = 0; q < kMaxPrefetch; ++q) {
+            int t = tid + q * nthr;
+            if (t < Pl) {
+                pa[q] = xl[t];
+                pb[q] = xl[Pl + t];
             }
-            s.xr[t] = sa;
-            s.xr[Pl + t] = sb;
         }
         __syncthreads();
-
-        // axial translation, outputs (n, +-k)
-        int nout = pj * (pj + 3) / 2;
-        for (int u = tid; u < nout; u += blockDim.x) {
-            int n, k;
-            decode_nk(u, n, k);
-            cplx yap = mk(0, 0), ybp = mk(0, 0), yam = mk(0, 0), ybm = mk(0, 0);
-            for (int nu = max(k, 1); nu <= pl; ++nu) {
-                cplx A, B;
-                axial_coeff(a.ax, s.zeta, k, n, nu, A, B);
-                int ip = nu * nu - 1 + nu + k;
-                cplx xap = s.xr[ip], xbp = s.xr[Pl + ip];
-                yap = yap + A * xap + B * xbp;
-                ybp = ybp + B * xap + A * xbp;
-                if (k > 0) {
-                    int im = nu * nu - 1 + nu - k;
-                    cplx xam = s.xr[im], xbm = s.xr[Pl + im];
-                    yam = yam + A * xam - B * xbm;
-                    ybm = ybm - B * xam + A * xbm;
+        if (warp == 0) {
+            double rho = s.geom[0], phi = s.geom[2];
+            if (lane == 0) dev_sph_jn(rho, P, s.jb);
+            else if (lane == 1 && a.z != 1) dev_sph_yn(rho, P, s.yb);
+            for (int mu = -pq + lane; mu <= pq; mu += 32) {
+                double sn, cs;
+                sincos((double)mu * phi, &sn, &cs);
+                s.eph[mu + pp] = mk(cs, sn);
+            }
+        } else {
+            double cb, cb2, sb2;
+            half_angles(s.geom[1], cb, cb2, sb2);
+            int ncol = (pq + 1) * (pq + 1);
+            for (int cc = tid - 32; cc < ncol; cc += nthr - 32) {
+                int mp, m;
+                decode_col(cc, mp, m);
+                dq_column2(s.dq, mp, m, pq, cb, cb2, sb2, a.dt);
+            }
+        }
+        __syncthreads();
+        // ---- 2. x1 = e^{i mu phi} x (a | b); zeta ---------------------------------------------
+#pragma unroll
+        for (int q = 0; q < kMaxPrefetch; ++q) {
+            int t = tid + q * nthr;
+            if (t < Pl) {
+                int nu, mu;
+                decode_nm(t, nu, mu);
+                cplx e = s.eph[mu + pp];
+                s.x1[t] = e * pa[q];
+                s.x1[Pl + t] = e * pb[q];
+            }
+        }
+        for (int t = kMaxPrefetch * nthr + tid; t < Pl; t += nthr) {   // orders above the prefetch
+            int nu, mu;
+            decode_nm(t, nu, mu);
+            cplx e = s.eph[mu + pp];
+            s.x1[t] = e * xl[t];
+            s.x1[Pl + t] = e * xl[Pl + t];
+        }
+        for (int p = tid; p <= P; p += nthr) s.zeta[p] = zeta_of(a.z, p, s.jb, s.yb);
+        __syncthreads();
+        // ---- 3. rotate the source: x'_nu[+-k] = sum_mu d^nu_{mu k} x1_nu[mu] (and partner) ----
+        {
+            int items = pl * (pl + 3);   // (nu, k >= 0) x {a, b}
+            for (int t = tid; t < items; t += nthr) {
+                int part = t & 1;
+                int nu, k;
+                decode_nk(t >> 1, nu, k);
+                int base = nu * nu - 1 + nu;
+                int db = dq_base(nu);
+                const cplx* xv = s.x1 + part * Pl + base;
+                double px = 0, py = 0, mx = 0, my = 0;
+                for (int mu = -nu; mu <= nu; ++mu) {
+                    double d = d_col(s.dq, db, mu, k);
+                    double dm = sgn(k - mu) * d;
+                    cplx x1p = xv[mu], x1m = xv[-mu];
+                    px += d * x1p.x;
+                    py += d * x1p.y;
+                    mx += dm * x1m.x;
+                    my += dm * x1m.y;
+                }
+                cplx* out = s.xr + part * Pl + base;
+                out[k] = mk(px, py);
+                if (k > 0) out[-k] = mk(mx, my);
+            }
+        }
+        __syncthreads();
+        // ---- 4. axial step in chunks of k -----------------------------------------------------
+        {
+            const int kmax = min(pj, pl);
+            // orders |k| > pl of the target receive nothing from this source
+            if (pj > kmax) {
+                int items = Pj;
+                for (int t = tid; t < 2 * items; t += nthr) {
+                    int part = t >= items;
+                    int n, k;
+                    decode_nm(t - part * items, n, k);
+                    if (k > kmax || k < -kmax) s.x1[part * Pj + t - part * items] = mk(0, 0);
                 }
             }
-            int op = n * n - 1 + n + k;
-            s.yr[op] = yap;
-            s.yr[Pj + op] = ybp;
-            if (k > 0) {
-                int om = n * n - 1 + n - k;
-                s.yr[om] = yam;
-                s.yr[Pj + om] = ybm;
+            int k0 = 0;
+            while (k0 <= kmax) {
+                // chunk [k0, k1): entries (k, n, nu) with n, nu >= max(1, k)
+                int k1 = k0, tot = 0;
+                while (k1 <= kmax) {
+                    int lo = max(1, k1);
+                    int e = (pj - lo + 1) * (pl - lo + 1);
+                    if (tot + e > kTab && k1 > k0) break;
+                    tot += e;
+                    ++k1;
+                }
+                // build (A, B) of the chunk
+                for (int t = tid; t < tot; t += nthr) {
+                    int k = k0, off = 0;
+                    for (;;) {
+                        int lo = max(1, k);
+                        int e = (pj - lo + 1) * (pl - lo + 1);
+                        if (t < off + e) break;
+                        off += e;
+                        ++k;
+                    }
+                    int lo = max(1, k);
+                    int r = t - off;
+                    int nnu = pl - lo + 1;
+                    int n = lo + r / nnu, nu = lo + r % nnu;
+                    // q-major 3j table: neighbouring threads read neighbouring (n, nu)
+                    const int W = a.ax.pmax - lo + 1;
+                    const size_t plane = (size_t)W * W;
+                    const double2* g = a.ax.gab + a.ax.koff[k] + (size_t)(n - lo) * W + (nu - lo);
+                    int qm = min(n, nu);
+                    int p = n + nu;
+                    double2 g0 = __ldg(g);
+                    double ax_ = g0.x * s.zeta[p].x, ay_ = g0.x * s.zeta[p].y, bx_ = 0.0, by_ = 0.0;
+                    for (int q = 1; q <= qm; ++q) {
+                        p -= 2;
+                        double2 gq = __ldg(g + q * plane);
+                        cplx z0 = s.zeta[p], z1 = s.zeta[p + 1];
+                        ax_ += gq.x * z0.x;
+                        ay_ += gq.x * z0.y;
+                        bx_ += gq.y * z1.x;
+                        by_ += gq.y * z1.y;
+                    }
+                    s.tab[2 * t] = mk(ax_, ay_);
+                    s.tab[2 * t + 1] = mk(bx_, by_);
+                }
+                __syncthreads();
+                // apply: items (n, k >= 0) x {a, b}
+                int items = 0;
+                for (int k = k0; k < k1; ++k) items += pj - max(1, k) + 1;
+                for (int t = tid; t < 2 * items; t += nthr) {
+                    int part = t & 1;
+                    int w = t >> 1;
+                    int k = k0, off = 0, toff = 0;
+                    for (;;) {
+                        int lo = max(1, k);
+                        int e = pj - lo + 1;
+                        if (w < off + e) break;
+                        off += e;
+                        toff += e * (pl - lo + 1);
+                        ++k;
+                    }
+                    int lo = max(1, k);
+                    int n = lo + (w - off);
+                    int nnu = pl - lo + 1;
+                    const cplx* row = s.tab + 2 * (toff + (n - lo) * nnu);
+                    // a' = A a + B b, b' = B a + A b at +k;  a' = A a - B b, b' = -B a + A b at -k
+                    const cplx* xs = s.xr + part * Pl;          // same part
+                    const cplx* xo = s.xr + (1 - part) * Pl;    // other part
+                    cplx yp = mk(0, 0), ym = mk(0, 0);
+                    for (int nu = lo; nu <= pl; ++nu) {
+                        cplx A = row[2 * (nu - lo)], B = row[2 * (nu - lo) + 1];
+                        int base = nu * nu - 1 + nu;
+                        yp = yp + A * xs[base + k] + B * xo[base + k];
+                        if (k > 0) ym = ym + A * xs[base - k] - B * xo[base - k];
+                    }
+                    int ob = part * Pj + n * n - 1 + n;
+                    s.x1[ob + k] = yp;
+                    if (k > 0) s.x1[ob - k] = ym;
+                }
+                __syncthreads();
+                k0 = k1;
             }
         }
-        __syncthreads();
-
-        // rotate back and accumulate: y_nm += e^{-i m phi} sum_k d^n_{mk} y'_n[k]
-        for (int t = tid; t < Pj; t += blockDim.x) {
-            int n, m;
-            decode_nm(t, n, m);
-            cplx sa = mk(0, 0), sb = mk(0, 0);
-            int base = n * n - 1 + n;
-            for (int k = -n; k <= n; ++k) {
-                double dv = dq_get(s.dq, n, m, k);
-                sa = sa + dv * s.yr[base + k];
-                sb = sb + dv * s.yr[Pj + base + k];
+        // ---- 5. rotate back into the accumulator ------------------------------------------------
+        {
+            int items = pj * (pj + 3);   // (n, m >= 0) x {a, b}
+            for (int t = tid; t < items; t += nthr) {
+                int part = t & 1;
+                int n, m;
+                decode_nk(t >> 1, n, m);
+                int base = n * n - 1 + n;
+                int db = dq_base(n);
+                const cplx* yv = s.x1 + part * Pj + base;
+                double px = 0, py = 0, mx = 0, my = 0;
+                for (int k = -n; k <= n; ++k) {
+                    double d = d_row(s.dq, db, m, k);
+                    double dm = sgn(m - k) * d;
+                    cplx yp = yv[k], ym = yv[-k];
+                    px += d * yp.x;
+                    py += d * yp.y;
+                    mx += dm * ym.x;
+                    my += dm * ym.y;
+                }
+                cplx* acc = s.acc + part * Pj + base;
+                cplx e = s.eph[m + pp];
+                acc[m] = acc[m] + conjg(e) * mk(px, py);
+                if (m > 0) acc[-m] = acc[-m] + e * mk(mx, my);
             }
-            cplx e = conjg(s.eph[m + pp]);
-            s.acc[t] = s.acc[t] + e * sa;
-            s.acc[Pj + t] = s.acc[Pj + t] + e * sb;
         }
         __syncthreads();
     }
-    cplx* out = a.partial + (size_t)c * a.n_unk + sc.off[j];
-    for (int t = tid; t < 2 * Pj; t += blockDim.x) out[t] = s.acc[t];
+    cplx* out = a.partial + (size_t)(bk.slab + c) * a.n_unk + sc.off[j];
+    for (int t = tid; t < 2 * Pj; t += nthr) out[t] = s.acc[t];
+    // slabs of this source bucket that launches with fewer chunks leave unused
+    if (c == bk.chunks - 1)
+        for (int e = c + 1; e < a.cmax; ++e) {
+            cplx* z = a.partial + (size_t)(bk.slab + e) * a.n_unk + sc.off[j];
+            for (int t = tid; t < 2 * Pj; t += nthr) z[t] = mk(0, 0);
+        }
 }
 
-void launch_direct(const DirectArgs& a, cudaStream_t s) {
-    size_t smem = direct_smem_bytes(a.sc.pmax);
+size_t direct_smem_bytes(int pp) { return smem_doubles(pp) * sizeof(double); }
+
+void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s) {
+    size_t smem = direct_smem_bytes(b.pp);
+    dim3 grid(b.ntargets, b.chunks);
     cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid(a.sc.n, a.chunks);
-    k_direct<<<grid, kThreads, smem, s>>>(a);
+    k_direct<<<grid, kThreads, smem, s>>>(a, b);
 }
 
-__global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial, int chunks, int64_t n_unk,
+// y = x + T (sum of the slabs) for coupled spheres, y = x otherwise
+__global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial, int slabs, int64_t n_unk,
                                 cplx* y) {
     int j = blockIdx.x;
     int pj = sc.p[j];
@@ -289,7 +482,7 @@ __global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial
         cplx v = x[o + t];
         if (cp) {
             cplx sum = mk(0, 0);
-            for (int c = 0; c < chunks; ++c) sum = sum + partial[(size_t)c * n_unk + o + t];
+            for (int c = 0; c < slabs; ++c) sum = sum + partial[(size_t)c * n_unk + o + t];
             int tt = t < Pj ? t : t - Pj;
             int n, m;
             decode_nm(tt, n, m);
@@ -300,21 +493,37 @@ __global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial
     }
 }
 
+size_t translation_pair_smem_bytes(int pmax) { return smem_doubles(pmax) * sizeof(double); }
+
 // A, B of one translation in the scaled basis, row (n, m) major: rows n = 1..pn, columns
 // nu = 1..pnu; one CTA.
-__global__ void __launch_bounds__(kThreads) k_translation_pair(AxialView ax, const double* sqrt_binom,
-                                                               const double* rs, int K, double x, double theta,
+__global__ void __launch_bounds__(kThreads) k_translation_pair(AxialView ax, DTabs dt, double x, double theta,
                                                                double phi, int pn, int pnu, int z, cplx* A,
                                                                cplx* B) {
     extern __shared__ double smem_t[];
-    int pmax = max(pn, pnu);
-    Smem s = carve(smem_t, pmax);
-    int pp = pmax;
-    int P = pn + pnu + 1;
-    pair_tables(s, x, theta, phi, P, pp, z, sqrt_binom, rs, K);
+    const int pp = max(pn, pnu);
+    Smem s = carve(smem_t, pp);
+    int tid = threadIdx.x;
+    const int P = pn + pnu + 1;
+    if (tid == 0) dev_sph_jn(x, P, s.jb);
+    if (tid == 1 && z != 1) dev_sph_yn(x, P, s.yb);
+    for (int t = tid; t < 2 * pp + 1; t += blockDim.x) {
+        double sn, cs;
+        sincos((double)(t - pp) * phi, &sn, &cs);
+        s.eph[t] = mk(cs, sn);
+    }
+    double cb, cb2, sb2;
+    half_angles(theta, cb, cb2, sb2);
+    for (int cc = tid; cc < (pp + 1) * (pp + 1); cc += blockDim.x) {
+        int mp, m;
+        decode_col(cc, mp, m);
+        dq_column2(s.dq, mp, m, pp, cb, cb2, sb2, dt);
+    }
+    __syncthreads();
+    for (int p = tid; p <= P; p += blockDim.x) s.zeta[p] = zeta_of(z, p, s.jb, s.yb);
     __syncthreads();
     int Pn = pn * (pn + 2), Pnu = pnu * (pnu + 2);
-    for (int t = threadIdx.x; t < Pn * Pnu; t += blockDim.x) {
+    for (int t = tid; t < Pn * Pnu; t += blockDim.x) {
         int r = t / Pnu, cidx = t % Pnu;
         int n, m, nu, mu;
         decode_nm(r, n, m);

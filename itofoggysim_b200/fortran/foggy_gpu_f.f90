@@ -1,0 +1,198 @@
+! foggy_gpu_f -- iso_c_binding module over the C ABI of libfoggy_b200 (include/foggy_gpu.h).
+!
+! It lets the FoggySim driver call the B200 solver in place of the Fortran solve path:
+!   lib_mie_ms_constructor / lib_mie_ms_solver_constructor
+!       (FoggySim/src/lib/mie_theory/lib_mie_multi_sphere.f90:111-150,
+!        lib_mie_ms_solver_interface.f90:91-129)            -> foggy_ms_constructor
+!   lib_mie_ms_solver_run (lib_mie_ms_solver_interface.f90:143-154)
+!                                                           -> foggy_ms_solver_run
+!   lib_mie_ms_solver_calculate_vector_b (:739-783)         -> foggy_ms_calculate_vector_b
+!   lib_mie_ms_solver_get_backward_error (:203-209)         -> foggy_ms_get_backward_error
+! Vectors keep the reference's flat layout (double complex, per sphere [a_nm | b_nm]), so the
+! solution can be handed to lib_mie_ms_solver_set_sphere_parameter_ab_nm_all unchanged.
+!
+! No Fortran compiler exists on the machines this project is built on, so this file has not
+! been compiled; its interfaces are checked by hand against include/foggy_gpu.h.
+module foggy_gpu_f
+    use iso_c_binding
+    implicit none
+    private
+
+    integer(c_int32_t), parameter, public :: FOGGY_OK = 0
+    integer(c_int32_t), parameter, public :: FOGGY_MEM_HOST = 0
+    integer(c_int32_t), parameter, public :: FOGGY_MATVEC_DIRECT = 0
+    integer(c_int32_t), parameter, public :: FOGGY_MATVEC_MLFMM = 1
+
+    type, bind(c), public :: foggy_params
+        real(c_double) :: lambda_0
+        real(c_double) :: n_medium
+        integer(c_int32_t) :: n_range(2)
+        integer(c_int32_t) :: z_coupling
+        integer(c_int32_t) :: reference_row_rule
+        integer(c_int32_t) :: matvec_mode
+        integer(c_int32_t) :: use_initial_guess
+        integer(c_int32_t) :: gmres_restart
+        integer(c_int32_t) :: gmres_max_iterations
+        real(c_double) :: gmres_tolerance
+        integer(c_int32_t) :: tree_l_max
+        integer(c_int32_t) :: tree_s_opt
+        real(c_double) :: fmm_digits
+        integer(c_int64_t) :: device_memory_budget
+    end type foggy_params
+
+    type, bind(c), public :: foggy_stats
+        integer(c_int32_t) :: iterations
+        integer(c_int32_t) :: restarts
+        integer(c_int32_t) :: matvecs
+        integer(c_int32_t) :: status
+        real(c_double) :: backward_error
+        real(c_double) :: ms_total
+        real(c_double) :: ms_matvec
+        real(c_double) :: ms_setup
+        integer(c_int64_t) :: kernel_launches
+    end type foggy_stats
+
+    interface
+        subroutine foggy_default_params(p) bind(c, name="foggy_default_params")
+            import :: foggy_params
+            type(foggy_params), intent(out) :: p
+        end subroutine
+        function foggy_create(p, device, h) result(rc) bind(c, name="foggy_create")
+            import :: foggy_params, c_int32_t, c_ptr
+            type(foggy_params), intent(in) :: p
+            integer(c_int32_t), value :: device
+            type(c_ptr), intent(out) :: h
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_destroy(h) result(rc) bind(c, name="foggy_destroy")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: h
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_set_spheres(h, n, centres, param_index, n_param, refractive_index, radius, n_range) &
+                result(rc) bind(c, name="foggy_set_spheres")
+            import :: c_ptr, c_int32_t, c_double, c_double_complex
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: n, n_param
+            real(c_double), intent(in) :: centres(3, *)
+            integer(c_int32_t), intent(in) :: param_index(*)
+            complex(c_double_complex), intent(in) :: refractive_index(*)
+            real(c_double), intent(in) :: radius(*)
+            integer(c_int32_t), intent(in) :: n_range(2, *)
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_set_plane_waves(h, nw, theta, phi, jones, g, phase, d_0_i) &
+                result(rc) bind(c, name="foggy_set_plane_waves")
+            import :: c_ptr, c_int32_t, c_double, c_double_complex
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: nw
+            real(c_double), intent(in) :: theta(*), phi(*), g(*), phase(*), d_0_i(3, *)
+            complex(c_double_complex), intent(in) :: jones(2, *)
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_vector_length(h) result(n) bind(c, name="foggy_vector_length")
+            import :: c_ptr, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int64_t) :: n
+        end function
+        function foggy_matvec(h, x, y, mem) result(rc) bind(c, name="foggy_matvec")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: h, x, y
+            integer(c_int32_t), value :: mem
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_solve(h, x0, x, mem, stats) result(rc) bind(c, name="foggy_solve")
+            import :: c_ptr, c_int32_t, foggy_stats
+            type(c_ptr), value :: h, x0, x
+            integer(c_int32_t), value :: mem
+            type(foggy_stats), intent(out) :: stats
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_get_backward_error(h) result(e) bind(c, name="foggy_get_backward_error")
+            import :: c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double) :: e
+        end function
+        function foggy_cross_sections(h, x, mem, c_out) result(rc) bind(c, name="foggy_cross_sections")
+            import :: c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h, x
+            integer(c_int32_t), value :: mem
+            real(c_double), intent(out) :: c_out(3)
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_translation_coefficients(x, theta, phi, n_range, nu_range, z_selector, a, b) &
+                result(rc) bind(c, name="foggy_translation_coefficients")
+            import :: c_double, c_int32_t, c_double_complex
+            real(c_double), value :: x, theta, phi
+            integer(c_int32_t), intent(in) :: n_range(2), nu_range(2)
+            integer(c_int32_t), value :: z_selector
+            complex(c_double_complex), intent(out) :: a(*), b(*)
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_wigner_3j(j1, j2, j3, m1, m2, m3) result(w) bind(c, name="foggy_wigner_3j")
+            import :: c_int32_t, c_double
+            integer(c_int32_t), value :: j1, j2, j3, m1, m2, m3
+            real(c_double) :: w
+        end function
+    end interface
+
+    public :: foggy_default_params, foggy_create, foggy_destroy, foggy_set_spheres
+    public :: foggy_set_plane_waves, foggy_vector_length, foggy_matvec, foggy_solve
+    public :: foggy_get_backward_error, foggy_cross_sections, foggy_translation_coefficients
+    public :: foggy_wigner_3j
+    public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
+    public :: foggy_ms_get_backward_error, foggy_ms_destructor
+
+    type(c_ptr), save :: m_handle = c_null_ptr
+
+    contains
+
+        ! Mirrors lib_mie_ms_constructor(n_range, use_ml_fmm, init_with_single_sphere) with the
+        ! scene passed explicitly instead of through simulation_data.
+        subroutine foggy_ms_constructor(p, centres, param_index, refractive_index, radius, n_range_param, &
+                                        theta, phi, jones, g, phase, d_0_i, rc)
+            type(foggy_params), intent(in) :: p
+            real(c_double), intent(in) :: centres(:, :)
+            integer(c_int32_t), intent(in) :: param_index(:)          ! 0-based
+            complex(c_double_complex), intent(in) :: refractive_index(:)
+            real(c_double), intent(in) :: radius(:)
+            integer(c_int32_t), intent(in) :: n_range_param(:, :)
+            real(c_double), intent(in) :: theta(:), phi(:), g(:), phase(:), d_0_i(:, :)
+            complex(c_double_complex), intent(in) :: jones(:, :)
+            integer(c_int32_t), intent(out) :: rc
+            rc = foggy_create(p, 0_c_int32_t, m_handle)
+            if (rc /= FOGGY_OK) return
+            rc = foggy_set_spheres(m_handle, int(size(centres, 2), c_int32_t), centres, param_index, &
+                                   int(size(radius), c_int32_t), refractive_index, radius, n_range_param)
+            if (rc /= FOGGY_OK) return
+            rc = foggy_set_plane_waves(m_handle, int(size(theta), c_int32_t), theta, phi, jones, g, phase, d_0_i)
+        end subroutine
+
+        ! Mirrors lib_mie_ms_solver_run: x receives the solution in the reference layout.
+        subroutine foggy_ms_solver_run(x, stats, rc)
+            complex(c_double_complex), intent(inout), target, contiguous :: x(:)
+            type(foggy_stats), intent(out) :: stats
+            integer(c_int32_t), intent(out) :: rc
+            rc = foggy_solve(m_handle, c_null_ptr, c_loc(x), FOGGY_MEM_HOST, stats)
+        end subroutine
+
+        ! Mirrors lib_mie_ms_solver_calculate_vector_b(vector_x, vector_b).
+        subroutine foggy_ms_calculate_vector_b(vector_x, vector_b, rc)
+            complex(c_double_complex), intent(in), target, contiguous :: vector_x(:)
+            complex(c_double_complex), intent(inout), target, contiguous :: vector_b(:)
+            integer(c_int32_t), intent(out) :: rc
+            rc = foggy_matvec(m_handle, c_loc(vector_x), c_loc(vector_b), FOGGY_MEM_HOST)
+        end subroutine
+
+        function foggy_ms_get_backward_error() result(e)
+            real(c_double) :: e
+            e = foggy_get_backward_error(m_handle)
+        end function
+
+        subroutine foggy_ms_destructor()
+            integer(c_int32_t) :: rc
+            if (c_associated(m_handle)) rc = foggy_destroy(m_handle)
+            m_handle = c_null_ptr
+        end subroutine
+
+end module foggy_gpu_f
