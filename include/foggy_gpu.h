@@ -73,6 +73,11 @@ typedef struct foggy_params {
     int32_t tree_s_opt;          /* elements per leaf for the reference l_max rule (10)     */
     double  fmm_digits;          /* d0 of the per-level order L = kd + 1.8 d0^(2/3) (kd)^(1/3) */
     int64_t device_memory_budget;/* bytes the handle may allocate; 0 = 90% of free memory  */
+    int32_t pair_tables;         /* geometry-only scalar translation coefficients of every sphere
+                                    pair kept in device memory for the solve: 0 = when they fit
+                                    half of the remaining budget, 1 = always, -1 = never (the
+                                    operator rebuilds them on every application)           */
+    int32_t reserved;
 } foggy_params;
 
 /* Per-solve statistics (the reference prints these; here they are returned). */

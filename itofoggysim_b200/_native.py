@@ -54,6 +54,8 @@ class FoggyParams(C.Structure):
         ("tree_s_opt", C.c_int32),
         ("fmm_digits", C.c_double),
         ("device_memory_budget", C.c_int64),
+        ("pair_tables", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

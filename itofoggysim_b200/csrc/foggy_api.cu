@@ -62,6 +62,14 @@ struct foggy_handle_s {
     double* d_gb = nullptr;
     int64_t* d_koff = nullptr;
     double* d_gab = nullptr;
+    int64_t* d_koffS = nullptr;   // scalar Gaunt table (build_scalar_gaunt_qmajor)
+    double* d_gs = nullptr;
+    int gs_nm = 0;
+    // per-pair scalar coaxial coefficients (geometry only), when they fit the memory budget
+    cplx* d_stab = nullptr;
+    int64_t* d_pair_off = nullptr;
+    int stab_z = 0;
+    bool stab_ready = false;
     double* d_sqrt_binom = nullptr;
     double* d_rs = nullptr;
     double* d_irs = nullptr;
@@ -222,7 +230,19 @@ int ensure_tables(foggy_handle h, int pmax) {
     CK(h, cudaMemcpy(h->d_axoff, t.offset.data(), t.offset.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->d_ga, t.ga.data(), t.ga.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->d_gb, t.gb.data(), t.gb.size() * sizeof(double), cudaMemcpyHostToDevice));
-    int K = pmax;
+    int K = pmax + 1;   // the scalar-coefficient relation reads sqrt((nu+1)^2 - k^2) at nu = pmax
+    {
+        std::vector<int64_t> koff;
+        std::vector<double> gs;
+        build_scalar_gaunt_qmajor(pmax + 1, koff, gs);
+        dfree(h, h->d_koffS);
+        dfree(h, h->d_gs);
+        TRY(dalloc(h, &h->d_koffS, koff.size()));
+        TRY(dalloc(h, &h->d_gs, gs.size()));
+        CK(h, cudaMemcpy(h->d_koffS, koff.data(), koff.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+        CK(h, cudaMemcpy(h->d_gs, gs.data(), gs.size() * sizeof(double), cudaMemcpyHostToDevice));
+        h->gs_nm = pmax + 1;
+    }
     std::vector<double> sb((size_t)(K + 1) * (2 * K + 1), 0.0), rs((size_t)(K + 1) * (K + 1), 0.0);
     for (int J = 0; J <= K; ++J)
         for (int m = -J; m <= J; ++m) {
@@ -279,6 +299,8 @@ DirectArgs direct_args(foggy_handle h, const cplx* x) {
     a.ax.koff = h->d_koff;
     a.ax.gab = reinterpret_cast<const double2*>(h->d_gab);
     a.dt = dtabs(h);
+    a.pt.stab = h->stab_ready ? h->d_stab : nullptr;
+    a.pt.pair_off = h->d_pair_off;
     a.z = h->prm.z_coupling;
     a.x = x;
     a.partial = h->d_partial;
@@ -340,10 +362,66 @@ int plan_direct(foggy_handle h) {
     return FOGGY_OK;
 }
 
+// Scalar coaxial coefficients of all unordered sphere pairs (geometry and z only), built once
+// and read by every operator application.  Skipped when they do not fit (pair_tables = 0) or
+// when switched off (pair_tables = -1).
+int ensure_pair_tables(foggy_handle h) {
+    if (h->prm.pair_tables < 0 || h->N < 2) {
+        h->stab_ready = false;
+        return FOGGY_OK;
+    }
+    if (h->stab_ready && h->stab_z == h->prm.z_coupling) return FOGGY_OK;
+    const int64_t npairs = (int64_t)h->N * (h->N - 1) / 2;
+    if (!h->d_stab) {
+        // total size from the counts of each truncation order
+        std::vector<int64_t> cnt(h->pmax + 1, 0);
+        for (int j = 0; j < h->N; ++j) cnt[h->p_s[j]]++;
+        int64_t tot = 0;
+        for (int a = 1; a <= h->pmax; ++a)
+            for (int b = a; b <= h->pmax; ++b) {
+                if (!cnt[a] || !cnt[b]) continue;
+                int64_t pairs = (a == b) ? cnt[a] * (cnt[a] - 1) / 2 : cnt[a] * cnt[b];
+                tot += pairs * pair_block_size(a, b);
+            }
+        size_t bytes = (size_t)tot * sizeof(cplx) + (size_t)npairs * 2 * sizeof(int64_t);
+        size_t room = h->budget > h->bytes_in_use ? h->budget - h->bytes_in_use : 0;
+        if (h->prm.pair_tables == 0 && bytes > room / 2) {
+            h->stab_ready = false;
+            return FOGGY_OK;
+        }
+        TRY(dalloc(h, &h->d_pair_off, npairs + 1));
+        TRY(dalloc(h, &h->d_stab, (size_t)tot));
+        int64_t* d_sizes = nullptr;
+        CK(h, cudaMalloc(&d_sizes, npairs * sizeof(int64_t)));
+        k_pair_sizes<<<h->N, 256, 0, h->stream>>>(scene_view(h), d_sizes);
+        size_t tmp = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_sizes, h->d_pair_off, npairs, h->stream);
+        void* d_tmp = nullptr;
+        cudaError_t e = cudaMalloc(&d_tmp, tmp);
+        if (e == cudaSuccess) {
+            cub::DeviceScan::ExclusiveSum(d_tmp, tmp, d_sizes, h->d_pair_off, npairs, h->stream);
+            e = cudaStreamSynchronize(h->stream);
+        }
+        cudaFree(d_tmp);
+        cudaFree(d_sizes);
+        if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("pair offsets: ") + cudaGetErrorString(e));
+    }
+    SGaunt g{h->d_koffS, h->d_gs, h->gs_nm};
+    int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, (148 * 8 + h->N - 1) / h->N));
+    dim3 grid(h->N, chunks);
+    k_pair_s<<<grid, 256, 0, h->stream>>>(scene_view(h), g, h->prm.z_coupling, h->d_pair_off, h->d_stab, chunks);
+    h->launches += 1;
+    CKL(h);
+    h->stab_ready = true;
+    h->stab_z = h->prm.z_coupling;
+    return FOGGY_OK;
+}
+
 // y = A x in the device layout
 int apply_operator(foggy_handle h, const cplx* x, cplx* y) {
     if (h->prm.matvec_mode != FOGGY_MATVEC_DIRECT)
         return fail(h, FOGGY_ERR_UNSUPPORTED, "matvec_mode: only FOGGY_MATVEC_DIRECT is built");
+    TRY(ensure_pair_tables(h));
     DirectArgs a = direct_args(h, x);
     for (const DirectBucket& b : h->launches_direct) {
         launch_direct(a, b, h->stream);
@@ -393,6 +471,9 @@ void free_scene(foggy_handle h) {
     dfree(h, h->d_b);
     dfree(h, h->d_pq);
     dfree(h, h->d_partial);
+    dfree(h, h->d_stab);
+    dfree(h, h->d_pair_off);
+    h->stab_ready = false;
     dfree(h, h->d_tmp_in);
     dfree(h, h->d_tmp_out);
     dfree(h, h->d_ref_a);
@@ -585,6 +666,7 @@ void foggy_default_params(foggy_params* p) {
     p->tree_s_opt = 10;
     p->fmm_digits = 3.0;
     p->device_memory_budget = 0;
+    p->pair_tables = 0;
 }
 
 static int check_params(foggy_handle h, const foggy_params* p) {

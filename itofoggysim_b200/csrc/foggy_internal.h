@@ -25,6 +25,7 @@ int wigner3j_family(int j1, int j2, int m1, int m2, std::vector<double>& f);
 double wigner3j(int j1, int j2, int j3, int m1, int m2, int m3);
 void build_axial_tables(int pmax, AxialTables& t);
 void build_axial_tables_qmajor(const AxialTables& t, std::vector<int64_t>& koff, std::vector<double>& gab);
+void build_scalar_gaunt_qmajor(int NM, std::vector<int64_t>& koff, std::vector<double>& gs);
 void build_g_table(int pmax, std::vector<double>& g);
 
 // Maximum truncation order of a sphere (the reference caps single spheres at 45,

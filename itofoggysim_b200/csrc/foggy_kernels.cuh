@@ -40,10 +40,39 @@ struct DTabs {
     const double* rj;          // [2j] = 1/(j(j-1)), [2j+1] = 1/((j-1)(2j-1))
     int K;
 };
+// Scalar coaxial coefficients S(k; a, b) of every unordered sphere pair (s < t), computed once
+// per scene and kept in HBM: block of pair u(s, t) = s N - s(s+1)/2 + t - s - 1 at pair_off[u],
+// for k = 0..min(p_s, p_t) a (p_s + 2 - k) x (p_t + 2 - k) grid over a = k..p_s+1 (sphere s)
+// and b = k..p_t+1 (sphere t).
+struct PairTabs {
+    const cplx* stab;          // nullptr: the operator builds its axial coefficients per matvec
+    const int64_t* pair_off;
+};
+struct SGaunt {
+    const int64_t* koff;       // build_scalar_gaunt_qmajor layout
+    const double* gs;
+    int NM;
+};
+__host__ __device__ __forceinline__ int64_t pair_index(int s, int t, int n) {
+    return (int64_t)s * n - (int64_t)s * (s + 1) / 2 + (t - s - 1);
+}
+// sum_{k' < k} (A - k')(B - k')
+__host__ __device__ __forceinline__ int64_t pair_block_offset(int k, int A, int B) {
+    int64_t kk = k;
+    return kk * A * B - (int64_t)(A + B) * kk * (kk - 1) / 2 + (kk - 1) * kk * (2 * kk - 1) / 6;
+}
+__host__ __device__ __forceinline__ int64_t pair_block_size(int ps, int pt) {
+    int km = ps < pt ? ps : pt;
+    return pair_block_offset(km + 1, ps + 2, pt + 2);
+}
+__global__ void k_pair_sizes(SceneView sc, int64_t* sizes);
+__global__ void k_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, cplx* stab, int chunks);
+
 struct DirectArgs {
     SceneView sc;
     AxialView ax;
     DTabs dt;
+    PairTabs pt;
     int z;                     // radial function selector (1 j_n, 2 y_n, 3 h1, 4 h2)
     const cplx* x;             // ragged scaled input
     cplx* partial;             // [slabs][n_unk] partial sums

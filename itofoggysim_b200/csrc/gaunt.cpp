@@ -218,6 +218,42 @@ void build_axial_tables_qmajor(const AxialTables& t, std::vector<int64_t>& koff,
     }
 }
 
+// Scalar coaxial coefficients.  With S(m; a, b) = sum_p i^p (2p+1) (a b p; -m m 0)(a b p; 0 0 0) z_p
+// (p = a + b - 2q) the axial coefficients above are
+//   A(m; n, nu) = pre [2 nu (nu+1) S(m;n,nu) + i kd c1 S(m;n,nu+1) - i kd c2 S(m;n,nu-1)]
+//   B(m; n, nu) = pre 2 i m kd S(m;n,nu)
+//   pre = (-1)^m (2nu+1)/(2n(n+1)), c1 = 2nu sqrt((nu+1)^2-m^2)/(2nu+1), c2 = 2(nu+1) sqrt(nu^2-m^2)/(2nu+1)
+// (the vector-from-scalar translation relation; checked against the 3j sums to rounding).  This
+// table holds (2p+1)(a b p; -m m 0)(a b p; 0 0 0) for m = 0..NM, a, b = m..NM, q = 0..min(a, b),
+// q-major: koff[m] + (q W + (a - m)) W + (b - m), W = NM - m + 1.
+void build_scalar_gaunt_qmajor(int NM, std::vector<int64_t>& koff, std::vector<double>& gs) {
+    koff.assign(NM + 2, 0);
+    int64_t tot = 0;
+    for (int m = 0; m <= NM; ++m) {
+        koff[m] = tot;
+        int W = NM - m + 1;
+        tot += (int64_t)(NM + 1) * W * W;
+    }
+    koff[NM + 1] = tot;
+    gs.assign((size_t)tot, 0.0);
+    std::vector<double> w, w0;
+    for (int m = 0; m <= NM; ++m) {
+        int W = NM - m + 1;
+        for (int a = m; a <= NM; ++a)
+            for (int b = m; b <= NM; ++b) {
+                int jw = wigner3j_family(a, b, -m, m, w);
+                int jw0 = wigner3j_family(a, b, 0, 0, w0);
+                int qm = std::min(a, b);
+                for (int q = 0; q <= qm; ++q) {
+                    int p = a + b - 2 * q;
+                    double W1 = (jw >= 0 && p >= jw && p <= a + b) ? w[p - jw] : 0.0;
+                    double W0 = (jw0 >= 0 && p >= jw0 && p <= a + b) ? w0[p - jw0] : 0.0;
+                    gs[(size_t)koff[m] + ((size_t)q * W + (a - m)) * W + (b - m)] = (2.0 * p + 1.0) * W1 * W0;
+                }
+            }
+    }
+}
+
 // g_nm = (-1)^m sqrt((n+m)!/(n-m)!) for n = 0..pmax, m = -n..n, index n(n+1)+m
 void build_g_table(int pmax, std::vector<double>& g) {
     g.assign((size_t)(pmax + 1) * (pmax + 1), 1.0);

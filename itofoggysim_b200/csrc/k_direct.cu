@@ -216,6 +216,68 @@ __device__ __forceinline__ double d_row(const double* dq, int db, int m, int k) 
 }  // namespace
 
 // ---------------------------------------------------------------------------------------------
+// Scalar coaxial coefficients of the unordered pairs (geometry only; once per scene).
+__global__ void k_pair_sizes(SceneView sc, int64_t* sizes) {
+    int s = blockIdx.x;
+    int ps = sc.p[s];
+    for (int t = s + 1 + threadIdx.x; t < sc.n; t += blockDim.x)
+        sizes[pair_index(s, t, sc.n)] = pair_block_size(ps, sc.p[t]);
+}
+
+// One CTA per (sphere s, chunk c) walks t = s + 1 + c, s + 1 + c + chunks, ...:
+//   S(k; a, b) = sum_q (2p+1)(a b p; -k k 0)(a b p; 0 0 0) i^p z_p(k |d_t - d_s|),  p = a + b - 2q
+__global__ void __launch_bounds__(kThreads) k_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off,
+                                                     cplx* stab, int chunks) {
+    __shared__ double jb[2 * kMaxDegree + 8], yb[2 * kMaxDegree + 8];
+    __shared__ cplx zeta[2 * kMaxDegree + 8];
+    __shared__ double rho_s;
+    const int s = blockIdx.x;
+    const int ps = sc.p[s];
+    const double* cs = sc.centres + 3 * (size_t)s;
+    for (int t = s + 1 + blockIdx.y; t < sc.n; t += chunks) {
+        const int pt = sc.p[t];
+        const int P = ps + pt + 2;
+        if (threadIdx.x == 0) {
+            const double* ct = sc.centres + 3 * (size_t)t;
+            double d0 = sc.k * (ct[0] - cs[0]);
+            double d1 = sc.k * (ct[1] - cs[1]);
+            double d2 = sc.k * (ct[2] - cs[2]);
+            rho_s = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) dev_sph_jn(rho_s, P, jb);
+        if (threadIdx.x == 32 && z != 1) dev_sph_yn(rho_s, P, yb);
+        __syncthreads();
+        for (int p = threadIdx.x; p <= P; p += blockDim.x) zeta[p] = zeta_of(z, p, jb, yb);
+        __syncthreads();
+        cplx* out = stab + pair_off[pair_index(s, t, sc.n)];
+        const int km = min(ps, pt);
+        const int64_t tot = pair_block_size(ps, pt);
+        for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+            // block k: (ps + 2 - k) x (pt + 2 - k)
+            int k = 0;
+            while (k < km && pair_block_offset(k + 1, ps + 2, pt + 2) <= e) ++k;
+            int64_t r = e - pair_block_offset(k, ps + 2, pt + 2);
+            int cols = pt + 2 - k;
+            int aa = k + (int)(r / cols), bb = k + (int)(r % cols);
+            const int W = g.NM - k + 1;
+            const size_t plane = (size_t)W * W;
+            const double* gp = g.gs + g.koff[k] + (size_t)(aa - k) * W + (bb - k);
+            int qm = min(aa, bb);
+            int p = aa + bb;
+            double sx = 0.0, sy = 0.0;
+            for (int q = 0; q <= qm; ++q, p -= 2) {
+                double c = __ldg(gp + q * plane);
+                sx += c * zeta[p].x;
+                sy += c * zeta[p].y;
+            }
+            out[e] = mk(sx, sy);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBucket bk) {
     extern __shared__ double smem_d[];
     const SceneView& sc = a.sc;
@@ -262,8 +324,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBuck
         __syncthreads();
         if (warp == 0) {
             double rho = s.geom[0], phi = s.geom[2];
-            if (lane == 0) dev_sph_jn(rho, P, s.jb);
-            else if (lane == 1 && a.z != 1) dev_sph_yn(rho, P, s.yb);
+            if (!a.pt.stab) {
+                if (lane == 0) dev_sph_jn(rho, P, s.jb);
+                else if (lane == 1 && a.z != 1) dev_sph_yn(rho, P, s.yb);
+            }
             for (int mu = -pq + lane; mu <= pq; mu += 32) {
                 double sn, cs;
                 sincos((double)mu * phi, &sn, &cs);
@@ -299,7 +363,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBuck
             s.x1[t] = e * xl[t];
             s.x1[Pl + t] = e * xl[Pl + t];
         }
-        for (int p = tid; p <= P; p += nthr) s.zeta[p] = zeta_of(a.z, p, s.jb, s.yb);
+        if (!a.pt.stab)
+            for (int p = tid; p <= P; p += nthr) s.zeta[p] = zeta_of(a.z, p, s.jb, s.yb);
         __syncthreads();
         // ---- 3. rotate the source: x'_nu[+-k] = sum_mu d^nu_{mu k} x1_nu[mu] (and partner) ----
         {
@@ -365,6 +430,33 @@ __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBuck
                     int r = t - off;
                     int nnu = pl - lo + 1;
                     int n = lo + r / nnu, nu = lo + r % nnu;
+                    if (a.pt.stab) {
+                        // A, B from the pair's scalar coaxial coefficients S(k; n, nu - 1 .. nu + 1)
+                        const bool jfirst = j < l;
+                        const int s_ = jfirst ? j : l, t_ = jfirst ? l : j;
+                        const int ps = jfirst ? pj : pl, pt = jfirst ? pl : pj;
+                        const cplx* blk = a.pt.stab + a.pt.pair_off[pair_index(s_, t_, sc.n)] +
+                                          pair_block_offset(k, ps + 2, pt + 2);
+                        const int cols = pt + 2 - k;
+                        auto T = [&](int dn, int dnu) {
+                            int ia = jfirst ? dn : dnu, ib = jfirst ? dnu : dn;
+                            return blk[(ia - k) * cols + (ib - k)];
+                        };
+                        cplx S0 = T(n, nu), Sp = T(n, nu + 1);
+                        cplx Sm = (nu - 1 >= k) ? T(n, nu - 1) : mk(0, 0);
+                        const int W = a.dt.K + 1;
+                        const double x = s.geom[0];
+                        double pre = sgn(k) * (2.0 * nu + 1.0) / (2.0 * n * (n + 1.0));
+                        double c0 = 2.0 * nu * (nu + 1.0);
+                        double c1 = x * 2.0 * nu * a.dt.rs[(nu + 1) * W + k] / (2.0 * nu + 1.0);
+                        double c2 = x * 2.0 * (nu + 1.0) * a.dt.rs[nu * W + k] / (2.0 * nu + 1.0);
+                        // A = pre [c0 S0 + i (c1 Sp - c2 Sm)],  B = pre 2 i k x S0
+                        cplx d = c1 * Sp - c2 * Sm;
+                        s.tab[2 * t] = pre * mk(c0 * S0.x - d.y, c0 * S0.y + d.x);
+                        double bk2 = pre * 2.0 * k * x;
+                        s.tab[2 * t + 1] = mk(-bk2 * S0.y, bk2 * S0.x);
+                        continue;
+                    }
                     // q-major 3j table: neighbouring threads read neighbouring (n, nu)
                     const int W = a.ax.pmax - lo + 1;
                     const size_t plane = (size_t)W * W;

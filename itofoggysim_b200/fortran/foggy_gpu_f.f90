@@ -38,6 +38,8 @@ module foggy_gpu_f
         integer(c_int32_t) :: tree_s_opt
         real(c_double) :: fmm_digits
         integer(c_int64_t) :: device_memory_budget
+        integer(c_int32_t) :: pair_tables
+        integer(c_int32_t) :: reserved
     end type foggy_params
 
     type, bind(c), public :: foggy_stats

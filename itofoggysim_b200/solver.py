@@ -22,7 +22,7 @@ import numpy as np
 from . import _native as N
 
 
-def _params(scene, use_ml_fmm=False, init_with_single_sphere=False, memory_budget=0):
+def _params(scene, use_ml_fmm=False, init_with_single_sphere=False, memory_budget=0, pair_tables=0):
     L = N.load()
     p = N.FoggyParams()
     L.foggy_default_params(C.byref(p))
@@ -39,16 +39,18 @@ def _params(scene, use_ml_fmm=False, init_with_single_sphere=False, memory_budge
     p.gmres_tolerance = float(scene.gmres_tolerance)
     p.tree_l_max = int(scene.tree_l_max)
     p.device_memory_budget = int(memory_budget)
+    p.pair_tables = int(pair_tables)
     return p
 
 
 class MultiSphereSolver:
     """lib_mie_ms_constructor + the solver interface, on one GPU."""
 
-    def __init__(self, scene, use_ml_fmm=False, init_with_single_sphere=False, device=0, memory_budget=0):
+    def __init__(self, scene, use_ml_fmm=False, init_with_single_sphere=False, device=0, memory_budget=0,
+                 pair_tables=0):
         self.L = N.load()
         self.scene = scene
-        self.params = _params(scene, use_ml_fmm, init_with_single_sphere, memory_budget)
+        self.params = _params(scene, use_ml_fmm, init_with_single_sphere, memory_budget, pair_tables)
         h = C.c_void_p()
         N.check(self.L.foggy_create(C.byref(self.params), int(device), C.byref(h)))
         self.h = h

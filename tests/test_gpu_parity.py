@@ -147,12 +147,14 @@ MATVEC_CASES = [
 ]
 
 
+@pytest.mark.parametrize("pair_tables", [0, -1])
 @pytest.mark.parametrize("n,p,z,rule,seed", MATVEC_CASES)
-def test_matvec(native, oracle, n, p, z, rule, seed):
+def test_matvec(native, oracle, n, p, z, rule, seed, pair_tables):
+    # pair_tables 0: per-pair scalar coefficients kept in device memory; -1: rebuilt per call
     sc = S.random_cluster(n, seed=seed, p=p, z_coupling=z, reference_row_rule=rule)
     P = oracle.Problem(sc)
     x = random_scaled(sc, seed)
-    with solver.MultiSphereSolver(sc) as s:
+    with solver.MultiSphereSolver(sc, pair_tables=pair_tables) as s:
         y = s.calculate_vector_b(x)
         y2 = s.calculate_vector_b(x)
     yo = P.matvec(x)
