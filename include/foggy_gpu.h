@@ -208,6 +208,32 @@ int32_t foggy_universal_index(int32_t n, const double* points, int32_t l, int64_
  * Call with boxes == NULL to query the count. */
 int32_t foggy_tree_boxes(foggy_handle h, int32_t l, int64_t* boxes, int32_t* count);
 
+/* ---- operator without allocation ------------------------------------------------------- */
+
+/* y = A x for device buffers x, y (reference layout), the direct operator only, with no
+ * device-memory allocation.  This entry point has no counterpart in the reference.
+ *
+ * It serves callers that must not call cudaMalloc once their set-up is done: an outer
+ * iteration (for example an eigen- or time-stepping loop, or another code's Krylov solver)
+ * that runs under a memory pool owning the rest of the GPU, or that has been checked to make
+ * no allocation after warm-up.  foggy_matvec may allocate staging buffers and, on its first
+ * call, the pair coefficient tables; this one only uses what foggy_set_spheres made and a
+ * fixed 32 MiB array of device memory that is part of the library, present on every GPU the
+ * library is loaded on until the process exits.  Pair tables that an earlier foggy_matvec
+ * or foggy_solve built on this handle are read, never built here.
+ *
+ * Limit: the scene's working memory, 16 * n * (2 + b) bytes for n scaled unknowns
+ * (sum over spheres of 2 p (p + 2)) and b truncation-order buckets of 4 degrees, must fit
+ * in 32 MiB; larger scenes return FOGGY_ERR_ARGUMENT and must use foggy_matvec.  Modes other
+ * than FOGGY_MATVEC_DIRECT return FOGGY_ERR_UNSUPPORTED.
+ *
+ * The first call on a GPU looks up the array's device address (cudaGetSymbolAddress) with
+ * that GPU current; make that first call before any stream capture.  All calls on one GPU
+ * share the array, from every handle and thread: calls whose work overlaps on the GPU (other
+ * streams, other threads) race and give wrong results.  The call returns after its work has
+ * finished on the handle's stream. */
+int32_t foggy_matvec_static(foggy_handle h, const double* x, double* y);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1224,3 +1224,68 @@ int32_t foggy_tree_boxes(foggy_handle h, int32_t l, int64_t* boxes, int32_t* cou
 }
 
 }  // extern "C"
+
+// ---- operator without allocation ------------------------------------------------------------
+// Working memory of foggy_matvec_static: the two scaled work vectors and one partial-sum slab
+// per truncation-order bucket.  It is a fixed array in device memory that exists on every GPU
+// this library is loaded on, for the life of the process, and is shared by all calls on that
+// GPU.
+namespace {
+constexpr size_t kStaticScratchBytes = (size_t)32 << 20;   // 32 MiB
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+constexpr int kMaxDevices = 64;
+void* g_static_scratch_ptr[kMaxDevices] = {};
+std::mutex g_static_mu;
+}  // namespace
+
+extern "C" int32_t foggy_matvec_static(foggy_handle h, const double* x, double* y) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!x || !y) return fail(h, FOGGY_ERR_ARGUMENT, "x or y is NULL");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    if (h->prm.matvec_mode != FOGGY_MATVEC_DIRECT)
+        return fail(h, FOGGY_ERR_UNSUPPORTED, "foggy_matvec_static: only the direct operator");
+    if (h->device < 0 || h->device >= kMaxDevices) return fail(h, FOGGY_ERR_ARGUMENT, "device index too large");
+    CK(h, cudaSetDevice(h->device));
+    // the array's device address, looked up once per GPU on the first call there
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_static_mu);
+        if (!g_static_scratch_ptr[h->device]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+            if (e != cudaSuccess)
+                return fail(h, FOGGY_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_static_scratch_ptr[h->device] = p;
+        }
+        base = g_static_scratch_ptr[h->device];
+    }
+    const size_t need = (size_t)h->n_unk * sizeof(cplx) * (2 + (size_t)h->nbuckets);
+    if (need > kStaticScratchBytes)
+        return fail(h, FOGGY_ERR_ARGUMENT,
+                    "foggy_matvec_static: the scene needs " + std::to_string(need) +
+                        " bytes of working memory, above the fixed " + std::to_string(kStaticScratchBytes) +
+                        " (use foggy_matvec)");
+    cplx* xin = reinterpret_cast<cplx*>(base);
+    cplx* yout = xin + h->n_unk;
+    cplx* partial = yout + h->n_unk;
+    // every slab entry that k_direct_finish reads is written by this call's k_direct launches,
+    // so nothing in the array needs clearing first
+    SceneView sv = scene_view(h);
+    const cplx* xr = reinterpret_cast<const cplx*>(x);
+    k_unpack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, xr, xin);
+    DirectArgs a = direct_args(h, xin);
+    a.partial = partial;
+    a.cmax = 1;
+    for (const DirectBucket& b : h->launches_direct) {
+        DirectBucket b1 = b;
+        b1.chunks = 1;
+        b1.slab = b.slab / h->cmax;
+        launch_direct(a, b1, h->stream);
+    }
+    CKL(h);
+    k_direct_finish<<<h->N, 256, 0, h->stream>>>(sv, xin, partial, h->nbuckets, h->n_unk, yout);
+    k_pack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, yout, xr, reinterpret_cast<cplx*>(y));
+    CKL(h);
+    CK(h, cudaStreamSynchronize(h->stream));
+    return FOGGY_OK;
+}
