@@ -74,6 +74,7 @@ struct foggy_handle_s {
     double* d_rs = nullptr;
     double* d_irs = nullptr;
     double* d_rj = nullptr;
+    double* d_delta = nullptr;    // d^j(pi/2), build_delta_table
     int K = 0;
     // operator launches: (target bucket, source bucket) pairs of truncation-order buckets
     std::vector<DirectBucket> launches_direct;
@@ -213,6 +214,7 @@ int ensure_tables(foggy_handle h, int pmax) {
     dfree(h, h->d_irs);
     dfree(h, h->d_rj);
     dfree(h, h->d_g);
+    dfree(h, h->d_delta);
     AxialTables t;
     build_axial_tables(pmax, t);
     TRY(dalloc(h, &h->d_axoff, t.offset.size()));
@@ -270,6 +272,12 @@ int ensure_tables(foggy_handle h, int pmax) {
     CK(h, cudaMemcpy(h->d_rs, rs.data(), rs.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->d_irs, irs.data(), irs.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->d_rj, rj.data(), rj.size() * sizeof(double), cudaMemcpyHostToDevice));
+    {
+        std::vector<double> dl;
+        build_delta_table(pmax, dl);
+        TRY(dalloc(h, &h->d_delta, dl.size()));
+        CK(h, cudaMemcpy(h->d_delta, dl.data(), dl.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     std::vector<double> g;
     build_g_table(pmax, g);
     TRY(dalloc(h, &h->d_g, g.size()));
@@ -292,12 +300,8 @@ DTabs dtabs(foggy_handle h) {
 DirectArgs direct_args(foggy_handle h, const cplx* x) {
     DirectArgs a;
     a.sc = scene_view(h);
-    a.ax.pmax = h->tab_pmax;
-    a.ax.offset = h->d_axoff;
-    a.ax.ga = h->d_ga;
-    a.ax.gb = h->d_gb;
-    a.ax.koff = h->d_koff;
-    a.ax.gab = reinterpret_cast<const double2*>(h->d_gab);
+    a.delta = h->d_delta;
+    a.g = SGaunt{h->d_koffS, h->d_gs, h->gs_nm};
     a.dt = dtabs(h);
     a.pt.stab = h->stab_ready ? h->d_stab : nullptr;
     a.pt.pair_off = h->d_pair_off;
@@ -384,8 +388,10 @@ int ensure_pair_tables(foggy_handle h) {
                 tot += pairs * pair_block_size(a, b);
             }
         size_t bytes = (size_t)tot * sizeof(cplx) + (size_t)npairs * 2 * sizeof(int64_t);
+        // keep room for the Krylov basis of the solve and 4 GiB for everything else
         size_t room = h->budget > h->bytes_in_use ? h->budget - h->bytes_in_use : 0;
-        if (h->prm.pair_tables == 0 && bytes > room / 2) {
+        size_t reserve = (size_t)(h->prm.gmres_restart + 4) * (size_t)h->n_unk * sizeof(cplx) + ((size_t)4 << 30);
+        if (h->prm.pair_tables == 0 && bytes + reserve > room) {
             h->stab_ready = false;
             return FOGGY_OK;
         }
@@ -1092,6 +1098,12 @@ int32_t foggy_translation_coefficients(double x, double theta, double phi, const
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     cudaFree(dA);
     cudaFree(dB);
+    {
+        std::vector<double> dl;
+        build_delta_table(pmax, dl);
+        TRY(dalloc(h, &h->d_delta, dl.size()));
+        CK(h, cudaMemcpy(h->d_delta, dl.data(), dl.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     std::vector<double> g;
     build_g_table(pmax, g);
     foggy_destroy(h);

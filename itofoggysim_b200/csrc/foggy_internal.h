@@ -27,6 +27,7 @@ void build_axial_tables(int pmax, AxialTables& t);
 void build_axial_tables_qmajor(const AxialTables& t, std::vector<int64_t>& koff, std::vector<double>& gab);
 void build_scalar_gaunt_qmajor(int NM, std::vector<int64_t>& koff, std::vector<double>& gs);
 void build_g_table(int pmax, std::vector<double>& g);
+void build_delta_table(int pmax, std::vector<double>& out);
 
 // Maximum truncation order of a sphere (the reference caps single spheres at 45,
 // lib_mie_ss_helper_functions.f90:32).

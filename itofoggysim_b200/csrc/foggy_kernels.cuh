@@ -42,10 +42,10 @@ struct DTabs {
 };
 // Scalar coaxial coefficients S(k; a, b) of every unordered sphere pair (s < t), computed once
 // per scene and kept in HBM: block of pair u(s, t) = s N - s(s+1)/2 + t - s - 1 at pair_off[u],
-// for k = 0..min(p_s, p_t) a (p_s + 2 - k) x (p_t + 2 - k) grid over a = k..p_s+1 (sphere s)
-// and b = k..p_t+1 (sphere t).
+// for k = 0..min(p_s, p_t) a square (M + 2 - k)^2 grid, M = max(p_s, p_t), over a, b = k..M+1,
+// row-major (S is symmetric in a and b).
 struct PairTabs {
-    const cplx* stab;          // nullptr: the operator builds its axial coefficients per matvec
+    const cplx* stab;          // nullptr: the operator sums S from the Gaunt table per matvec
     const int64_t* pair_off;
 };
 struct SGaunt {
@@ -63,15 +63,17 @@ __host__ __device__ __forceinline__ int64_t pair_block_offset(int k, int A, int 
 }
 __host__ __device__ __forceinline__ int64_t pair_block_size(int ps, int pt) {
     int km = ps < pt ? ps : pt;
-    return pair_block_offset(km + 1, ps + 2, pt + 2);
+    int M2 = (ps > pt ? ps : pt) + 2;
+    return pair_block_offset(km + 1, M2, M2);
 }
 __global__ void k_pair_sizes(SceneView sc, int64_t* sizes);
 __global__ void k_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, cplx* stab, int chunks);
 
 struct DirectArgs {
     SceneView sc;
-    AxialView ax;
-    DTabs dt;
+    DTabs dt;                  // rs[j][k] = sqrt(j^2 - k^2) for the coaxial relation
+    const double* delta;       // d^j(pi/2), gaunt.cpp::build_delta_table layout
+    SGaunt g;                  // scalar Gaunt sums (no pair tables)
     PairTabs pt;
     int z;                     // radial function selector (1 j_n, 2 y_n, 3 h1, 4 h2)
     const cplx* x;             // ragged scaled input

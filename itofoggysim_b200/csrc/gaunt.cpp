@@ -254,6 +254,51 @@ void build_scalar_gaunt_qmajor(int NM, std::vector<int64_t>& koff, std::vector<d
     }
 }
 
+// Wigner small-d at a right angle, Delta^j_{ba} = d^j_{ba}(pi/2), for j = 0..pmax and
+// a, b = 0..j, stored a-major: out[delta_offset(j) + a (j + 1) + b], delta_offset(j) =
+// j (j + 1)(2j + 1)/6.  Every rotation of the operator factors through it,
+//   d^j_{m'm}(beta) = i^{m'-m} sum_s Delta^j_{sm'} e^{-i s beta} Delta^j_{sm},
+// and the other three quadrants follow from
+//   Delta_{b,-a} = (-1)^{j+b} Delta_{ba},  Delta_{-b,a} = (-1)^{j+a} Delta_{ba}.
+// Each column (m' >= |m|) is run up in j by the three-term recurrence of the Jacobi polynomials
+// behind d^j_{m'm}, in long double, from d^{m'}_{m'm} = (-1)^{m'-m} sqrt(C(2m', m'+m)) 2^{-m'}.
+void build_delta_table(int pmax, std::vector<double>& out) {
+    auto off = [](int j) { return (size_t)j * (j + 1) * (2 * j + 1) / 6; };
+    out.assign(off(pmax + 1), 0.0);
+    // quarter values d^j_{m'm}, m' >= |m| >= 0 (m >= 0 is all that the table needs)
+    for (int mp = 0; mp <= pmax; ++mp)
+        for (int m = 0; m <= mp; ++m) {
+            long double lc = 0.0L;   // log of sqrt(C(2mp, mp+m)) 2^{-mp}
+            for (int i = 1; i <= 2 * mp; ++i) lc += std::log((long double)i);
+            for (int i = 1; i <= mp + m; ++i) lc -= std::log((long double)i);
+            for (int i = 1; i <= mp - m; ++i) lc -= std::log((long double)i);
+            long double seed = std::exp(0.5L * lc - mp * std::log(2.0L));
+            if ((mp - m) & 1) seed = -seed;
+            long double prev2 = 0.0L, prev1 = seed;
+            for (int j = mp; j <= pmax; ++j) {
+                long double v;
+                if (j == mp) {
+                    v = seed;
+                } else if (j == 1) {
+                    v = 0.0L;   // cos(pi/2) d^0_{00}
+                } else {
+                    long double jj = j;
+                    long double c1 = jj * (2 * jj - 1) / std::sqrt((jj * jj - (long double)m * m) * (jj * jj - (long double)mp * mp));
+                    long double c2 = c1 * std::sqrt(((jj - 1) * (jj - 1) - (long double)m * m) * ((jj - 1) * (jj - 1) - (long double)mp * mp)) /
+                                     ((jj - 1) * (2 * jj - 1));
+                    v = c1 * (-(long double)m * mp / (jj * (jj - 1))) * prev1 - c2 * prev2;
+                }
+                if (j > mp) {
+                    prev2 = prev1;
+                    prev1 = v;
+                }
+                // Delta_{mp, m} (b = mp, a = m) and its mirror Delta_{m, mp} = (-1)^{m - mp} Delta_{mp, m}
+                out[off(j) + (size_t)m * (j + 1) + mp] = (double)v;
+                out[off(j) + (size_t)mp * (j + 1) + m] = (double)(((mp - m) & 1) ? -v : v);
+            }
+        }
+}
+
 // g_nm = (-1)^m sqrt((n+m)!/(n-m)!) for n = 0..pmax, m = -n..n, index n(n+1)+m
 void build_g_table(int pmax, std::vector<double>& g) {
     g.assign((size_t)(pmax + 1) * (pmax + 1), 1.0);
