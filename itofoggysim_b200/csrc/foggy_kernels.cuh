@@ -91,7 +91,7 @@ struct DirectBucket {
     int chunks;                // CTAs per target (<= cmax)
     int pp;                    // largest degree of the launch (sizes shared memory)
 };
-size_t direct_smem_bytes(int pp);
+size_t direct_smem_bytes(int pp, bool tabs);
 size_t translation_pair_smem_bytes(int pmax);
 void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s);
 // y = x + T (sum of the slab partials) for coupled spheres, y = x otherwise

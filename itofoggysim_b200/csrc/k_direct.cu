@@ -57,7 +57,7 @@
 namespace foggy {
 
 namespace {
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;
 
 // offset of degree j in the folded [+ 0..j | - 0..j] layout (2(j+1) entries per degree)
 __host__ __device__ __forceinline__ int off2(int j) { return (j - 1) * (j + 2); }
@@ -69,6 +69,7 @@ __host__ __device__ inline int szAcc(int pp) { return 2 * pp * (pp + 2); }
 __host__ __device__ inline int szZ(int pp) { return 2 * pp + 4; }
 
 struct Bufs {
+    short2* nk;    // [pp (pp + 3) / 2] item u -> (degree, order >= 0)
     cplx* A;       // folded source (1), rotated source x' (3), folded translated field (5)
     cplx* B;       // folded rotated source (2), w (4), folded rotated field (6)
     cplx* acc;     // target accumulator (a | b), standard layout
@@ -80,13 +81,16 @@ struct Bufs {
     double* rho;   // [2]
 };
 
-__host__ __device__ inline size_t smem_bytes(int pp) {
-    size_t c = (size_t)szA(pp) + szB(pp) + szAcc(pp) + 4 * (size_t)(pp + 1) + szZ(pp);
-    size_t d = 4 * (size_t)szZ(pp) + 2;
-    return c * sizeof(cplx) + d * sizeof(double);
+__host__ __device__ inline int szNK(int pp) { return (pp * (pp + 3) / 2 + 3) & ~3; }
+
+// the radial functions and zeta are only kept when S is summed in the kernel (no pair tables)
+__host__ __device__ inline size_t smem_bytes(int pp, bool tabs) {
+    size_t c = (size_t)szA(pp) + szB(pp) + szAcc(pp) + 4 * (size_t)(pp + 1) + (tabs ? 0 : szZ(pp));
+    size_t d = (tabs ? 0 : 4 * (size_t)szZ(pp)) + 2;
+    return c * sizeof(cplx) + d * sizeof(double) + (size_t)szNK(pp) * sizeof(short2);
 }
 
-__device__ inline Bufs carve(double* base, int pp) {
+__device__ inline Bufs carve(double* base, int pp, bool tabs) {
     Bufs s;
     cplx* c = reinterpret_cast<cplx*>(base);
     s.A = c;           c += szA(pp);
@@ -94,17 +98,27 @@ __device__ inline Bufs carve(double* base, int pp) {
     s.acc = c;         c += szAcc(pp);
     s.eps = c;         c += 2 * (pp + 1);
     s.eth = c;         c += 2 * (pp + 1);
-    s.zeta = c;        c += szZ(pp);
+    s.zeta = c;        c += tabs ? 0 : szZ(pp);
     double* d = reinterpret_cast<double*>(c);
-    s.jb = d;          d += 2 * szZ(pp);
-    s.yb = d;          d += 2 * szZ(pp);
-    s.rho = d;
+    s.jb = d;          d += tabs ? 0 : 2 * szZ(pp);
+    s.yb = d;          d += tabs ? 0 : 2 * szZ(pp);
+    s.rho = d;         d += 2;
+    s.nk = reinterpret_cast<short2*>(d);
     return s;
+}
+
+// r += s w in two fused multiply-adds per component
+__device__ __forceinline__ void cmac(double& rx, double& ry, cplx s, cplx w) {
+    rx = fma(s.x, w.x, rx);
+    rx = fma(-s.y, w.y, rx);
+    ry = fma(s.x, w.y, ry);
+    ry = fma(s.y, w.x, ry);
 }
 
 // Geometry of the pair (target j <- source l) and the phase tables of buffer b, spread over
 // fixed threads: tid <= pq the azimuthal phases, 64 <= tid <= 64 + pq the polar ones, 100/101 the
-// Bessel functions (only without pair tables), 127 the distance.
+// Bessel functions (only without pair tables), the last thread the distance; with pair tables,
+// 32..63 prefetch the rows of the pair's coaxial blocks into L2.
 __device__ inline void prep_pair(const DirectArgs& a, const Bufs& s, int j, int l, int pj, int pp, int b, int tid,
                                  bool bessel) {
     const SceneView& sc = a.sc;
@@ -114,6 +128,16 @@ __device__ inline void prep_pair(const DirectArgs& a, const Bufs& s, int j, int 
     const bool e2 = tid >= 64 && tid - 64 <= pq;
     const bool e3 = bessel && (tid == 100 || (tid == 101 && a.z != 1));
     const bool e4 = tid == kThreads - 1;
+    if (!bessel && tid >= 32 && tid < 64) {
+        // rows mu = k..pl+1 of each order's square block, read by the coaxial stage of that pair
+        const int M2 = pq + 2;
+        const cplx* blk = a.pt.stab + a.pt.pair_off[pair_index(min(j, l), max(j, l), sc.n)];
+        for (int k = tid - 32; k <= min(pj, pl); k += 32) {
+            const cplx* rows = blk + pair_block_offset(k, M2, M2);
+            const unsigned bytes = (unsigned)((pl + 2 - k) * (M2 - k) * sizeof(cplx));
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rows), "r"(bytes) : "memory");
+        }
+    }
     if (!(e1 || e2 || e3 || e4)) return;
     const double* cj = sc.centres + 3 * (size_t)j;
     const double* cl = sc.centres + 3 * (size_t)l;
@@ -271,11 +295,12 @@ __global__ void __launch_bounds__(256) k_pair_s(SceneView sc, SGaunt g, int z, c
 }
 
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBucket bk) {
+__global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBucket bk) {
     extern __shared__ __align__(16) double smem_d[];
     const SceneView& sc = a.sc;
     const int pp = bk.pp;
-    const Bufs s = carve(smem_d, pp);
+    const bool tabs = a.pt.stab != nullptr;
+    const Bufs s = carve(smem_d, pp, tabs);
     const int j = bk.targets[blockIdx.x];
     const int c = blockIdx.y;
     if (!sc.couple[j]) return;
@@ -284,9 +309,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBuck
     const int Pj = pj * (pj + 2);
     const int SP = pp * (pp + 3);   // part stride of the folded buffers
     const int XP = pp * (pp + 2);   // part stride of x'
-    const bool tabs = a.pt.stab != nullptr;
     const double* delta = a.delta;
     for (int t = tid; t < 2 * Pj; t += kThreads) s.acc[t] = mk(0, 0);
+    for (int t = tid; t < pp * (pp + 3) / 2; t += kThreads) {
+        int n, k;
+        decode_nk(t, n, k);
+        s.nk[t] = make_short2((short)n, (short)k);
+    }
 
     int i = c;
     if (i < bk.nsources && bk.sources[i] == j) i += bk.chunks;
@@ -307,22 +336,27 @@ __global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBuck
             const cplx* xl = a.x + sc.off[l];
             const int items = pl * (pl + 3) / 2;
             for (int t = tid; t < items; t += kThreads) {
-                int nu, mu;
-                decode_nk(t, nu, mu);
+                const short2 d_ = s.nk[t];
+                const int nu = d_.x, mu = d_.y;
                 const int base = nu * nu - 1 + nu;
                 const cplx e = eps[mu];
                 cplx* U = s.A + off2(nu) + mu;
-#pragma unroll
-                for (int part = 0; part < 2; ++part) {
-                    const cplx up = e * xl[part * Pl + base + mu];
-                    if (mu == 0) {
-                        U[part * SP] = up;
-                        U[part * SP + nu + 1] = up;
-                    } else {
-                        const cplx um = conjg(e) * xl[part * Pl + base - mu];
-                        U[part * SP] = up + um;
-                        U[part * SP + nu + 1] = up - um;
-                    }
+                // the four source entries are all in flight before any use
+                const double2* xv = reinterpret_cast<const double2*>(xl + base);
+                const double2 ap = __ldcg(xv + mu), am = __ldcg(xv - mu);
+                const double2 bp = __ldcg(xv + Pl + mu), bm = __ldcg(xv + Pl - mu);
+                const cplx ua = e * mk(ap.x, ap.y), ub = e * mk(bp.x, bp.y);
+                if (mu == 0) {
+                    U[0] = ua;
+                    U[nu + 1] = ua;
+                    U[SP] = ub;
+                    U[SP + nu + 1] = ub;
+                } else {
+                    const cplx va = conjg(e) * mk(am.x, am.y), vb = conjg(e) * mk(bm.x, bm.y);
+                    U[0] = ua + va;
+                    U[nu + 1] = ua - va;
+                    U[SP] = ub + vb;
+                    U[SP + nu + 1] = ub - vb;
                 }
             }
             if (!tabs) {
@@ -337,8 +371,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBuck
         {
             const int items = pl * (pl + 3) / 2;
             for (int t = tid; t < items; t += kThreads) {
-                int nu, s_;
-                decode_nk(t, nu, s_);
+                const short2 d_ = s.nk[t];
+                const int nu = d_.x, s_ = d_.y;
                 fwd_item(delta, s.A, s.B, SP, nu, s_, nu, eth[s_]);
             }
         }
@@ -347,8 +381,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBuck
         {
             const int items = pl * (pl + 3) / 2;
             for (int t = tid; t < items; t += kThreads) {
-                int nu, k;
-                decode_nk(t, nu, k);
+                const short2 d_ = s.nk[t];
+                const int nu = d_.x, k = d_.y;
                 const int fold = ((nu + k) & 1) ? nu + 1 : 0;
                 const cplx* va = s.B + off2(nu) + fold;
                 cplx Ea, Oa, Eb, Ob;
@@ -431,17 +465,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBuck
                     const int Wk = M2 - k;
                     const cplx* sp = pair_s + pair_block_offset(k, M2, M2) + (n - k);
                     for (int q = 0; q < cnt; ++q) {
-                        const double2 sv = __ldg(reinterpret_cast<const double2*>(sp + q * Wk));
+                        const double2 sv = __ldcg(reinterpret_cast<const double2*>(sp + q * Wk));
                         const cplx S = mk(sv.x, sv.y);
-                        const cplx w0 = w[4 * q], w1 = w[4 * q + 1], w2 = w[4 * q + 2], w3 = w[4 * q + 3];
-                        r0x += S.x * w0.x - S.y * w0.y;
-                        r0y += S.x * w0.y + S.y * w0.x;
-                        r1x += S.x * w1.x - S.y * w1.y;
-                        r1y += S.x * w1.y + S.y * w1.x;
-                        r2x += S.x * w2.x - S.y * w2.y;
-                        r2y += S.x * w2.y + S.y * w2.x;
-                        r3x += S.x * w3.x - S.y * w3.y;
-                        r3y += S.x * w3.y + S.y * w3.x;
+                        cmac(r0x, r0y, S, w[4 * q]);
+                        cmac(r1x, r1y, S, w[4 * q + 1]);
+                        cmac(r2x, r2y, S, w[4 * q + 2]);
+                        cmac(r3x, r3y, S, w[4 * q + 3]);
                     }
                 } else {
                     const int W = a.g.NM - k + 1;
@@ -458,15 +487,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBuck
                             sx += gq * s.zeta[p].x;
                             sy += gq * s.zeta[p].y;
                         }
-                        const cplx w0 = w[4 * q], w1 = w[4 * q + 1], w2 = w[4 * q + 2], w3 = w[4 * q + 3];
-                        r0x += sx * w0.x - sy * w0.y;
-                        r0y += sx * w0.y + sy * w0.x;
-                        r1x += sx * w1.x - sy * w1.y;
-                        r1y += sx * w1.y + sy * w1.x;
-                        r2x += sx * w2.x - sy * w2.y;
-                        r2y += sx * w2.y + sy * w2.x;
-                        r3x += sx * w3.x - sy * w3.y;
-                        r3y += sx * w3.y + sy * w3.x;
+                        const cplx S = mk(sx, sy);
+                        cmac(r0x, r0y, S, w[4 * q]);
+                        cmac(r1x, r1y, S, w[4 * q + 1]);
+                        cmac(r2x, r2y, S, w[4 * q + 2]);
+                        cmac(r3x, r3y, S, w[4 * q + 3]);
                     }
                 }
                 const double f = sgn(k) / (2.0 * n * (n + 1.0));
@@ -492,8 +517,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBuck
         {
             const int items = pj * (pj + 3) / 2;
             for (int t = tid; t < items; t += kThreads) {
-                int n, s_;
-                decode_nk(t, n, s_);
+                const short2 d_ = s.nk[t];
+                const int n = d_.x, s_ = d_.y;
                 fwd_item(delta, s.A, s.B, SP, n, s_, min(n, kmax), eth[s_]);
             }
         }
@@ -502,8 +527,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBuck
         {
             const int items = pj * (pj + 3) / 2;
             for (int t = tid; t < items; t += kThreads) {
-                int n, m;
-                decode_nk(t, n, m);
+                const short2 d_ = s.nk[t];
+                const int n = d_.x, m = d_.y;
                 const int fold = ((n + m) & 1) ? n + 1 : 0;
                 const cplx* va = s.B + off2(n) + fold;
                 cplx Ea, Oa, Eb, Ob;
@@ -534,10 +559,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_direct(DirectArgs a, DirectBuck
         }
 }
 
-size_t direct_smem_bytes(int pp) { return smem_bytes(pp); }
+size_t direct_smem_bytes(int pp, bool tabs) { return smem_bytes(pp, tabs); }
 
 void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s) {
-    size_t smem = direct_smem_bytes(b.pp);
+    size_t smem = direct_smem_bytes(b.pp, a.pt.stab != nullptr);
     dim3 grid(b.ntargets, b.chunks);
     cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_direct<<<grid, kThreads, smem, s>>>(a, b);
