@@ -71,12 +71,23 @@ typedef struct foggy_params {
     double  gmres_tolerance;     /* stop when ||b - A x|| / ||b|| <= tolerance              */
     int32_t tree_l_max;          /* 0: reference rule from tree_s_opt; > 0: fixed deepest level */
     int32_t tree_s_opt;          /* elements per leaf for the reference l_max rule (10)     */
-    double  fmm_digits;          /* d0 of the per-level order L = kd + 1.8 d0^(2/3) (kd)^(1/3) */
+    double  fmm_digits;          /* not used: the ML-FMM expands every box to the global order,
+                                    as the reference does                                  */
     int64_t device_memory_budget;/* bytes the handle may allocate; 0 = 90% of free memory  */
     int32_t pair_tables;         /* geometry-only scalar translation coefficients of every sphere
                                     pair kept in device memory for the solve: 0 = when they fit
-                                    half of the remaining budget, 1 = always, -1 = never (the
-                                    operator rebuilds them on every application)           */
+                                    beside the Krylov basis, 1 = always, -1 = never (the
+                                    operator sums them on every application)               */
+    int32_t fmm_convention;      /* ML-FMM translations: 0 = as the reference writes them
+                                    (lib_mie_ms_ml_fmm_interface.f90:259-981: z_coupling for
+                                    every box translation, box-to-sphere with
+                                    z_translation_gt_r, its displacement signs, and the
+                                    box-to-sphere offset of lib_tree_get_unscaled_point);
+                                    1 = consistent expansion (regular translations up and down
+                                    the tree, z_coupling across the interaction lists), which
+                                    tends to the direct operator as the order grows        */
+    int32_t z_translation_gt_r;  /* radial function of the box-to-sphere step in convention 0
+                                    (the reference's tests set 3)                          */
     int32_t reserved;
 } foggy_params;
 
@@ -207,6 +218,14 @@ int32_t foggy_universal_index(int32_t n, const double* points, int32_t l, int64_
  * (lib_ml_fmm_hf_create_hierarchy, libmlfmm/src/lib/lib_ml_fmm_helper_functions.f90:366-457).
  * Call with boxes == NULL to query the count. */
 int32_t foggy_tree_boxes(foggy_handle h, int32_t l, int64_t* boxes, int32_t* count);
+
+/* Octree lists of box n at level l for the ML-FMM: kind 1 -> E1, the spheres in the box
+ * (lib_tree_get_domain_e1, libtree/src/lib/lib_tree.f90:492-609); kind 2 -> E2, the spheres in
+ * the box and its neighbours (lib_tree_get_domain_e2, :611-724); kind 4 -> I4, the level-l box
+ * indices of the interaction list, every candidate inside the domain (lib_tree_get_domain_i4,
+ * :994-1143).  Spheres are 0-based input indices in key order, boxes ascending.  Call with
+ * out == NULL to query the count. */
+int32_t foggy_tree_domain(foggy_handle h, int32_t l, int64_t n, int32_t kind, int64_t* out, int32_t* count);
 
 /* ---- operator without allocation ------------------------------------------------------- */
 

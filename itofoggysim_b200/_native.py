@@ -34,7 +34,7 @@ EXPORTS = [
     "foggy_set_spheres", "foggy_set_plane_waves", "foggy_vector_length", "foggy_get_mie_coefficients",
     "foggy_get_vector_b", "foggy_matvec", "foggy_solve", "foggy_get_backward_error",
     "foggy_cross_sections", "foggy_translation_coefficients", "foggy_wigner_3j", "foggy_build_tree",
-    "foggy_universal_index", "foggy_tree_boxes", "foggy_matvec_static",
+    "foggy_universal_index", "foggy_tree_boxes", "foggy_matvec_static", "foggy_tree_domain",
 ]
 
 
@@ -55,6 +55,8 @@ class FoggyParams(C.Structure):
         ("fmm_digits", C.c_double),
         ("device_memory_budget", C.c_int64),
         ("pair_tables", C.c_int32),
+        ("fmm_convention", C.c_int32),
+        ("z_translation_gt_r", C.c_int32),
         ("reserved", C.c_int32),
     ]
 
@@ -119,6 +121,7 @@ def load():
         "foggy_universal_index": (i32, [i32, pd, i32, pi64]),
         "foggy_tree_boxes": (i32, [vp, i32, pi64, pi32]),
         "foggy_matvec_static": (i32, [vp, vp, vp]),
+        "foggy_tree_domain": (i32, [vp, i32, i64, i32, pi64, pi32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -121,6 +121,19 @@ struct foggy_handle_s {
     int* d_idx_sorted = nullptr;
     int tree_lmax = 0, tree_lmin = 0;
     bool tree_ready = false;
+    // ML-FMM: octree lists, box coefficients, final-summation slabs
+    bool fmm_ready = false;
+    FmmTree fmm;
+    double fmm_xmin[3] = {0, 0, 0};
+    double* d_fmm_c = nullptr;       // box centres
+    int* d_fmm_p = nullptr;          // box orders (the global order)
+    int64_t* d_fmm_off = nullptr;    // box coefficient offsets
+    cplx* d_fmm_C = nullptr;         // outgoing coefficients of every box
+    cplx* d_fmm_D = nullptr;         // incoming coefficients of every box
+    int* d_fmm_list = nullptr;       // CSR lists of the passes, concatenated
+    int fmm_lofs[12] = {0};          // offsets of (ptr, idx) of: aggregation, children, I4, parent,
+                                     // box-to-sphere, near field
+    cplx* d_fmm_slab = nullptr;      // box-to-sphere and near-field sums, 2 x n_unk
 };
 
 namespace {
@@ -423,10 +436,210 @@ int ensure_pair_tables(foggy_handle h) {
     return FOGGY_OK;
 }
 
+// ---- ML-FMM (lib_ml_fmm_run, libmlfmm/src/lib/lib_ml_fmm.f90:231-262) ---------------------------
+int build_tree_dev(foggy_handle h) {
+    if (h->tree_ready) return FOGGY_OK;
+    int n = h->N;
+    if (!h->d_keys) {
+        TRY(dalloc(h, &h->d_keys, n));
+        TRY(dalloc(h, &h->d_idx, n));
+        TRY(dalloc(h, &h->d_keys_sorted, n));
+        TRY(dalloc(h, &h->d_idx_sorted, n));
+    }
+    double* d_mm = nullptr;
+    int* d_lmax = nullptr;
+    CK(h, cudaMalloc(&d_mm, 6 * sizeof(double)));
+    CK(h, cudaMalloc(&d_lmax, sizeof(int)));
+    k_minmax<<<1, 256, 0, h->stream>>>(n, h->d_centres, d_mm);
+    k_morton<<<(n + 255) / 256, 256, 0, h->stream>>>(n, h->d_centres, d_mm, h->d_keys, h->d_idx);
+    size_t tmp_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, h->d_keys, h->d_keys_sorted, h->d_idx, h->d_idx_sorted, n, 0,
+                                    63, h->stream);
+    void* d_tmp = nullptr;
+    CK(h, cudaMalloc(&d_tmp, tmp_bytes));
+    cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, h->d_keys, h->d_keys_sorted, h->d_idx, h->d_idx_sorted, n, 0,
+                                    63, h->stream);
+    int one = 1;
+    CK(h, cudaMemcpyAsync(d_lmax, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    int s = std::max(1, h->prm.tree_s_opt);
+    if (n > s) k_level_max<<<(n + 255) / 256, 256, 0, h->stream>>>(n, s, h->d_keys_sorted, d_lmax);
+    int lmax = 1;
+    cudaError_t e = cudaMemcpyAsync(&lmax, d_lmax, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_tmp);
+    cudaFree(d_mm);
+    cudaFree(d_lmax);
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("tree: ") + cudaGetErrorString(e));
+    CKL(h);
+    // l_min = 1 + floor(log(k + 1) / log(2)) for k = 1 (lib_tree.f90:1162-1170)
+    h->tree_lmin = (int)(1 + std::floor(std::log(2.0f) / std::log(2.0f)));
+    h->tree_lmax = h->prm.tree_l_max > 0 ? h->prm.tree_l_max : lmax;
+    h->tree_ready = true;
+    return FOGGY_OK;
+}
+
+
+void free_fmm(foggy_handle h) {
+    dfree(h, h->d_fmm_c);
+    dfree(h, h->d_fmm_p);
+    dfree(h, h->d_fmm_off);
+    dfree(h, h->d_fmm_C);
+    dfree(h, h->d_fmm_D);
+    dfree(h, h->d_fmm_list);
+    dfree(h, h->d_fmm_slab);
+    h->fmm = FmmTree();
+    h->fmm_ready = false;
+}
+
+// Octree lists (host) and box storage (device) of the current scene and tree parameters.
+int ensure_fmm(foggy_handle h) {
+    if (h->fmm_ready) return FOGGY_OK;
+    free_fmm(h);
+    // boxes carry the global order, which may exceed every sphere's
+    TRY(ensure_tables(h, std::max(h->pg, 1)));
+    TRY(build_tree_dev(h));
+    const int n = h->N;
+    std::vector<unsigned long long> keys(n);
+    std::vector<int> order(n);
+    CK(h, cudaMemcpy(keys.data(), h->d_keys_sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    CK(h, cudaMemcpy(order.data(), h->d_idx_sorted, n * sizeof(int), cudaMemcpyDeviceToHost));
+    FmmTree& t = h->fmm;
+    build_fmm_tree(n, reinterpret_cast<const uint64_t*>(keys.data()), order.data(), h->tree_lmin, h->tree_lmax, t);
+    // the reference's scaling (lib_tree_get_scaled_element_list, lib_tree.f90:320-374)
+    double D = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        double lo = h->centres[d], hi = h->centres[d];
+        for (int i = 1; i < n; ++i) {
+            lo = std::min(lo, h->centres[3 * (size_t)i + d]);
+            hi = std::max(hi, h->centres[3 * (size_t)i + d]);
+        }
+        h->fmm_xmin[d] = lo;
+        D = std::max(D, (hi - lo) * (1.0 + std::ldexp(1.0, -52)));
+    }
+    const int nbox = (int)t.box_n.size();
+    const int nlev = t.lmax - t.lmin + 1;
+    const int leaf0 = t.level_base[nlev - 1], nleaf = nbox - leaf0;
+    const int Pg = h->pg * (h->pg + 2);
+    std::vector<double> bc(3 * (size_t)nbox);
+    std::vector<int> bp(nbox, h->pg);
+    std::vector<int64_t> bo(nbox);
+    for (int b = 0; b < nbox; ++b) {
+        box_centre(t.box_n[b], t.box_level[b], &bc[3 * (size_t)b]);
+        for (int d = 0; d < 3; ++d) bc[3 * (size_t)b + d] = bc[3 * (size_t)b + d] * D + h->fmm_xmin[d];
+        bo[b] = (int64_t)b * 2 * Pg;
+    }
+    // lists: aggregation (leaf <- its spheres; under the row rule only spheres of the global order
+    // contribute), children, I4, parent, box-to-sphere (sphere <- its leaf), near field
+    // (sphere <- E2 of its leaf without itself)
+    std::vector<int> agg_ptr(nleaf + 1, 0), agg_idx, par_ptr(nbox + 1, 0), par_idx, dor_ptr(n + 1), dor_idx(n),
+        near_ptr(n + 1, 0), near_idx;
+    for (int q = 0; q < nleaf; ++q) {
+        for (int e = t.e1_ptr[q]; e < t.e1_ptr[q + 1]; ++e)
+            if (h->couple[t.e1_idx[e]]) agg_idx.push_back(t.e1_idx[e]);
+        agg_ptr[q + 1] = (int)agg_idx.size();
+    }
+    for (int b = 0; b < nbox; ++b) {
+        if (t.parent[b] >= 0) par_idx.push_back(t.parent[b]);
+        par_ptr[b + 1] = (int)par_idx.size();
+    }
+    for (int j = 0; j < n; ++j) {
+        dor_ptr[j] = j;
+        dor_idx[j] = t.leaf_of[j];
+        const int q = t.leaf_of[j] - leaf0;
+        for (int e = t.e2_ptr[q]; e < t.e2_ptr[q + 1]; ++e)
+            if (t.e2_idx[e] != j) near_idx.push_back(t.e2_idx[e]);
+        near_ptr[j + 1] = (int)near_idx.size();
+    }
+    dor_ptr[n] = n;
+    const std::vector<int>* parts[12] = {&agg_ptr, &agg_idx, &t.child_ptr, &t.child_idx, &t.i4_ptr, &t.i4_idx,
+                                         &par_ptr, &par_idx, &dor_ptr, &dor_idx, &near_ptr, &near_idx};
+    std::vector<int> all;
+    for (int i = 0; i < 12; ++i) {
+        h->fmm_lofs[i] = (int)all.size();
+        all.insert(all.end(), parts[i]->begin(), parts[i]->end());
+    }
+    all.push_back(0);
+    TRY(dalloc(h, &h->d_fmm_list, all.size()));
+    TRY(dalloc(h, &h->d_fmm_c, bc.size()));
+    TRY(dalloc(h, &h->d_fmm_p, bp.size()));
+    TRY(dalloc(h, &h->d_fmm_off, bo.size()));
+    TRY(dalloc(h, &h->d_fmm_C, (size_t)nbox * 2 * Pg));
+    TRY(dalloc(h, &h->d_fmm_D, (size_t)nbox * 2 * Pg));
+    TRY(dalloc(h, &h->d_fmm_slab, 2 * (size_t)h->n_unk));
+    CK(h, cudaMemcpy(h->d_fmm_list, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_fmm_c, bc.data(), bc.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_fmm_p, bp.data(), bp.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_fmm_off, bo.data(), bo.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+    h->fmm_ready = true;
+    return FOGGY_OK;
+}
+
+// y = A x by the ML-FMM passes (upward :387-640, downward :656-982, final summation :994-1204;
+// the Mie handles lib_mie_ms_ml_fmm_interface.f90:259-981), in the device layout.
+int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
+    TRY(ensure_fmm(h));
+    const FmmTree& t = h->fmm;
+    const int conv = h->prm.fmm_convention;
+    const int zi = h->prm.z_coupling;
+    const int z_reg = conv == 0 ? zi : 1;                            // aggregation, M2M, L2L
+    const int z_dor = conv == 0 ? h->prm.z_translation_gt_r : 1;     // box to sphere
+    const double sts = conv == 0 ? -1.0 : 1.0;                       // aggregation, M2L, box to sphere
+    const int nlev = t.lmax - t.lmin + 1;
+    const int nbox = (int)t.box_n.size();
+    const int leaf0 = t.level_base[nlev - 1];
+    const int* L = h->d_fmm_list;
+    const int* lo = h->fmm_lofs;
+    SceneView sv = scene_view(h);
+    TransArgs base{};
+    base.delta = h->d_delta;
+    base.dt = dtabs(h);
+    base.g = SGaunt{h->d_koffS, h->d_gs, h->gs_nm};
+    base.k = sv.k;
+    base.pp = h->pg;
+    const PointSet S{h->d_centres, h->d_p, h->d_off};
+    const PointSet B{h->d_fmm_c, h->d_fmm_p, h->d_fmm_off};
+    auto pass = [&](PointSet tg, PointSet sr, const cplx* in, cplx* out, int lp, int li, int tbase, int ntgt,
+                    double sign, int z, int add, bool shift) {
+        TransArgs a = base;
+        a.tgt = tg;
+        a.src = sr;
+        a.x = in;
+        a.out = out;
+        a.lptr = L + lo[lp] + (lp == 0 || lp >= 8 ? 0 : tbase);
+        a.lidx = L + lo[li];
+        a.tbase = tbase;
+        a.sign = sign;
+        for (int d = 0; d < 3; ++d) a.sh[d] = shift ? h->fmm_xmin[d] : 0.0;
+        a.z = z;
+        a.add = add;
+        launch_translate(a, ntgt, h->stream);
+        if (ntgt > 0) h->launches += 1;
+    };
+    // upward: aggregation at the leaves, then M2M level by level
+    pass(B, S, x, h->d_fmm_C, 0, 1, leaf0, nbox - leaf0, sts, z_reg, 0, false);
+    for (int li = nlev - 2; li >= 0; --li)
+        pass(B, B, h->d_fmm_C, h->d_fmm_C, 2, 3, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
+             z_reg, 0, false);
+    // downward: M2L on every level, then L2L from the coarsest level down
+    for (int li = 0; li < nlev; ++li)
+        pass(B, B, h->d_fmm_C, h->d_fmm_D, 4, 5, t.level_base[li], t.level_base[li + 1] - t.level_base[li], sts, zi,
+             0, false);
+    for (int li = 1; li < nlev; ++li)
+        pass(B, B, h->d_fmm_D, h->d_fmm_D, 6, 7, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
+             z_reg, 1, false);
+    // final summation: box to sphere, near field, then y = x + T (both)
+    pass(S, B, h->d_fmm_D, h->d_fmm_slab, 8, 9, 0, h->N, sts, z_dor, 0, conv == 0);
+    pass(S, S, x, h->d_fmm_slab + h->n_unk, 10, 11, 0, h->N, 1.0, zi, 0, false);
+    CKL(h);
+    k_direct_finish<<<h->N, 256, 0, h->stream>>>(sv, x, h->d_fmm_slab, 2, h->n_unk, y);
+    h->launches += 1;
+    CKL(h);
+    return FOGGY_OK;
+}
+
 // y = A x in the device layout
 int apply_operator(foggy_handle h, const cplx* x, cplx* y) {
-    if (h->prm.matvec_mode != FOGGY_MATVEC_DIRECT)
-        return fail(h, FOGGY_ERR_UNSUPPORTED, "matvec_mode: only FOGGY_MATVEC_DIRECT is built");
+    if (h->prm.matvec_mode == FOGGY_MATVEC_MLFMM) return apply_operator_fmm(h, x, y);
     TRY(ensure_pair_tables(h));
     DirectArgs a = direct_args(h, x);
     for (const DirectBucket& b : h->launches_direct) {
@@ -495,6 +708,7 @@ void free_scene(foggy_handle h) {
     h->ws_restart = 0;
     h->tree_ready = false;
     h->rhs_ready = false;
+    free_fmm(h);
 }
 
 int ensure_workspace(foggy_handle h, int restart) {
@@ -673,6 +887,8 @@ void foggy_default_params(foggy_params* p) {
     p->fmm_digits = 3.0;
     p->device_memory_budget = 0;
     p->pair_tables = 0;
+    p->fmm_convention = 0;
+    p->z_translation_gt_r = 3;
 }
 
 static int check_params(foggy_handle h, const foggy_params* p) {
@@ -687,6 +903,10 @@ static int check_params(foggy_handle h, const foggy_params* p) {
     if (!(p->gmres_tolerance > 0)) return fail(h, FOGGY_ERR_ARGUMENT, "gmres_tolerance must be > 0");
     if (p->matvec_mode != FOGGY_MATVEC_DIRECT && p->matvec_mode != FOGGY_MATVEC_MLFMM)
         return fail(h, FOGGY_ERR_ARGUMENT, "matvec_mode");
+    if (p->fmm_convention != 0 && p->fmm_convention != 1)
+        return fail(h, FOGGY_ERR_ARGUMENT, "fmm_convention must be 0 or 1");
+    if (p->z_translation_gt_r < 1 || p->z_translation_gt_r > 4)
+        return fail(h, FOGGY_ERR_ARGUMENT, "z_translation_gt_r must be 1..4");
     return FOGGY_OK;
 }
 
@@ -746,6 +966,10 @@ int32_t foggy_set_params(foggy_handle h, const foggy_params* params) {
                         params->reference_row_rule != h->prm.reference_row_rule;
     foggy_params old = h->prm;
     h->prm = *params;
+    if (params->tree_l_max != old.tree_l_max || params->tree_s_opt != old.tree_s_opt) {
+        h->tree_ready = false;
+        free_fmm(h);
+    }
     if (scene_change && h->N > 0) {
         // rebuild the scene with the new global settings
         std::vector<double> c = h->centres, mr, rad = h->radius;
@@ -1127,47 +1351,6 @@ int32_t foggy_translation_coefficients(double x, double theta, double phi, const
 }
 
 // ---- octree -------------------------------------------------------------------------------
-static int build_tree_dev(foggy_handle h) {
-    if (h->tree_ready) return FOGGY_OK;
-    int n = h->N;
-    if (!h->d_keys) {
-        TRY(dalloc(h, &h->d_keys, n));
-        TRY(dalloc(h, &h->d_idx, n));
-        TRY(dalloc(h, &h->d_keys_sorted, n));
-        TRY(dalloc(h, &h->d_idx_sorted, n));
-    }
-    double* d_mm = nullptr;
-    int* d_lmax = nullptr;
-    CK(h, cudaMalloc(&d_mm, 6 * sizeof(double)));
-    CK(h, cudaMalloc(&d_lmax, sizeof(int)));
-    k_minmax<<<1, 256, 0, h->stream>>>(n, h->d_centres, d_mm);
-    k_morton<<<(n + 255) / 256, 256, 0, h->stream>>>(n, h->d_centres, d_mm, h->d_keys, h->d_idx);
-    size_t tmp_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, h->d_keys, h->d_keys_sorted, h->d_idx, h->d_idx_sorted, n, 0,
-                                    63, h->stream);
-    void* d_tmp = nullptr;
-    CK(h, cudaMalloc(&d_tmp, tmp_bytes));
-    cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, h->d_keys, h->d_keys_sorted, h->d_idx, h->d_idx_sorted, n, 0,
-                                    63, h->stream);
-    int one = 1;
-    CK(h, cudaMemcpyAsync(d_lmax, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    int s = std::max(1, h->prm.tree_s_opt);
-    if (n > s) k_level_max<<<(n + 255) / 256, 256, 0, h->stream>>>(n, s, h->d_keys_sorted, d_lmax);
-    int lmax = 1;
-    cudaError_t e = cudaMemcpyAsync(&lmax, d_lmax, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(d_tmp);
-    cudaFree(d_mm);
-    cudaFree(d_lmax);
-    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("tree: ") + cudaGetErrorString(e));
-    CKL(h);
-    // l_min = 1 + floor(log(k + 1) / log(2)) for k = 1 (lib_tree.f90:1162-1170)
-    h->tree_lmin = (int)(1 + std::floor(std::log(2.0f) / std::log(2.0f)));
-    h->tree_lmax = h->prm.tree_l_max > 0 ? h->prm.tree_l_max : lmax;
-    h->tree_ready = true;
-    return FOGGY_OK;
-}
-
 int32_t foggy_build_tree(foggy_handle h, int64_t* uindex_out, int32_t* order_out, int32_t* l_min_out,
                          int32_t* l_max_out) {
     if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
@@ -1232,6 +1415,41 @@ int32_t foggy_tree_boxes(foggy_handle h, int32_t l, int64_t* boxes, int32_t* cou
         std::copy(u.begin(), u.end(), boxes);
     }
     *count = (int)u.size();
+    return FOGGY_OK;
+}
+
+int32_t foggy_tree_domain(foggy_handle h, int32_t l, int64_t n, int32_t kind, int64_t* out, int32_t* count) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!count) return fail(h, FOGGY_ERR_ARGUMENT, "count is NULL");
+    if (l < 0 || l > 21) return fail(h, FOGGY_ERR_ARGUMENT, "level must be 0..21");
+    if (n < 0 || (l < 21 && n >= ((int64_t)1 << (3 * l)))) return fail(h, FOGGY_ERR_ARGUMENT, "box index out of range");
+    if (kind != 1 && kind != 2 && kind != 4) return fail(h, FOGGY_ERR_ARGUMENT, "kind must be 1 (E1), 2 (E2) or 4 (I4)");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    CK(h, cudaSetDevice(h->device));
+    std::vector<int64_t> v;
+    if (kind == 4) {
+        tree_i4(n, l, v);
+    } else {
+        TRY(build_tree_dev(h));
+        const int N = h->N;
+        std::vector<unsigned long long> ks(N);
+        std::vector<int> is(N);
+        CK(h, cudaMemcpy(ks.data(), h->d_keys_sorted, N * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        CK(h, cudaMemcpy(is.data(), h->d_idx_sorted, N * sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<int64_t> boxes;
+        if (kind == 1) boxes.push_back(n);
+        else tree_i2(n, l, boxes);
+        std::sort(boxes.begin(), boxes.end());
+        const int sh = 3 * (21 - l);
+        for (int64_t b : boxes)
+            for (int i = 0; i < N; ++i)
+                if ((int64_t)(ks[i] >> sh) == b) v.push_back(is[i]);
+    }
+    if (out) {
+        if (*count < (int)v.size()) return fail(h, FOGGY_ERR_ARGUMENT, "out buffer too small");
+        std::copy(v.begin(), v.end(), out);
+    }
+    *count = (int)v.size();
     return FOGGY_OK;
 }
 

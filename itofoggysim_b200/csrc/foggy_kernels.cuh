@@ -97,6 +97,30 @@ void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s);
 // y = x + T (sum of the slab partials) for coupled spheres, y = x otherwise
 __global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial, int slabs, int64_t n_unk,
                                 cplx* y);
+// Sphere or box centres with their truncation orders and the offsets of their coefficient
+// vectors (scaled basis, a then b, standard (n, m) order).
+struct PointSet {
+    const double* c;
+    const int* p;
+    const int64_t* off;
+};
+// One ML-FMM pass: targets tbase .. tbase + n - 1 of tgt, target tbase + b translating its sources
+// lidx[lptr[b] .. lptr[b+1]) of src by t = k (sign (c_src - c_tgt) + sh) with radial function z;
+// the result is written to (add = 0) or added onto (add = 1) out + tgt.off[target].
+struct TransArgs {
+    PointSet tgt, src;
+    const cplx* x;
+    cplx* out;
+    const int* lptr;
+    const int* lidx;
+    int tbase;
+    double k, sign, sh[3];
+    int z, add, pp;
+    const double* delta;
+    DTabs dt;
+    SGaunt g;
+};
+void launch_translate(const TransArgs& a, int ntargets, cudaStream_t s);
 // single-pair translation for the parity entry point: A, B blocks in the scaled basis
 __global__ void k_translation_pair(AxialView ax, DTabs dt, double x, double theta, double phi, int pn, int pnu,
                                    int z, cplx* A, cplx* B);

@@ -115,35 +115,40 @@ __device__ __forceinline__ void cmac(double& rx, double& ry, cplx s, cplx w) {
     ry = fma(s.y, w.x, ry);
 }
 
-// Geometry of the pair (target j <- source l) and the phase tables of buffer b, spread over
-// fixed threads: tid <= pq the azimuthal phases, 64 <= tid <= 64 + pq the polar ones, 100/101 the
-// Bessel functions (only without pair tables), the last thread the distance; with pair tables,
-// 32..63 prefetch the rows of the pair's coaxial blocks into L2.
-__device__ inline void prep_pair(const DirectArgs& a, const Bufs& s, int j, int l, int pj, int pp, int b, int tid,
-                                 bool bessel) {
-    const SceneView& sc = a.sc;
-    const int pl = sc.p[l];
+// Where a translation points: t = k (sign (c_src - c_tgt) + shift).  The direct operator uses
+// sign = 1, shift = 0 (t = k (d_l - d_j), the reference's d_j_l); the ML-FMM passes follow the
+// reference's own choices per pass.
+struct Disp {
+    const double* ct;   // target centre
+    const double* cs;   // source centre
+    double k, sign;
+    double sh[3];
+};
+
+// Geometry of one translation and the phase tables of buffer b, spread over fixed threads:
+// tid <= pq the azimuthal phases, 64 <= tid <= 64 + pq the polar ones, 100/101 the Bessel
+// functions (only without pair tables), the last thread the distance; with a coaxial block
+// (sblock), 32..63 prefetch its rows into L2.
+__device__ inline void prep_pair(const Bufs& s, const Disp& g, int z, const cplx* sblock, int pj, int pl, int pp,
+                                 int b, int tid, bool bessel) {
     const int pq = max(pj, pl);
     const bool e1 = tid <= pq;
     const bool e2 = tid >= 64 && tid - 64 <= pq;
-    const bool e3 = bessel && (tid == 100 || (tid == 101 && a.z != 1));
+    const bool e3 = bessel && (tid == 100 || (tid == 101 && z != 1));
     const bool e4 = tid == kThreads - 1;
-    if (!bessel && tid >= 32 && tid < 64) {
+    if (sblock && tid >= 32 && tid < 64) {
         // rows mu = k..pl+1 of each order's square block, read by the coaxial stage of that pair
         const int M2 = pq + 2;
-        const cplx* blk = a.pt.stab + a.pt.pair_off[pair_index(min(j, l), max(j, l), sc.n)];
         for (int k = tid - 32; k <= min(pj, pl); k += 32) {
-            const cplx* rows = blk + pair_block_offset(k, M2, M2);
+            const cplx* rows = sblock + pair_block_offset(k, M2, M2);
             const unsigned bytes = (unsigned)((pl + 2 - k) * (M2 - k) * sizeof(cplx));
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rows), "r"(bytes) : "memory");
         }
     }
     if (!(e1 || e2 || e3 || e4)) return;
-    const double* cj = sc.centres + 3 * (size_t)j;
-    const double* cl = sc.centres + 3 * (size_t)l;
-    const double d0 = sc.k * (cl[0] - cj[0]);
-    const double d1 = sc.k * (cl[1] - cj[1]);
-    const double d2 = sc.k * (cl[2] - cj[2]);
+    const double d0 = g.k * (g.sign * (g.cs[0] - g.ct[0]) + g.sh[0]);
+    const double d1 = g.k * (g.sign * (g.cs[1] - g.ct[1]) + g.sh[1]);
+    const double d2 = g.k * (g.sign * (g.cs[2] - g.ct[2]) + g.sh[2]);
     const double r = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
     if (e1) {
         const double ph = (d0 == 0.0 && d1 == 0.0) ? 0.0 : atan2(d1, d0);
@@ -228,6 +233,255 @@ __device__ __forceinline__ void fwd_item(const double* delta, const cplx* src, c
         }
     }
 }
+// Shared-memory buffers and tables of one CTA's translations.
+struct PairCtx {
+    Bufs s;
+    const double* delta;   // d^j(pi/2)
+    DTabs dt;              // rs[j][k] = sqrt(j^2 - k^2)
+    SGaunt g;              // scalar Gaunt sums (no coaxial block)
+    int z;                 // radial function of the translation
+    int pp, SP, XP;        // largest degree; part strides of the folded buffers and of x'
+    bool tabs;             // coaxial blocks given (else S is summed from the Gaunt table)
+};
+
+// One translation (target degree pj <- source degree pl, source coefficients xl, scaled basis)
+// added into c.s.acc: the seven stages with their barriers.  Its geometry and phase tables
+// were prepared in buffer cur; next(tid) prepares the following translation into the other
+// buffer while the last stage runs.  Coincident centres (distance 0) add the source unchanged,
+// as the reference does for them.
+template <class Next>
+__device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const cplx* __restrict__ xl,
+                                const cplx* pair_s, int cur, Next next) {
+    const Bufs& s = c.s;
+    const double* delta = c.delta;
+    const int pp = c.pp, SP = c.SP, XP = c.XP;
+    const bool tabs = c.tabs;
+    const int Pj = pj * (pj + 2);
+    if (s.rho[cur] == 0.0) {
+        const int pm = min(pj, pl), Pm = pm * (pm + 2), Pl = pl * (pl + 2);
+        for (int t = tid; t < 2 * Pm; t += kThreads) {
+            const int part = t >= Pm, e = t - part * Pm;
+            s.acc[part * Pj + e] = s.acc[part * Pj + e] + xl[part * Pl + e];
+        }
+        next(tid);
+        __syncthreads();
+        return;
+    }
+    const int Pl = pl * (pl + 2);
+    const int kmax = min(pj, pl);
+    const cplx* eps = s.eps + cur * (pp + 1);
+    const cplx* eth = s.eth + cur * (pp + 1);
+    // ---- 1. u = e^{i mu (phi + pi/2)} x, folded ------------------------------------------
+    {
+        const int items = pl * (pl + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            const int nu = d_.x, mu = d_.y;
+            const int base = nu * nu - 1 + nu;
+            const cplx e = eps[mu];
+            cplx* U = s.A + off2(nu) + mu;
+            // the four source entries are all in flight before any use
+            const double2* xv = reinterpret_cast<const double2*>(xl + base);
+            const double2 ap = __ldcg(xv + mu), am = __ldcg(xv - mu);
+            const double2 bp = __ldcg(xv + Pl + mu), bm = __ldcg(xv + Pl - mu);
+            const cplx ua = e * mk(ap.x, ap.y), ub = e * mk(bp.x, bp.y);
+            if (mu == 0) {
+                U[0] = ua;
+                U[nu + 1] = ua;
+                U[SP] = ub;
+                U[SP + nu + 1] = ub;
+            } else {
+                const cplx va = conjg(e) * mk(am.x, am.y), vb = conjg(e) * mk(bm.x, bm.y);
+                U[0] = ua + va;
+                U[nu + 1] = ua - va;
+                U[SP] = ub + vb;
+                U[SP + nu + 1] = ub - vb;
+            }
+        }
+        if (!tabs) {
+            const int P = pj + pl + 1;
+            const double* jb = s.jb + cur * szZ(pp);
+            const double* yb = s.yb + cur * szZ(pp);
+            for (int p = tid; p <= P; p += kThreads) s.zeta[p] = zeta_of(c.z, p, jb, yb);
+        }
+    }
+    __syncthreads();
+    // ---- 2. Delta u, e^{-i s theta} ----------------------------------------------------------
+    {
+        const int items = pl * (pl + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            const int nu = d_.x, s_ = d_.y;
+            fwd_item(delta, s.A, s.B, SP, nu, s_, nu, eth[s_]);
+        }
+    }
+    __syncthreads();
+    // ---- 3. Delta^T: x'(nu, +-k) = i^{+-k} T_{+-k}, stored times (2nu+1) ------------------
+    {
+        const int items = pl * (pl + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            const int nu = d_.x, k = d_.y;
+            const int fold = ((nu + k) & 1) ? nu + 1 : 0;
+            const cplx* va = s.B + off2(nu) + fold;
+            cplx Ea, Oa, Eb, Ob;
+            delta_sum(delta + qoff(nu), nu, k, nu, va, va + SP, Ea, Oa, Eb, Ob);
+            const double f = 2.0 * nu + 1.0;
+            const double pn = sgn(nu);
+            cplx* X = s.A + nu * nu - 1 + nu;
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                const cplx E = part ? Eb : Ea, O = part ? Ob : Oa;
+                X[part * XP + k] = ipow_mul(k, f * (E + O));
+                if (k > 0) X[part * XP - k] = ipow_mul(-k, (f * pn) * (E - O));
+            }
+        }
+    }
+    __syncthreads();
+    // ---- 4. w(k, mu) for a', b' at +k and -k ---------------------------------------------
+    {
+        const double x = s.rho[cur];
+        const int items = (kmax + 1) * (pl + 2) - kmax * (kmax + 1) / 2;
+        const int W = c.dt.K + 1;
+        for (int t = tid; t < items; t += kThreads) {
+            int k = 0, rem = t;
+            while (rem >= pl + 2 - k) {
+                rem -= pl + 2 - k;
+                ++k;
+            }
+            const int mu = k + rem;
+            const int lo = max(1, k);
+            const double c0 = 2.0 * mu * (mu + 1.0);
+            const double c1m = (mu - 1 >= lo) ? x * 2.0 * (mu - 1) * c.dt.rs[mu * W + k] / (2.0 * mu - 1.0) : 0.0;
+            const double c2p = (mu + 1 <= pl) ? x * 2.0 * (mu + 2) * c.dt.rs[(mu + 1) * W + k] / (2.0 * mu + 3.0) : 0.0;
+            const double bk2 = 2.0 * k * x;
+            cplx* w = s.B + 4 * t;
+#pragma unroll
+            for (int sg = 0; sg < 2; ++sg) {
+                const int kk = sg ? -k : k;
+                const double bs = sg ? -bk2 : bk2;
+                cplx av[3], bv[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const int nu = mu - 1 + d;
+                    const bool ok = nu >= lo && nu <= pl;
+                    const int o = nu * nu - 1 + nu + kk;
+                    av[d] = ok ? s.A[o] : mk(0, 0);
+                    bv[d] = ok ? s.A[XP + o] : mk(0, 0);
+                }
+                // wa = c0 a + i (bs b + c1m a_- - c2p a_+),  wb = c0 b + i (bs a + c1m b_- - c2p b_+)
+                const cplx ia = bs * bv[1] + c1m * av[0] - c2p * av[2];
+                const cplx ib = bs * av[1] + c1m * bv[0] - c2p * bv[2];
+                w[2 * sg] = mk(c0 * av[1].x - ia.y, c0 * av[1].y + ia.x);
+                w[2 * sg + 1] = mk(c0 * bv[1].x - ib.y, c0 * bv[1].y + ib.x);
+            }
+        }
+    }
+    __syncthreads();
+    // ---- 5. out(k, n) = sum_mu S(k; n, mu) w(k, mu), folded for the back rotation ----------
+    {
+        // rows(k) = pj - max(1, k) + 1: k = 0 and k = 1 both have pj rows
+        const int rows_tot = pj + (kmax >= 1 ? kmax * pj - (kmax - 1) * kmax / 2 : 0);
+        const int M2 = max(pj, pl) + 2;
+        for (int t = tid; t < rows_tot; t += kThreads) {
+            int k = 0, rem = t;
+            for (;;) {
+                const int rk = pj - max(1, k) + 1;
+                if (rem < rk) break;
+                rem -= rk;
+                ++k;
+            }
+            const int n = max(1, k) + rem;
+            const cplx* w = s.B + 4 * (k * (pl + 2) - k * (k - 1) / 2);
+            const int cnt = pl + 2 - k;
+            double r0x = 0, r0y = 0, r1x = 0, r1y = 0, r2x = 0, r2y = 0, r3x = 0, r3y = 0;
+            if (tabs) {
+                const int Wk = M2 - k;
+                const cplx* sp = pair_s + pair_block_offset(k, M2, M2) + (n - k);
+                for (int q = 0; q < cnt; ++q) {
+                    const double2 sv = __ldcg(reinterpret_cast<const double2*>(sp + q * Wk));
+                    const cplx S = mk(sv.x, sv.y);
+                    cmac(r0x, r0y, S, w[4 * q]);
+                    cmac(r1x, r1y, S, w[4 * q + 1]);
+                    cmac(r2x, r2y, S, w[4 * q + 2]);
+                    cmac(r3x, r3y, S, w[4 * q + 3]);
+                }
+            } else {
+                const int W = c.g.NM - k + 1;
+                const size_t plane = (size_t)W * W;
+                const double* G = c.g.gs + c.g.koff[k] + (n - k);
+                for (int q = 0; q < cnt; ++q) {
+                    const int mu = k + q;
+                    const double* gp = G + (size_t)(mu - k) * W;
+                    const int qm = min(n, mu);
+                    int p = n + mu;
+                    double sx = 0.0, sy = 0.0;
+                    for (int qq = 0; qq <= qm; ++qq, p -= 2) {
+                        const double gq = __ldg(gp + qq * plane);
+                        sx += gq * s.zeta[p].x;
+                        sy += gq * s.zeta[p].y;
+                    }
+                    const cplx S = mk(sx, sy);
+                    cmac(r0x, r0y, S, w[4 * q]);
+                    cmac(r1x, r1y, S, w[4 * q + 1]);
+                    cmac(r2x, r2y, S, w[4 * q + 2]);
+                    cmac(r3x, r3y, S, w[4 * q + 3]);
+                }
+            }
+            const double f = sgn(k) / (2.0 * n * (n + 1.0));
+            cplx* U = s.A + off2(n) + k;
+            if (k == 0) {
+                U[0] = mk(f * r0x, f * r0y);
+                U[n + 1] = U[0];
+                U[SP] = mk(f * r1x, f * r1y);
+                U[SP + n + 1] = U[SP];
+            } else {
+                // u'_{+k} = i^{-k} y'(+k), u'_{-k} = i^{k} y'(-k)
+                const cplx ap = ipow_mul(-k, mk(f * r0x, f * r0y)), am = ipow_mul(k, mk(f * r2x, f * r2y));
+                const cplx bp = ipow_mul(-k, mk(f * r1x, f * r1y)), bm = ipow_mul(k, mk(f * r3x, f * r3y));
+                U[0] = ap + am;
+                U[n + 1] = ap - am;
+                U[SP] = bp + bm;
+                U[SP + n + 1] = bp - bm;
+            }
+        }
+    }
+    __syncthreads();
+    // ---- 6. Delta on the translated field, e^{-i s theta} (orders |k| <= kmax only) ----------
+    {
+        const int items = pj * (pj + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            const int n = d_.x, s_ = d_.y;
+            fwd_item(delta, s.A, s.B, SP, n, s_, min(n, kmax), eth[s_]);
+        }
+    }
+    __syncthreads();
+    // ---- 7. Delta^T, phase, accumulate; then the next pair's tables ---------------------------
+    {
+        const int items = pj * (pj + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            const int n = d_.x, m = d_.y;
+            const int fold = ((n + m) & 1) ? n + 1 : 0;
+            const cplx* va = s.B + off2(n) + fold;
+            cplx Ea, Oa, Eb, Ob;
+            delta_sum(delta + qoff(n), n, m, n, va, va + SP, Ea, Oa, Eb, Ob);
+            const double pn = sgn(n);
+            const cplx e = eps[m];
+            cplx* acc = s.acc + n * n - 1 + n;
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                const cplx E = part ? Eb : Ea, O = part ? Ob : Oa;
+                acc[part * Pj + m] = acc[part * Pj + m] + conjg(e) * (E + O);
+                if (m > 0) acc[part * Pj - m] = acc[part * Pj - m] + e * (pn * (E - O));
+            }
+        }
+        next(tid);
+    }
+    __syncthreads();
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------------------------
@@ -309,7 +563,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBuck
     const int Pj = pj * (pj + 2);
     const int SP = pp * (pp + 3);   // part stride of the folded buffers
     const int XP = pp * (pp + 2);   // part stride of x'
-    const double* delta = a.delta;
+    const PairCtx ctx{s, a.delta, a.dt, a.g, a.z, pp, SP, XP, tabs};
     for (int t = tid; t < 2 * Pj; t += kThreads) s.acc[t] = mk(0, 0);
     for (int t = tid; t < pp * (pp + 3) / 2; t += kThreads) {
         int n, k;
@@ -317,235 +571,30 @@ __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBuck
         s.nk[t] = make_short2((short)n, (short)k);
     }
 
+    auto block = [&](int l) -> const cplx* {
+        return tabs ? a.pt.stab + a.pt.pair_off[pair_index(min(j, l), max(j, l), sc.n)] : nullptr;
+    };
+    auto disp = [&](int l) {
+        return Disp{sc.centres + 3 * (size_t)j, sc.centres + 3 * (size_t)l, sc.k, 1.0, {0.0, 0.0, 0.0}};
+    };
     int i = c;
     if (i < bk.nsources && bk.sources[i] == j) i += bk.chunks;
-    if (i < bk.nsources) prep_pair(a, s, j, bk.sources[i], pj, pp, 0, tid, !tabs);
+    if (i < bk.nsources) {
+        const int l = bk.sources[i];
+        prep_pair(s, disp(l), a.z, block(l), pj, sc.p[l], pp, 0, tid, !tabs);
+    }
     __syncthreads();
     int cur = 0;
     while (i < bk.nsources) {
         const int l = bk.sources[i];
         int inext = i + bk.chunks;
         if (inext < bk.nsources && bk.sources[inext] == j) inext += bk.chunks;
-        const int pl = sc.p[l];
-        const int Pl = pl * (pl + 2);
-        const int kmax = min(pj, pl);
-        const cplx* eps = s.eps + cur * (pp + 1);
-        const cplx* eth = s.eth + cur * (pp + 1);
-        // ---- 1. u = e^{i mu (phi + pi/2)} x, folded ------------------------------------------
-        {
-            const cplx* xl = a.x + sc.off[l];
-            const int items = pl * (pl + 3) / 2;
-            for (int t = tid; t < items; t += kThreads) {
-                const short2 d_ = s.nk[t];
-                const int nu = d_.x, mu = d_.y;
-                const int base = nu * nu - 1 + nu;
-                const cplx e = eps[mu];
-                cplx* U = s.A + off2(nu) + mu;
-                // the four source entries are all in flight before any use
-                const double2* xv = reinterpret_cast<const double2*>(xl + base);
-                const double2 ap = __ldcg(xv + mu), am = __ldcg(xv - mu);
-                const double2 bp = __ldcg(xv + Pl + mu), bm = __ldcg(xv + Pl - mu);
-                const cplx ua = e * mk(ap.x, ap.y), ub = e * mk(bp.x, bp.y);
-                if (mu == 0) {
-                    U[0] = ua;
-                    U[nu + 1] = ua;
-                    U[SP] = ub;
-                    U[SP + nu + 1] = ub;
-                } else {
-                    const cplx va = conjg(e) * mk(am.x, am.y), vb = conjg(e) * mk(bm.x, bm.y);
-                    U[0] = ua + va;
-                    U[nu + 1] = ua - va;
-                    U[SP] = ub + vb;
-                    U[SP + nu + 1] = ub - vb;
-                }
+        run_pair(ctx, tid, pj, sc.p[l], a.x + sc.off[l], block(l), cur, [&](int t) {
+            if (inext < bk.nsources) {
+                const int ln = bk.sources[inext];
+                prep_pair(s, disp(ln), a.z, block(ln), pj, sc.p[ln], pp, cur ^ 1, t, !tabs);
             }
-            if (!tabs) {
-                const int P = pj + pl + 1;
-                const double* jb = s.jb + cur * szZ(pp);
-                const double* yb = s.yb + cur * szZ(pp);
-                for (int p = tid; p <= P; p += kThreads) s.zeta[p] = zeta_of(a.z, p, jb, yb);
-            }
-        }
-        __syncthreads();
-        // ---- 2. Delta u, e^{-i s theta} ----------------------------------------------------------
-        {
-            const int items = pl * (pl + 3) / 2;
-            for (int t = tid; t < items; t += kThreads) {
-                const short2 d_ = s.nk[t];
-                const int nu = d_.x, s_ = d_.y;
-                fwd_item(delta, s.A, s.B, SP, nu, s_, nu, eth[s_]);
-            }
-        }
-        __syncthreads();
-        // ---- 3. Delta^T: x'(nu, +-k) = i^{+-k} T_{+-k}, stored times (2nu+1) ------------------
-        {
-            const int items = pl * (pl + 3) / 2;
-            for (int t = tid; t < items; t += kThreads) {
-                const short2 d_ = s.nk[t];
-                const int nu = d_.x, k = d_.y;
-                const int fold = ((nu + k) & 1) ? nu + 1 : 0;
-                const cplx* va = s.B + off2(nu) + fold;
-                cplx Ea, Oa, Eb, Ob;
-                delta_sum(delta + qoff(nu), nu, k, nu, va, va + SP, Ea, Oa, Eb, Ob);
-                const double f = 2.0 * nu + 1.0;
-                const double pn = sgn(nu);
-                cplx* X = s.A + nu * nu - 1 + nu;
-#pragma unroll
-                for (int part = 0; part < 2; ++part) {
-                    const cplx E = part ? Eb : Ea, O = part ? Ob : Oa;
-                    X[part * XP + k] = ipow_mul(k, f * (E + O));
-                    if (k > 0) X[part * XP - k] = ipow_mul(-k, (f * pn) * (E - O));
-                }
-            }
-        }
-        __syncthreads();
-        // ---- 4. w(k, mu) for a', b' at +k and -k ---------------------------------------------
-        {
-            const double x = s.rho[cur];
-            const int items = (kmax + 1) * (pl + 2) - kmax * (kmax + 1) / 2;
-            const int W = a.dt.K + 1;
-            for (int t = tid; t < items; t += kThreads) {
-                int k = 0, rem = t;
-                while (rem >= pl + 2 - k) {
-                    rem -= pl + 2 - k;
-                    ++k;
-                }
-                const int mu = k + rem;
-                const int lo = max(1, k);
-                const double c0 = 2.0 * mu * (mu + 1.0);
-                const double c1m = (mu - 1 >= lo) ? x * 2.0 * (mu - 1) * a.dt.rs[mu * W + k] / (2.0 * mu - 1.0) : 0.0;
-                const double c2p = (mu + 1 <= pl) ? x * 2.0 * (mu + 2) * a.dt.rs[(mu + 1) * W + k] / (2.0 * mu + 3.0) : 0.0;
-                const double bk2 = 2.0 * k * x;
-                cplx* w = s.B + 4 * t;
-#pragma unroll
-                for (int sg = 0; sg < 2; ++sg) {
-                    const int kk = sg ? -k : k;
-                    const double bs = sg ? -bk2 : bk2;
-                    cplx av[3], bv[3];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        const int nu = mu - 1 + d;
-                        const bool ok = nu >= lo && nu <= pl;
-                        const int o = nu * nu - 1 + nu + kk;
-                        av[d] = ok ? s.A[o] : mk(0, 0);
-                        bv[d] = ok ? s.A[XP + o] : mk(0, 0);
-                    }
-                    // wa = c0 a + i (bs b + c1m a_- - c2p a_+),  wb = c0 b + i (bs a + c1m b_- - c2p b_+)
-                    const cplx ia = bs * bv[1] + c1m * av[0] - c2p * av[2];
-                    const cplx ib = bs * av[1] + c1m * bv[0] - c2p * bv[2];
-                    w[2 * sg] = mk(c0 * av[1].x - ia.y, c0 * av[1].y + ia.x);
-                    w[2 * sg + 1] = mk(c0 * bv[1].x - ib.y, c0 * bv[1].y + ib.x);
-                }
-            }
-        }
-        __syncthreads();
-        // ---- 5. out(k, n) = sum_mu S(k; n, mu) w(k, mu), folded for the back rotation ----------
-        {
-            // rows(k) = pj - max(1, k) + 1: k = 0 and k = 1 both have pj rows
-            const int rows_tot = pj + (kmax >= 1 ? kmax * pj - (kmax - 1) * kmax / 2 : 0);
-            const int M2 = max(pj, pl) + 2;
-            const cplx* pair_s = nullptr;
-            if (tabs) {
-                const int s0 = min(j, l), t0 = max(j, l);
-                pair_s = a.pt.stab + a.pt.pair_off[pair_index(s0, t0, sc.n)];
-            }
-            for (int t = tid; t < rows_tot; t += kThreads) {
-                int k = 0, rem = t;
-                for (;;) {
-                    const int rk = pj - max(1, k) + 1;
-                    if (rem < rk) break;
-                    rem -= rk;
-                    ++k;
-                }
-                const int n = max(1, k) + rem;
-                const cplx* w = s.B + 4 * (k * (pl + 2) - k * (k - 1) / 2);
-                const int cnt = pl + 2 - k;
-                double r0x = 0, r0y = 0, r1x = 0, r1y = 0, r2x = 0, r2y = 0, r3x = 0, r3y = 0;
-                if (tabs) {
-                    const int Wk = M2 - k;
-                    const cplx* sp = pair_s + pair_block_offset(k, M2, M2) + (n - k);
-                    for (int q = 0; q < cnt; ++q) {
-                        const double2 sv = __ldcg(reinterpret_cast<const double2*>(sp + q * Wk));
-                        const cplx S = mk(sv.x, sv.y);
-                        cmac(r0x, r0y, S, w[4 * q]);
-                        cmac(r1x, r1y, S, w[4 * q + 1]);
-                        cmac(r2x, r2y, S, w[4 * q + 2]);
-                        cmac(r3x, r3y, S, w[4 * q + 3]);
-                    }
-                } else {
-                    const int W = a.g.NM - k + 1;
-                    const size_t plane = (size_t)W * W;
-                    const double* G = a.g.gs + a.g.koff[k] + (n - k);
-                    for (int q = 0; q < cnt; ++q) {
-                        const int mu = k + q;
-                        const double* gp = G + (size_t)(mu - k) * W;
-                        const int qm = min(n, mu);
-                        int p = n + mu;
-                        double sx = 0.0, sy = 0.0;
-                        for (int qq = 0; qq <= qm; ++qq, p -= 2) {
-                            const double gq = __ldg(gp + qq * plane);
-                            sx += gq * s.zeta[p].x;
-                            sy += gq * s.zeta[p].y;
-                        }
-                        const cplx S = mk(sx, sy);
-                        cmac(r0x, r0y, S, w[4 * q]);
-                        cmac(r1x, r1y, S, w[4 * q + 1]);
-                        cmac(r2x, r2y, S, w[4 * q + 2]);
-                        cmac(r3x, r3y, S, w[4 * q + 3]);
-                    }
-                }
-                const double f = sgn(k) / (2.0 * n * (n + 1.0));
-                cplx* U = s.A + off2(n) + k;
-                if (k == 0) {
-                    U[0] = mk(f * r0x, f * r0y);
-                    U[n + 1] = U[0];
-                    U[SP] = mk(f * r1x, f * r1y);
-                    U[SP + n + 1] = U[SP];
-                } else {
-                    // u'_{+k} = i^{-k} y'(+k), u'_{-k} = i^{k} y'(-k)
-                    const cplx ap = ipow_mul(-k, mk(f * r0x, f * r0y)), am = ipow_mul(k, mk(f * r2x, f * r2y));
-                    const cplx bp = ipow_mul(-k, mk(f * r1x, f * r1y)), bm = ipow_mul(k, mk(f * r3x, f * r3y));
-                    U[0] = ap + am;
-                    U[n + 1] = ap - am;
-                    U[SP] = bp + bm;
-                    U[SP + n + 1] = bp - bm;
-                }
-            }
-        }
-        __syncthreads();
-        // ---- 6. Delta on the translated field, e^{-i s theta} (orders |k| <= kmax only) ----------
-        {
-            const int items = pj * (pj + 3) / 2;
-            for (int t = tid; t < items; t += kThreads) {
-                const short2 d_ = s.nk[t];
-                const int n = d_.x, s_ = d_.y;
-                fwd_item(delta, s.A, s.B, SP, n, s_, min(n, kmax), eth[s_]);
-            }
-        }
-        __syncthreads();
-        // ---- 7. Delta^T, phase, accumulate; then the next pair's tables ---------------------------
-        {
-            const int items = pj * (pj + 3) / 2;
-            for (int t = tid; t < items; t += kThreads) {
-                const short2 d_ = s.nk[t];
-                const int n = d_.x, m = d_.y;
-                const int fold = ((n + m) & 1) ? n + 1 : 0;
-                const cplx* va = s.B + off2(n) + fold;
-                cplx Ea, Oa, Eb, Ob;
-                delta_sum(delta + qoff(n), n, m, n, va, va + SP, Ea, Oa, Eb, Ob);
-                const double pn = sgn(n);
-                const cplx e = eps[m];
-                cplx* acc = s.acc + n * n - 1 + n;
-#pragma unroll
-                for (int part = 0; part < 2; ++part) {
-                    const cplx E = part ? Eb : Ea, O = part ? Ob : Oa;
-                    acc[part * Pj + m] = acc[part * Pj + m] + conjg(e) * (E + O);
-                    if (m > 0) acc[part * Pj - m] = acc[part * Pj - m] + e * (pn * (E - O));
-                }
-            }
-            if (inext < bk.nsources) prep_pair(a, s, j, bk.sources[inext], pj, pp, cur ^ 1, tid, !tabs);
-        }
-        __syncthreads();
+        });
         cur ^= 1;
         i = inext;
     }
@@ -566,6 +615,58 @@ void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s) {
     dim3 grid(b.ntargets, b.chunks);
     cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_direct<<<grid, kThreads, smem, s>>>(a, b);
+}
+
+// ---------------------------------------------------------------------------------------------
+// ML-FMM passes: one CTA per target (sphere or box), the same seven stages per source, S summed
+// from the Gaunt table (the displacements are box geometry, so no pair tables), result written
+// to (or added onto) the target's coefficients.
+__global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
+    extern __shared__ __align__(16) double smem_d[];
+    const int pp = a.pp;
+    const Bufs s = carve(smem_d, pp, false);
+    const int t = a.tbase + blockIdx.x;
+    const int tid = threadIdx.x;
+    const int pj = a.tgt.p[t];
+    const int Pj = pj * (pj + 2);
+    const int SP = pp * (pp + 3);
+    const int XP = pp * (pp + 2);
+    const PairCtx ctx{s, a.delta, a.dt, a.g, a.z, pp, SP, XP, false};
+    cplx* out = a.out + a.tgt.off[t];
+    for (int e = tid; e < 2 * Pj; e += kThreads) s.acc[e] = a.add ? out[e] : mk(0, 0);
+    for (int e = tid; e < pp * (pp + 3) / 2; e += kThreads) {
+        int n, k;
+        decode_nk(e, n, k);
+        s.nk[e] = make_short2((short)n, (short)k);
+    }
+    const int i0 = a.lptr[blockIdx.x], i1 = a.lptr[blockIdx.x + 1];
+    auto disp = [&](int l) {
+        return Disp{a.tgt.c + 3 * (size_t)t, a.src.c + 3 * (size_t)l, a.k, a.sign, {a.sh[0], a.sh[1], a.sh[2]}};
+    };
+    if (i0 < i1) {
+        const int l = a.lidx[i0];
+        prep_pair(s, disp(l), a.z, nullptr, pj, a.src.p[l], pp, 0, tid, true);
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int i = i0; i < i1; ++i) {
+        const int l = a.lidx[i];
+        run_pair(ctx, tid, pj, a.src.p[l], a.x + a.src.off[l], nullptr, cur, [&](int tt) {
+            if (i + 1 < i1) {
+                const int ln = a.lidx[i + 1];
+                prep_pair(s, disp(ln), a.z, nullptr, pj, a.src.p[ln], pp, cur ^ 1, tt, true);
+            }
+        });
+        cur ^= 1;
+    }
+    for (int e = tid; e < 2 * Pj; e += kThreads) out[e] = s.acc[e];
+}
+
+void launch_translate(const TransArgs& a, int ntargets, cudaStream_t s) {
+    if (ntargets <= 0) return;
+    size_t smem = smem_bytes(a.pp, false);
+    cudaFuncSetAttribute(k_translate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_translate<<<ntargets, kThreads, smem, s>>>(a);
 }
 
 // y = x + T (sum of the slabs) for coupled spheres, y = x otherwise

@@ -39,6 +39,8 @@ module foggy_gpu_f
         real(c_double) :: fmm_digits
         integer(c_int64_t) :: device_memory_budget
         integer(c_int32_t) :: pair_tables
+        integer(c_int32_t) :: fmm_convention
+        integer(c_int32_t) :: z_translation_gt_r
         integer(c_int32_t) :: reserved
     end type foggy_params
 

@@ -22,7 +22,8 @@ import numpy as np
 from . import _native as N
 
 
-def _params(scene, use_ml_fmm=False, init_with_single_sphere=False, memory_budget=0, pair_tables=0):
+def _params(scene, use_ml_fmm=False, init_with_single_sphere=False, memory_budget=0, pair_tables=0,
+            fmm_convention=0, z_translation_gt_r=3):
     L = N.load()
     p = N.FoggyParams()
     L.foggy_default_params(C.byref(p))
@@ -40,6 +41,8 @@ def _params(scene, use_ml_fmm=False, init_with_single_sphere=False, memory_budge
     p.tree_l_max = int(scene.tree_l_max)
     p.device_memory_budget = int(memory_budget)
     p.pair_tables = int(pair_tables)
+    p.fmm_convention = int(fmm_convention)
+    p.z_translation_gt_r = int(z_translation_gt_r)
     return p
 
 
@@ -47,10 +50,13 @@ class MultiSphereSolver:
     """lib_mie_ms_constructor + the solver interface, on one GPU."""
 
     def __init__(self, scene, use_ml_fmm=False, init_with_single_sphere=False, device=0, memory_budget=0,
-                 pair_tables=0):
+                 pair_tables=0, fmm_convention=0, z_translation_gt_r=3):
+        """fmm_convention 0 runs the ML-FMM as the reference writes it, 1 the consistent
+        expansion (see foggy_params.fmm_convention)."""
         self.L = N.load()
         self.scene = scene
-        self.params = _params(scene, use_ml_fmm, init_with_single_sphere, memory_budget, pair_tables)
+        self.params = _params(scene, use_ml_fmm, init_with_single_sphere, memory_budget, pair_tables,
+                              fmm_convention, z_translation_gt_r)
         h = C.c_void_p()
         N.check(self.L.foggy_create(C.byref(self.params), int(device), C.byref(h)))
         self.h = h
@@ -185,6 +191,16 @@ class MultiSphereSolver:
         N.check(self.L.foggy_build_tree(self.h, N.ptr(u, C.c_int64), N.ptr(order, C.c_int32), C.byref(lmin),
                                         C.byref(lmax)), self.h)
         return u, order, lmin.value, lmax.value
+
+    def tree_domain(self, level, n, kind):
+        """E1 (kind 1) / E2 (kind 2) sphere lists or the I4 (kind 4) box list of box n at a level
+        (lib_tree_get_domain_e1 / _e2 / _i4)."""
+        cnt = C.c_int32(0)
+        N.check(self.L.foggy_tree_domain(self.h, int(level), int(n), int(kind), None, C.byref(cnt)), self.h)
+        out = np.zeros(max(cnt.value, 1), np.int64)
+        N.check(self.L.foggy_tree_domain(self.h, int(level), int(n), int(kind), N.ptr(out, C.c_int64), C.byref(cnt)),
+                self.h)
+        return out[:cnt.value]
 
     def tree_boxes(self, level):
         cnt = C.c_int32(0)

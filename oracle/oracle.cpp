@@ -23,6 +23,8 @@
 #include <cstdint>
 #include <cstring>
 #include <vector>
+#include <map>
+#include <array>
 #include <omp.h>
 
 extern "C" {
@@ -828,6 +830,324 @@ int orc_build_tree(int n, const double* centres, int s, int l_max_fixed, int64_t
     return 0;
 }
 
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// ML-FMM operator of the reference: libmlfmm/src/lib/lib_ml_fmm.f90 (upward pass :387-640,
+// downward pass :656-982, final summation :994-1204) with the Mie handles of
+// FoggySim/src/lib/mie_theory/lib_mie_ms_ml_fmm_interface.f90 (get_u_B_i :259-379,
+// translation_SS/SR/RR :381-595, get_u_phi_i_j :600-813, dor :825-981) and the octree of
+// libtree/src/lib/lib_tree.f90 (E1 :492-609, E2 :611-724, I4 :994-1143, box centre
+// lib_tree_helper_functions.f90:774-799, neighbours :914-997).
+//
+// convention 0 reproduces the reference as written: every translation uses the incident-wave
+// radial function except the box-to-sphere one (z_translation_gt_r), the global order for all
+// boxes, displacement target - source in the aggregation, M2L and box-to-sphere steps (source -
+// target in M2M, L2L and the near field), and the box-to-sphere displacement unscaled as a point
+// (lib_tree_get_unscaled_point of a difference adds x_min).  convention 1 is the consistent
+// expansion: regular (j_n) translations for aggregation, M2M, L2L and box-to-sphere, the
+// coupling's radial function for M2L and the near field, displacement source - target
+// everywhere; it tends to the direct operator as the box order grows.
+// ------------------------------------------------------------------------------------------
+namespace fmmo {
+
+void deinterleave(int64_t n, int l, int64_t c[3]) {
+    c[0] = c[1] = c[2] = 0;
+    for (int b = 0; b < l; ++b)
+        for (int d = 0; d < 3; ++d) c[d] |= ((n >> (3 * b + (2 - d))) & 1) << b;
+}
+int64_t interleave(const int64_t c[3], int l) {
+    int64_t n = 0;
+    for (int b = 0; b < l; ++b)
+        for (int d = 0; d < 3; ++d) n |= ((c[d] >> b) & 1) << (3 * b + (2 - d));
+    return n;
+}
+void centre_norm(int64_t n, int l, double c[3]) {
+    int64_t q[3];
+    deinterleave(n, l, q);
+    for (int d = 0; d < 3; ++d) c[d] = std::ldexp(1.0, -l) * ((double)q[d] + 0.5);
+}
+// I2: the box and its neighbours at distance 1 inside the domain (lib_tree_get_domain_i2)
+std::vector<int64_t> i2(int64_t n, int l) {
+    std::vector<int64_t> out{n};
+    int64_t c[3], q[3];
+    deinterleave(n, l, c);
+    int64_t hi = ((int64_t)1 << l) - 1;
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz) {
+                if (!dx && !dy && !dz) continue;
+                q[0] = c[0] + dx, q[1] = c[1] + dy, q[2] = c[2] + dz;
+                if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] > hi || q[1] > hi || q[2] > hi) continue;
+                out.push_back(interleave(q, l));
+            }
+    return out;
+}
+// I4: children of the parent's I2 that are not in the box's own I2, ascending
+std::vector<int64_t> i4(int64_t n, int l) {
+    std::vector<int64_t> out;
+    if (l == 0) return out;
+    std::vector<int64_t> own = i2(n, l), par = i2(n >> 3, l - 1);
+    std::sort(own.begin(), own.end());
+    for (int64_t q : par)
+        for (int c = 0; c < 8; ++c) {
+            int64_t b = (q << 3) | c;
+            if (!std::binary_search(own.begin(), own.end(), b)) out.push_back(b);
+        }
+    std::sort(out.begin(), out.end());
+    return out;
+}
+
+struct Tree {
+    int lmin, lmax;
+    double D, xmin[3];
+    std::vector<double> pn;          // normalised centres
+    std::vector<int64_t> u21;
+    std::vector<int> order;          // spheres by key
+    std::vector<std::vector<int64_t>> boxes;   // per level (index l - lmin), ascending
+    std::vector<std::map<int64_t, int>> id;
+    // spheres of box n at level l (E1), in key order
+    std::vector<int> e1(int64_t n, int l) const {
+        std::vector<int> out;
+        for (int i : order)
+            if ((u21[i] >> (3 * (21 - l))) == n) out.push_back(i);
+        return out;
+    }
+    std::vector<int> e2(int64_t n, int l) const {
+        std::vector<int64_t> bs = i2(n, l);
+        std::sort(bs.begin(), bs.end());
+        std::vector<int> out;
+        for (int64_t b : bs) {
+            std::vector<int> e = e1(b, l);
+            out.insert(out.end(), e.begin(), e.end());
+        }
+        return out;
+    }
+    bool exists(int64_t n, int l) const { return id[l - lmin].count(n) > 0; }
+    void unscaled_centre(int64_t n, int l, double c[3]) const {
+        centre_norm(n, l, c);
+        for (int d = 0; d < 3; ++d) c[d] = c[d] * D + xmin[d];
+    }
+};
+
+Tree build(int N, const double* centres, int s, int l_max_fixed) {
+    Tree t;
+    t.pn.resize(3 * (size_t)N);
+    scale_points(N, centres, t.pn.data(), &t.D, t.xmin);
+    t.u21.resize(N);
+    for (int i = 0; i < N; ++i) t.u21[i] = universal_index(&t.pn[3 * (size_t)i], 21);
+    t.order.resize(N);
+    for (int i = 0; i < N; ++i) t.order[i] = i;
+    std::sort(t.order.begin(), t.order.end(), [&](int a, int b) { return t.u21[a] < t.u21[b]; });
+    int lm = 1;
+    if (l_max_fixed > 0) {
+        lm = l_max_fixed;
+    } else {
+        for (int i = 0; i + s < N; ++i) {
+            int64_t a = t.u21[t.order[i]], b = t.u21[t.order[i + s]];
+            for (int j = 21; j >= 0; --j) {
+                a >>= 3;
+                b >>= 3;
+                if (a == b) { lm = std::max(lm, j); break; }
+            }
+        }
+    }
+    t.lmax = lm;
+    t.lmin = std::min(2, lm);
+    for (int l = t.lmin; l <= t.lmax; ++l) {
+        std::vector<int64_t> b;
+        for (int i : t.order) {
+            int64_t v = t.u21[i] >> (3 * (21 - l));
+            if (b.empty() || b.back() != v) b.push_back(v);
+        }
+        std::map<int64_t, int> m;
+        for (size_t q = 0; q < b.size(); ++q) m[b[q]] = (int)q;
+        t.boxes.push_back(b);
+        t.id.push_back(m);
+    }
+    return t;
+}
+
+typedef std::vector<cd> Vec;   // reference layout, global range, [a | b]
+
+struct Fmm {
+    Problem& P;
+    int conv, zgt;
+    Tree t;
+    std::map<std::array<double, 8>, std::pair<std::vector<cd>, std::vector<cd>>> cache;
+    Fmm(Problem& p, int c, int z, const Tree& tr) : P(p), conv(c), zgt(z), t(tr) {}
+
+    // out(rows r1..r2) += T(kd; z) in(cols c1..c2), both in the global layout
+    void apply(const double kd[3], int z, int r1, int r2, int c1, int c2, const cd* in, cd* out,
+               const std::vector<cd>* scale_a = nullptr, const std::vector<cd>* scale_b = nullptr, int a0 = 0) {
+        int C = P.cnt();
+        double rho, th, ph;
+        to_spherical(kd, &rho, &th, &ph);
+        if (rho == 0.0) {   // coincident centres: the reference passes the coefficients through
+            for (int n = std::max(r1, c1); n <= std::min(r2, c2); ++n)
+                for (int m = -n; m <= n; ++m) {
+                    int o = blk(P.n1, n, m);
+                    out[o] += in[o];
+                    out[C + o] += in[C + o];
+                }
+            return;
+        }
+        std::array<double, 8> key{kd[0], kd[1], kd[2], (double)z, (double)r1, (double)r2, (double)c1, (double)c2};
+        auto it = cache.find(key);
+        if (it == cache.end()) {
+            int cr = (r2 + 1) * (r2 + 1) - r1 * r1, cc = (c2 + 1) * (c2 + 1) - c1 * c1;
+            std::vector<cd> A((size_t)cr * cc), B((size_t)cr * cc);
+            wig_thread_temp_init(2 * (4 * P.n2 + 8));
+            translation_xu(rho, th, ph, r1, r2, c1, c2, z, A.data(), B.data());
+            it = cache.emplace(key, std::make_pair(std::move(A), std::move(B))).first;
+        }
+        const std::vector<cd>& A = it->second.first;
+        const std::vector<cd>& B = it->second.second;
+        int cc = (c2 + 1) * (c2 + 1) - c1 * c1;
+        for (int n = r1; n <= r2; ++n)
+            for (int m = -n; m <= n; ++m) {
+                int row = blk(r1, n, m);
+                cd s1(0, 0), s2(0, 0);
+                for (int nu = c1; nu <= c2; ++nu)
+                    for (int mu = -nu; mu <= nu; ++mu) {
+                        int col = blk(c1, nu, mu), xo = blk(P.n1, nu, mu);
+                        cd a = A[(size_t)row * cc + col], b = B[(size_t)row * cc + col];
+                        s1 += a * in[xo] + b * in[C + xo];
+                        s2 += b * in[xo] + a * in[C + xo];
+                    }
+                int o = blk(P.n1, n, m);
+                if (scale_a) {
+                    s1 *= (*scale_a)[n - a0];
+                    s2 *= (*scale_b)[n - a0];
+                }
+                out[o] += s1;
+                out[C + o] += s2;
+            }
+    }
+
+    void run(const cd* x, cd* y) {
+        const int C = P.cnt(), n1 = P.n1, n2 = P.n2, zi = P.z;
+        const int z_reg = conv == 0 ? zi : 1, z_m2l = zi, z_dor = conv == 0 ? zgt : 1;
+        const double sts = conv == 0 ? -1.0 : 1.0;   // aggregation, M2L, box-to-sphere
+        const double k = P.k;
+        const int nlev = t.lmax - t.lmin + 1;
+        std::vector<std::vector<Vec>> Cc(nlev), Dd(nlev);
+        for (int li = 0; li < nlev; ++li) {
+            Cc[li].assign(t.boxes[li].size(), Vec(2 * (size_t)C, cd(0, 0)));
+            Dd[li].assign(t.boxes[li].size(), Vec(2 * (size_t)C, cd(0, 0)));
+        }
+        auto rows_of = [&](int j, int* a, int* b) {
+            sphere_range(P, j, a, b);
+            return !P.row_rule || (n2 <= *b && n1 >= *a);
+        };
+        // upward step 1: aggregation at the leaves
+        const int L = nlev - 1;
+        for (size_t q = 0; q < t.boxes[L].size(); ++q) {
+            int64_t nb = t.boxes[L][q];
+            double cb[3];
+            t.unscaled_centre(nb, t.lmax, cb);
+            for (int i : t.e1(nb, t.lmax)) {
+                int ia, ib;
+                if (!rows_of(i, &ia, &ib)) continue;
+                double kd[3];
+                for (int d = 0; d < 3; ++d) kd[d] = k * sts * (P.centres[3 * i + d] - cb[d]);
+                apply(kd, z_reg, n1, n2, ia, ib, x + (size_t)2 * C * i, Cc[L][q].data());
+            }
+        }
+        // upward step 2: M2M
+        for (int li = L - 1; li >= 0; --li) {
+            int l = t.lmin + li;
+            for (size_t q = 0; q < t.boxes[li].size(); ++q) {
+                int64_t nb = t.boxes[li][q];
+                double cp[3];
+                t.unscaled_centre(nb, l, cp);
+                for (int c = 0; c < 8; ++c) {
+                    int64_t ch = (nb << 3) | c;
+                    auto it = t.id[li + 1].find(ch);
+                    if (it == t.id[li + 1].end()) continue;
+                    double cc[3], kd[3];
+                    t.unscaled_centre(ch, l + 1, cc);
+                    for (int d = 0; d < 3; ++d) kd[d] = k * (cc[d] - cp[d]);
+                    apply(kd, z_reg, n1, n2, n1, n2, Cc[li + 1][it->second].data(), Cc[li][q].data());
+                }
+            }
+        }
+        // downward step 1: M2L over the interaction lists
+        for (int li = 0; li < nlev; ++li) {
+            int l = t.lmin + li;
+            for (size_t q = 0; q < t.boxes[li].size(); ++q) {
+                int64_t nb = t.boxes[li][q];
+                double cb[3];
+                t.unscaled_centre(nb, l, cb);
+                for (int64_t s : i4(nb, l)) {
+                    auto it = t.id[li].find(s);
+                    if (it == t.id[li].end()) continue;
+                    double cs[3], kd[3];
+                    t.unscaled_centre(s, l, cs);
+                    for (int d = 0; d < 3; ++d) kd[d] = k * sts * (cs[d] - cb[d]);
+                    apply(kd, z_m2l, n1, n2, n1, n2, Cc[li][it->second].data(), Dd[li][q].data());
+                }
+            }
+        }
+        // downward step 2: L2L
+        for (int li = 1; li < nlev; ++li) {
+            int l = t.lmin + li;
+            for (size_t q = 0; q < t.boxes[li].size(); ++q) {
+                int64_t nb = t.boxes[li][q];
+                int pi = t.id[li - 1].at(nb >> 3);
+                double cb[3], cp[3], kd[3];
+                t.unscaled_centre(nb, l, cb);
+                t.unscaled_centre(nb >> 3, l - 1, cp);
+                for (int d = 0; d < 3; ++d) kd[d] = k * (cp[d] - cb[d]);
+                apply(kd, z_reg, n1, n2, n1, n2, Dd[li - 1][pi].data(), Dd[li][q].data());
+            }
+        }
+        // final summation: box-to-sphere and near field, y = x + a/b (...)
+        for (size_t i = 0; i < (size_t)2 * C * P.N; ++i) y[i] = 0.0;
+        for (size_t q = 0; q < t.boxes[L].size(); ++q) {
+            int64_t nb = t.boxes[L][q];
+            double cn[3], cb[3];
+            centre_norm(nb, t.lmax, cn);
+            t.unscaled_centre(nb, t.lmax, cb);
+            std::vector<int> near = t.e2(nb, t.lmax);
+            for (int j : t.e1(nb, t.lmax)) {
+                cd* yj = y + (size_t)2 * C * j;
+                int ja, jb;
+                bool rows = rows_of(j, &ja, &jb);
+                int ip = P.pidx[j], a0 = P.nr[2 * ip];
+                double kd[3];
+                for (int d = 0; d < 3; ++d)
+                    kd[d] = conv == 0 ? k * ((t.pn[3 * (size_t)j + d] - cn[d]) * t.D + t.xmin[d])
+                                      : k * (cb[d] - P.centres[3 * j + d]);
+                if (rows) {
+                    double r = std::sqrt(kd[0] * kd[0] + kd[1] * kd[1] + kd[2] * kd[2]);
+                    if (r == 0.0) {
+                        for (int i = 0; i < 2 * C; ++i) yj[i] += Dd[L][q][i];
+                    } else {
+                        apply(kd, z_dor, ja, jb, n1, n2, Dd[L][q].data(), yj, &P.an[ip], &P.bn[ip], a0);
+                    }
+                }
+                for (int l : near) {
+                    if (l == j) {
+                        for (int i = 0; i < 2 * C; ++i) yj[i] += x[(size_t)2 * C * j + i];
+                        continue;
+                    }
+                    if (!rows) continue;
+                    int la, lb;
+                    sphere_range(P, l, &la, &lb);
+                    for (int d = 0; d < 3; ++d) kd[d] = k * (P.centres[3 * l + d] - P.centres[3 * j + d]);
+                    apply(kd, zi, ja, jb, la, lb, x + (size_t)2 * C * l, yj, &P.an[ip], &P.bn[ip], a0);
+                }
+            }
+        }
+    }
+};
+
+}  // namespace fmmo
+
+extern "C" {
+
 // ---- problem-level API (mirrors foggy_set_spheres / foggy_set_plane_waves) ----------------
 void* orc_problem_create(double lambda0, double n_medium, int n1, int n2, int z, int row_rule,
                          int N, const double* centres, const int* pidx, int NP,
@@ -1021,6 +1341,37 @@ int orc_cross_sections(void* p, const double* xin, double* out) {
     out[2] = f * cabs;
     out[0] = out[1] - out[2];
     return 0;
+}
+
+
+// ML-FMM operator (convention 0: the reference as written; 1: consistent expansion) with
+// l_max fixed (> 0) or from s_opt; x, y in the reference layout.
+int orc_fmm_matvec(void* p, int l_max_fixed, int s_opt, int convention, int z_gt_r, const double* x, double* y) {
+    Problem* P = static_cast<Problem*>(p);
+    fmmo::Tree t = fmmo::build(P->N, P->centres.data(), s_opt, l_max_fixed);
+    fmmo::Fmm f(*P, convention, z_gt_r, t);
+    f.run(reinterpret_cast<const cd*>(x), reinterpret_cast<cd*>(y));
+    return 0;
+}
+
+// Octree lists of box n at level l (lib_tree_get_domain_e1 / e2 / i4): kind 1 -> spheres of
+// the box, 2 -> spheres of the box and its neighbours, 3 -> the neighbour boxes
+// (lib_tree_hf_get_neighbour_all_xD), 4 -> interaction-list box indices (every candidate
+// inside the domain, ascending).  Returns the count; out may be NULL.
+int orc_tree_domain(int N, const double* centres, int l_max_fixed, int l, int64_t n, int kind, int64_t* out,
+                    int cap) {
+    fmmo::Tree t = fmmo::build(N, centres, 10, l_max_fixed > 0 ? l_max_fixed : 21);
+    std::vector<int64_t> v;
+    if (kind == 1) for (int i : t.e1(n, l)) v.push_back(i);
+    if (kind == 2) for (int i : t.e2(n, l)) v.push_back(i);
+    if (kind == 3) {   // neighbours at distance 1 inside the domain, without the box itself
+        std::vector<int64_t> b = fmmo::i2(n, l);
+        v.assign(b.begin() + 1, b.end());
+        std::sort(v.begin(), v.end());
+    }
+    if (kind == 4) v = fmmo::i4(n, l);
+    if (out) for (int i = 0; i < (int)v.size() && i < cap; ++i) out[i] = v[i];
+    return (int)v.size();
 }
 
 }  // extern "C"

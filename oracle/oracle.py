@@ -258,3 +258,32 @@ def _pairs_apply(self, x, targets, sources):
 
 
 Problem.pairs_apply = _pairs_apply
+
+
+def _fmm_matvec(self, x, l_max=0, s_opt=10, convention=0, z_gt_r=3):
+    """The reference's ML-FMM operator y = A x (convention 0, as the Fortran does it) or the
+    consistent expansion (convention 1); l_max > 0 fixes the leaf level."""
+    L = lib()
+    if not getattr(L, "_fmm_sig", False):
+        L.orc_fmm_matvec.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, dp, dp]
+        L._fmm_sig = True
+    y = np.zeros(2 * self.n)
+    L.orc_fmm_matvec(self.h, int(l_max), int(s_opt), int(convention), int(z_gt_r), _c(x), y)
+    return y.view(np.complex128)
+
+
+Problem.fmm_matvec = _fmm_matvec
+
+
+def tree_domain(centres, l_max, l, n, kind):
+    """E1 (kind 1), E2 (kind 2) sphere lists or I4 (kind 4) box list of box n at level l."""
+    L = lib()
+    if not getattr(L, "_dom_sig", False):
+        L.orc_tree_domain.argtypes = [C.c_int, dp, C.c_int, C.c_int, C.c_int64, C.c_int, C.c_void_p, C.c_int]
+        L.orc_tree_domain.restype = C.c_int
+        L._dom_sig = True
+    c = np.ascontiguousarray(centres, np.float64).reshape(-1)
+    cnt = L.orc_tree_domain(len(c) // 3, c, int(l_max), int(l), int(n), int(kind), None, 0)
+    out = np.zeros(max(cnt, 1), np.int64)
+    L.orc_tree_domain(len(c) // 3, c, int(l_max), int(l), int(n), int(kind), out.ctypes.data, cnt)
+    return out[:cnt]

@@ -19,6 +19,9 @@ golden values of the reference's Fortran unit tests (read as text, never compile
       pi_tau_theta2      libmath/src/math/lib_math_legendre.f90:2099-2210
       mie_ab_m15_x10     FoggySim/src/lib/mie_theory/lib_mie_ss_helper_functions.f90:1639-1703
       universal_index    libtree/src/lib/lib_tree_helper_functions.f90:2166-2204
+      tree_neighbours    libtree/src/lib/lib_tree_helper_functions.f90:2438-2470, 2529-2560
+      tree_parent        libtree/src/lib/lib_tree_helper_functions.f90:2277-2310
+      tree_children      libtree/src/lib/lib_tree_helper_functions.f90:2312-2356
 
 The tests read only the files written here, so they run where the reference is absent.
 """
@@ -106,6 +109,21 @@ def main(ref):
 
     # universal index of (0.75, 0.5, 2^-9 + 2^-8) at level 1 is 6 (3-D build)
     g["universal_index"] = [{"point": [0.75, 0.5, 2.0 ** -9 + 2.0 ** -8], "l": 1, "n": 6}]
+
+    # neighbours at distance 1 (3-D build): the ground-truth arrays, -1 marks an unused slot
+    tre = os.path.join(ref, "libtree/src/lib/lib_tree_helper_functions.f90")
+
+    def int_array(a, b):
+        txt = "\n".join(lines(tre, a, b))
+        m = re.search(r"neighbour_all_ground_truth\s*=\s*\(/(.*?)/\)", txt, re.S)
+        return [int(t) for t in re.sub(r"&", " ", m.group(1)).replace("\n", " ").split(",")]
+
+    g["tree_neighbours"] = [{"l": 2, "n": 35, "neighbours": [v for v in int_array(2438, 2472) if v >= 0]},
+                            {"l": 1, "n": 5, "neighbours": [v for v in int_array(2529, 2562) if v >= 0]}]
+    par = [int(m.group(1)) for l in lines(tre, 2290, 2296) for m in [re.search(r"n_parent_ground_trouth\s*=\s*(\d+)", l)] if m]
+    g["tree_parent"] = {"l": 1, "n": 6, "parent": par[-1]}
+    kids = [int(m.group(1)) for l in lines(tre, 2330, 2340) for m in [re.search(r"children_n_ground_truth\(\d\)\s*=\s*(\d+)", l)] if m]
+    g["tree_children"] = {"n": 1, "children": kids[-8:]}
 
     with open(os.path.join(HERE, "inline_goldens.json"), "w") as f:
         json.dump(g, f, indent=1)
