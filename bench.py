@@ -1,6 +1,7 @@
 """Benchmark of the multi-sphere T-matrix GMRES solve on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload medium|small]
+                    [--operator direct|mlfmm] [--fmm-convention 0|1]
 
 One step = one complete solve (GMRES to the workload's tolerance) of the seeded synthetic
 scene.  The default workload is the 2000-sphere lognormal cluster (40 um cube, per-sphere
@@ -75,6 +76,78 @@ def algorithmic_flops(sc):
         for b in ps:
             pairs = cnt[a] * cnt[b] - (cnt[a] if a == b else 0)
             total += pairs * (4.0 * 2 * (rot[b] + rot[a]) + 8.0 * 4 * ax[(a, b)])
+    total += 8.0 * float(np.sum(2 * p * (p + 2)))
+    return total
+
+
+def translation_flops(pt, ps):
+    """Flops of one translation from a degree-ps expansion to a degree-pt one, counted as in
+    algorithmic_flops (two rotations and the axial step)."""
+    rot = lambda p: sum((2 * n + 1) ** 2 for n in range(1, p + 1))
+    mn = min(pt, ps)
+    ax = sum((pt - max(1, abs(k)) + 1) * (ps - max(1, abs(k)) + 1) for k in range(-mn, mn + 1))
+    return 4.0 * 2 * (rot(ps) + rot(pt)) + 8.0 * 4 * ax
+
+
+def _morton(c, l):
+    n = 0
+    for b in range(l):
+        for d in range(3):
+            n |= ((c[d] >> b) & 1) << (3 * b + (2 - d))
+    return n
+
+
+def _demorton(n, l):
+    c = [0, 0, 0]
+    for b in range(l):
+        for d in range(3):
+            c[d] |= ((n >> (3 * b + (2 - d))) & 1) << b
+    return c
+
+
+def fmm_flops(sc, uindex, lmin, lmax, row_rule):
+    """Flops of one ML-FMM operator application from the tree the library built (per-sphere box
+    index at l_max): aggregation, M2M, M2L over the interaction lists, L2L, box-to-sphere and the
+    near field, each translation counted by translation_flops, plus the T-matrix scaling."""
+    p = sc.p_of_sphere().astype(int)
+    pg = int(sc.n_range[1])
+    lmin = min(lmin, lmax)
+    boxes = {l: set(int(u) >> (3 * (lmax - l)) for u in uindex) for l in range(lmin, lmax + 1)}
+    tp = translation_flops(pg, pg)
+    total = 0.0
+    total += sum(translation_flops(pg, int(pi)) for pi in p if not row_rule or pi >= pg)
+    total += sum(len(boxes[l]) for l in range(lmin + 1, lmax + 1)) * tp * 2     # M2M and L2L
+    for l in range(lmin, lmax + 1):
+        hi = (1 << l) - 1
+        for nb in boxes[l]:
+            c = _demorton(nb, l)
+            own = {_morton([c[0] + dx, c[1] + dy, c[2] + dz], l)
+                   for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)
+                   if all(0 <= c[d] + v <= hi for d, v in enumerate((dx, dy, dz)))}
+            pc = _demorton(nb >> 3, l - 1) if l > 0 else [0, 0, 0]
+            phi = (1 << (l - 1)) - 1 if l > 0 else -1
+            par = {_morton([pc[0] + dx, pc[1] + dy, pc[2] + dz], l - 1)
+                   for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)
+                   if l > 0 and all(0 <= pc[d] + v <= phi for d, v in enumerate((dx, dy, dz)))}
+            i4 = {(q << 3) | ch for q in par for ch in range(8)} - own
+            total += len(i4 & boxes[l]) * tp
+    leaf = [int(u) for u in uindex]
+    total += sum(translation_flops(int(pj), pg) for pj in p)
+    members = {}
+    for j, b in enumerate(leaf):
+        members.setdefault(b, []).append(j)
+    hi = (1 << lmax) - 1
+    for b, js in members.items():
+        c = _demorton(b, lmax)
+        near = []
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    q = [c[0] + dx, c[1] + dy, c[2] + dz]
+                    if all(0 <= v <= hi for v in q):
+                        near += members.get(_morton(q, lmax), [])
+        for j in js:
+            total += sum(translation_flops(int(p[j]), int(p[l])) for l in near if l != j)
     total += 8.0 * float(np.sum(2 * p * (p + 2)))
     return total
 
@@ -212,7 +285,10 @@ def run_reference(args, rank, world):
 def config_of(sc, args):
     p = sc.p_of_sphere()
     return {"workload": sc.name, "spheres": sc.n_spheres, "p_max": int(p.max()), "p_median": float(np.median(p)),
-            "unknowns_ragged": sc.ragged_unknowns(), "matvec": "direct (all pairs, rotation-axial-rotation)",
+            "unknowns_ragged": sc.ragged_unknowns(),
+            "matvec": ("ML-FMM, %s passes, every box at the global order" %
+                       ("reference" if args.fmm_convention == 0 else "consistent") if args.operator == "mlfmm"
+                       else "direct (all pairs, rotation-axial-rotation)"),
             "z_coupling": "h_n^(1)" if sc.z_coupling == 3 else "j_n", "gmres_restart": sc.gmres_restart,
             "gmres_tolerance": sc.gmres_tolerance, "rhs": 1, "parallelism": "replicas x%d" % args.gpus,
             "l2": "Krylov basis (restart+1 vectors) exceeds L2; 256 MB L2 flush between steps"}
@@ -225,6 +301,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="medium", choices=["medium", "small"])
+    ap.add_argument("--operator", default="direct", choices=["direct", "mlfmm"],
+                    help="mlfmm: the ML-FMM passes (fmm_convention below) instead of all pairs")
+    ap.add_argument("--fmm-convention", type=int, default=0, choices=[0, 1])
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU sampling")
     ap.add_argument("--matvecs-per-solve", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -251,7 +330,9 @@ def main():
     from itofoggysim_b200 import solver
 
     sc = workload_scene(args.workload)
-    s = solver.MultiSphereSolver(sc, device=local)
+    fmm = args.operator == "mlfmm"
+    mk = lambda: solver.MultiSphereSolver(sc, device=local, use_ml_fmm=fmm, fmm_convention=args.fmm_convention)
+    s = mk()
     n = s.n
     xbuf = torch.empty(2 * n, dtype=torch.float64, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
@@ -290,6 +371,7 @@ def main():
     value = world * args.steps / (max_ms * 1e-3)
     x_dev = xbuf.cpu().numpy().view(np.complex128)
     berr = s.get_backward_error()
+    tree = s.build_tree() if fmm else None
     # the timed handle's pair tables take most of HBM; free them so the end-to-end handle gets
     # the same operator path
     s.close()
@@ -302,7 +384,7 @@ def main():
     for i in range(max(1, min(args.steps, 2))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        with solver.MultiSphereSolver(sc, device=local) as s2:
+        with mk() as s2:
             xh, st2 = s2.solve()
         torch.cuda.synchronize()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
@@ -317,14 +399,15 @@ def main():
     result = None
     if rank == 0:
         peak = measure_fp64_peak(torch, dev)
-        flops = algorithmic_flops(sc)
+        flops = (fmm_flops(sc, tree[0], tree[2], tree[3], sc.reference_row_rule) if fmm
+                 else algorithmic_flops(sc))
         avg_mv = mv_ms / max(mv_count, 1)
         achieved = flops / (avg_mv * 1e-3) / 1e12
         traffic = None
         tf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tf):
             with open(tf) as f:
-                traffic = json.load(f).get(sc.name)
+                traffic = json.load(f).get(sc.name + ("_mlfmm" if fmm else ""))
         result = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
@@ -335,7 +418,8 @@ def main():
                       "backward_error": berr, "ms_operator_per_solve": mv_ms / args.steps},
             "roofline": {"bound": "tensor", "compute": "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_direct (+k_direct_finish)", "flops_per_launch": flops,
+                         "kernel": ("k_translate (ML-FMM passes) + k_direct_finish" if fmm
+                                    else "k_direct (+k_direct_finish)"), "flops_per_launch": flops,
                          "ms_per_launch": avg_mv,
                          "peak_source": "cuBLAS FP64 DGEMM 8192^3 measured in this run (no FP64 figure in "
                                         "MEASURED_PEAKS.json)"},
