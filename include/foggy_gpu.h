@@ -219,6 +219,17 @@ int32_t foggy_universal_index(int32_t n, const double* points, int32_t l, int64_
  * Call with boxes == NULL to query the count. */
 int32_t foggy_tree_boxes(foggy_handle h, int32_t l, int64_t* boxes, int32_t* count);
 
+/* Scattered electric and magnetic field of the cluster at npoints points (3 doubles each):
+ * replaces lib_mie_ms_get_field (FoggySim/src/lib/mie_theory/lib_mie_multi_sphere.f90:379-434)
+ * with lib_mie_ss_get_field per sphere (lib_mie_single_sphere.f90:1397-1582) and the vector
+ * spherical wave functions of lib_math_vector_spherical_harmonics_components_real_xu
+ * (libmath/src/math/lib_math_vector_spherical_harmonics.f90:132-419): x holds the coefficients
+ * a_nm, b_nm in the reference layout, e_field_0 the amplitude |E0|; e_out and h_out receive 3
+ * complex cartesian components per point (H includes n_medium / c0).  Both fields are zero at a
+ * point inside any sphere, as in the reference.  mem applies to x, points, e_out and h_out. */
+int32_t foggy_get_field(foggy_handle h, const double* x, int32_t mem, int32_t npoints, const double* points,
+                        double e_field_0, double* e_out, double* h_out);
+
 /* Octree lists of box n at level l for the ML-FMM: kind 1 -> E1, the spheres in the box
  * (lib_tree_get_domain_e1, libtree/src/lib/lib_tree.f90:492-609); kind 2 -> E2, the spheres in
  * the box and its neighbours (lib_tree_get_domain_e2, :611-724); kind 4 -> I4, the level-l box

@@ -1246,6 +1246,57 @@ int32_t foggy_solve(foggy_handle h, const double* x0, double* x, int32_t mem, fo
 
 double foggy_get_backward_error(foggy_handle h) { return h ? h->last_berr : -1.0; }
 
+int32_t foggy_get_field(foggy_handle h, const double* x, int32_t mem, int32_t npoints, const double* points,
+                        double e_field_0, double* e_out, double* h_out) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!x || !points || !e_out || !h_out) return fail(h, FOGGY_ERR_ARGUMENT, "x, points, e_out or h_out is NULL");
+    if (npoints < 0) return fail(h, FOGGY_ERR_ARGUMENT, "npoints must be >= 0");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    if (npoints == 0) return FOGGY_OK;
+    CK(h, cudaSetDevice(h->device));
+    const size_t len = (size_t)foggy_vector_length(h);
+    const int C = (h->pg + 1) * (h->pg + 1) - 1;
+    std::vector<double> rad(h->N);
+    for (int j = 0; j < h->N; ++j) rad[j] = h->radius[h->pidx[j]];
+    const cplx* xd = reinterpret_cast<const cplx*>(x);
+    const double* pd = points;
+    cplx* ed = reinterpret_cast<cplx*>(e_out);
+    cplx* hd = reinterpret_cast<cplx*>(h_out);
+    // per-call buffers: sphere radii, and the points and fields when they live on the host
+    void* tmp = nullptr;
+    const size_t np = (size_t)npoints;
+    size_t bytes = rad.size() * sizeof(double);
+    if (mem == FOGGY_MEM_HOST) bytes += len * sizeof(cplx) + 3 * np * sizeof(double) + 6 * np * sizeof(cplx);
+    CK(h, cudaMalloc(&tmp, bytes));
+    double* d_rad = static_cast<double*>(tmp);
+    char* q = reinterpret_cast<char*>(d_rad + rad.size());
+    cudaError_t e = cudaMemcpyAsync(d_rad, rad.data(), rad.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (mem == FOGGY_MEM_HOST) {
+        cplx* xs = reinterpret_cast<cplx*>(q);
+        double* ps = reinterpret_cast<double*>(xs + len);
+        ed = reinterpret_cast<cplx*>(ps + 3 * np);
+        hd = ed + 3 * np;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(xs, x, len * sizeof(cplx), cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ps, points, 3 * np * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+        xd = xs;
+        pd = ps;
+    }
+    if (e == cudaSuccess) {
+        k_field<<<npoints, 128, 0, h->stream>>>(scene_view(h), d_rad, h->pg, C, xd, pd, e_field_0,
+                                                h->prm.n_medium / 299792458.0, ed, hd);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && mem == FOGGY_MEM_HOST) {
+        e = cudaMemcpyAsync(e_out, ed, 3 * np * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, hd, 3 * np * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("field: ") + cudaGetErrorString(e));
+    return FOGGY_OK;
+}
+
 int32_t foggy_cross_sections(foggy_handle h, const double* x, int32_t mem, double* out) {
     if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
     if (!x || !out) return fail(h, FOGGY_ERR_ARGUMENT, "x or out is NULL");

@@ -30,6 +30,9 @@ __global__ void k_unpack(SceneView sc, int pg, const double* g, const cplx* xref
 __global__ void k_pack(SceneView sc, int pg, const double* g, const cplx* ydev, const cplx* identity_ref,
                        cplx* yref);
 __global__ void k_cross_sections(SceneView sc, const cplx* x, const cplx* pq, double* part);
+// scattered E, H at points (reference layout coefficients x, C entries per part and sphere)
+__global__ void k_field(SceneView sc, const double* radius_s, int pg, int C, const cplx* x, const double* pts,
+                        double e0, double h_factor, cplx* E_out, cplx* H_out);
 
 // k_direct.cu -- all-pairs sphere coupling (the direct operator)
 // Tables of the Wigner small-d recurrence (degrees <= K).

@@ -2,6 +2,7 @@
 // the reference's flat coefficient vector and the device's ragged scaled layout, and the
 // cluster cross-sections.
 #include "foggy_kernels.cuh"
+#include "k_common.cuh"
 #include "k_special.cuh"
 
 namespace foggy {
@@ -272,6 +273,172 @@ __global__ void k_cross_sections(SceneView sc, const cplx* x, const cplx* pq, do
     if (threadIdx.x == 0) {
         part[2 * j] = red[0][0];
         part[2 * j + 1] = red[1][0];
+    }
+}
+
+// ---- scattered field at observation points (lib_mie_ms_get_field,
+// FoggySim/src/lib/mie_theory/lib_mie_multi_sphere.f90:379-434; per sphere lib_mie_ss_get_field,
+// lib_mie_single_sphere.f90:1397-1582; vector spherical wave functions of
+// lib_math_vector_spherical_harmonics_components_real_xu,
+// libmath/src/math/lib_math_vector_spherical_harmonics.f90:132-419) -------------------------------
+//   E += sum_nm E_nm i (a_nm N_nm + b_nm M_nm),  H += n_medium / c0 sum_nm E_nm (b_nm N_nm + a_nm M_nm)
+//   E_nm = |E0| (2n+1) (n-m)!/(n+m)! i^n, with h_n^(1) in M, N, per sphere in its own frame,
+// converted to cartesian components and summed; zero at a point inside any sphere.  One CTA per
+// point, each thread a strided subset of the spheres; Legendre functions (no Condon-Shortley
+// phase), pi_nm = m P_n^m / sin t and tau_nm = dP_n^m/dt by recurrence per order m.
+namespace {
+constexpr int kFieldThreads = 128;
+
+// contribution of degree n and order mm to the spherical components of E and H, given P_n^mm,
+// pi_n,mm, tau_n,mm and (n-mm)!/(n+mm)!
+__device__ __forceinline__ void field_term(int n, int mm, double P, double pv, double tv, double ratio, cplx zn,
+                                           cplx xid, double rho, cplx e, const cplx* a, const cplx* b, int base,
+                                           double e0, cplx* es, cplx* hs) {
+    const cplx Mt = mk(0.0, pv) * zn * e, Mp = (-tv) * (zn * e);
+    const cplx Nr = ((double)(n * (n + 1)) * P / rho) * (zn * e), Nt = (tv / rho) * (xid * e),
+               Np = (1.0 / rho) * (mk(0.0, pv) * (xid * e));
+    const cplx Enm = ipow_mul(n, mk(e0 * (2.0 * n + 1.0) * ratio, 0.0));
+    const cplx an = a[base + mm], bn = b[base + mm];
+    const cplx ie = mk(-Enm.y, Enm.x);   // i E_nm
+    es[0] = es[0] + ie * (an * Nr);
+    es[1] = es[1] + ie * (an * Nt + bn * Mt);
+    es[2] = es[2] + ie * (an * Np + bn * Mp);
+    hs[0] = hs[0] + Enm * (bn * Nr);
+    hs[1] = hs[1] + Enm * (bn * Nt + an * Mt);
+    hs[2] = hs[2] + Enm * (bn * Np + an * Mp);
+}
+}  // namespace
+
+__global__ void __launch_bounds__(kFieldThreads) k_field(SceneView sc, const double* radius_s, int pg, int C,
+                                                         const cplx* x, const double* pts, double e0,
+                                                         double h_factor, cplx* E_out, cplx* H_out) {
+    const int ip = blockIdx.x;
+    const int tid = threadIdx.x;
+    __shared__ int inside;
+    __shared__ double red[12][kFieldThreads];
+    if (tid == 0) inside = 0;
+    __syncthreads();
+    const double* pt = pts + 3 * (size_t)ip;
+    cplx acc[6];
+    for (int c = 0; c < 6; ++c) acc[c] = mk(0.0, 0.0);
+    double jb[2 * kMaxDegree + 4], yb[2 * kMaxDegree + 4];
+    for (int j = tid; j < sc.n; j += kFieldThreads) {
+        const double d0 = pt[0] - sc.centres[3 * (size_t)j];
+        const double d1 = pt[1] - sc.centres[3 * (size_t)j + 1];
+        const double d2 = pt[2] - sc.centres[3 * (size_t)j + 2];
+        const double r = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        if (!(r > radius_s[j])) {
+            inside = 1;
+            continue;
+        }
+        if (!(e0 > 1e-200)) continue;
+        const double th = (r == 0.0) ? 0.0 : acos(d2 / r);
+        const double ph = (d0 == 0.0 && d1 == 0.0) ? 0.0 : atan2(d1, d0);
+        const double rho = sc.k * r;
+        dev_sph_jn(rho, pg + 1, jb);
+        dev_sph_yn(rho, pg + 1, yb);
+        const double xc = cos(th), st = sin(th);
+        const bool pole = (xc == 1.0 || xc == -1.0);
+        const cplx* a = x + (size_t)2 * C * j;
+        const cplx* b = a + C;
+        cplx es[3] = {mk(0, 0), mk(0, 0), mk(0, 0)}, hs[3] = {mk(0, 0), mk(0, 0), mk(0, 0)};
+        // Q_n^m = P_n^m / sin t by the LPMNS recurrence; pi_nm = m Q_n^m, tau_nm = n x Q_n^m - (n+m) Q_{n-1}^m,
+        // tau_n0 = -P_n^1 = -sin t Q_n^1; negative orders from P_n^{-m} = f P_n^m, f = (-1)^m (n-m)!/(n+m)!
+        // (pi_{n,-m} = -f pi_nm, tau_{n,-m} = f tau_nm); at the poles the reference's table
+        // (lib_math_legendre.f90:854-920, without the phase)
+        double fact2m = 1.0;   // (2m)!
+        for (int m = 0; m <= pg; ++m) {
+            if (m > 0) fact2m *= (2.0 * m - 1.0) * (2.0 * m);
+            double sphi, cphi;
+            sincos((double)m * ph, &sphi, &cphi);
+            const cplx ep = mk(cphi, sphi), em = mk(cphi, -sphi);
+            const int mq = m == 0 ? 1 : m;   // order of the Q sequence (Q^1 for tau_n0)
+            double qmm = 1.0;
+            for (int q = 1; q <= mq; ++q) qmm *= (2.0 * q - 1.0);
+            for (int q = 1; q < mq; ++q) qmm *= st;
+            double qc = qmm, qprev = 0.0;                       // Q_n^mq at n = mq, and n - 1
+            double pc = m == 0 ? 1.0 : qmm * st, pprev = 0.0;   // P_n^m at n = m, and n - 1
+            double fr = 1.0 / fact2m;                           // (n-m)!/(n+m)! at n = m
+            int nq = mq, np_ = m;
+            for (int n = max(m, 1); n <= pg; ++n) {
+                while (np_ < n) {   // advance P_n^m and (n-m)!/(n+m)!
+                    ++np_;
+                    const double pn = ((2.0 * np_ - 1.0) * xc * pc - (np_ + m - 1.0) * pprev) / (np_ - m);
+                    pprev = pc;
+                    pc = pn;
+                    fr *= (double)(np_ - m) / (double)(np_ + m);
+                }
+                while (nq < n) {    // advance Q_n^mq
+                    ++nq;
+                    const double qn = ((2.0 * nq - 1.0) * xc * qc - (nq + mq - 1.0) * qprev) / (nq - mq);
+                    qprev = qc;
+                    qc = qn;
+                }
+                const cplx zn = mk(jb[n], yb[n]);
+                const cplx zm1 = mk(jb[n - 1], yb[n - 1]), zp1 = mk(jb[n + 1], yb[n + 1]);
+                const cplx xid = 0.5 * (rho * zm1 + zn - rho * zp1);
+                const int base = n * n - 1 + n;
+                if (m == 0) {
+                    const double P0 = pole ? ((xc < 0.0 && (n & 1)) ? -1.0 : 1.0) : pc;
+                    const double t0 = pole ? 0.0 : -st * qc;
+                    field_term(n, 0, P0, 0.0, t0, 1.0, zn, xid, rho, ep, a, b, base, e0, es, hs);
+                    continue;
+                }
+                double pip, taup, pim, taum, Pp, Pm;
+                if (pole) {
+                    Pp = Pm = 0.0;
+                    pip = taup = pim = taum = 0.0;
+                    if (m == 1) {
+                        const double N2 = (double)(n * (n + 1) / 2);
+                        if (xc > 0.0) {
+                            pip = N2; pim = 0.5; taup = N2; taum = -0.5;
+                        } else if ((n & 1) == 0) {
+                            pip = -N2; pim = -0.5; taup = N2; taum = -0.5;
+                        } else {
+                            pip = N2; pim = 0.5; taup = -N2; taum = -0.5;
+                        }
+                    }
+                } else {
+                    const double f = (m & 1) ? -fr : fr;
+                    Pp = pc;
+                    Pm = f * pc;
+                    pip = m * qc;
+                    taup = n * xc * qc - (n + m) * qprev;
+                    pim = -f * pip;
+                    taum = f * taup;
+                }
+                field_term(n, m, Pp, pip, taup, fr, zn, xid, rho, ep, a, b, base, e0, es, hs);
+                field_term(n, -m, Pm, pim, taum, 1.0 / fr, zn, xid, rho, em, a, b, base, e0, es, hs);
+            }
+        }
+        const double ct = xc, cp = cos(ph), sp = sin(ph);
+        const cplx ex = st * cp * es[0] + ct * cp * es[1] - sp * es[2];
+        const cplx ey = st * sp * es[0] + ct * sp * es[1] + cp * es[2];
+        const cplx ez = ct * es[0] - st * es[1];
+        const cplx hx = st * cp * hs[0] + ct * cp * hs[1] - sp * hs[2];
+        const cplx hy = st * sp * hs[0] + ct * sp * hs[1] + cp * hs[2];
+        const cplx hz = ct * hs[0] - st * hs[1];
+        acc[0] = acc[0] + ex;
+        acc[1] = acc[1] + ey;
+        acc[2] = acc[2] + ez;
+        acc[3] = acc[3] + h_factor * hx;
+        acc[4] = acc[4] + h_factor * hy;
+        acc[5] = acc[5] + h_factor * hz;
+    }
+    for (int c = 0; c < 6; ++c) {
+        red[2 * c][tid] = acc[c].x;
+        red[2 * c + 1][tid] = acc[c].y;
+    }
+    __syncthreads();
+    for (int s_ = kFieldThreads / 2; s_ > 0; s_ >>= 1) {
+        if (tid < s_)
+            for (int c = 0; c < 12; ++c) red[c][tid] += red[c][tid + s_];
+        __syncthreads();
+    }
+    if (tid < 6) {
+        const cplx v = inside ? mk(0.0, 0.0) : mk(red[2 * tid][0], red[2 * tid + 1][0]);
+        if (tid < 3) E_out[3 * (size_t)ip + tid] = v;
+        else H_out[3 * (size_t)ip + tid - 3] = v;
     }
 }
 

@@ -181,6 +181,18 @@ class MultiSphereSolver:
         N.check(self.L.foggy_cross_sections(self.h, x.ctypes.data, N.FOGGY_MEM_HOST, N.ptr(out)), self.h)
         return out
 
+    def get_field(self, x, points, e_field_0=1.0):
+        """Scattered E and H (complex, shape (npoints, 3), cartesian) of coefficients x at points
+        (lib_mie_ms_get_field); zero inside a sphere."""
+        x = N.as_c128(x)
+        pts = N.as_f64(points).reshape(-1)
+        npt = len(pts) // 3
+        E = np.zeros(3 * npt, np.complex128)
+        H = np.zeros(3 * npt, np.complex128)
+        N.check(self.L.foggy_get_field(self.h, x.ctypes.data, N.FOGGY_MEM_HOST, npt, pts.ctypes.data,
+                                       float(e_field_0), E.ctypes.data, H.ctypes.data), self.h)
+        return E.reshape(npt, 3), H.reshape(npt, 3)
+
     # ---- libtree -----------------------------------------------------------------------
     def build_tree(self):
         n = self.scene.n_spheres

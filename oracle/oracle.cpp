@@ -834,6 +834,88 @@ int orc_build_tree(int n, const double* centres, int s, int l_max_fixed, int64_t
 }  // extern "C"
 
 // ------------------------------------------------------------------------------------------
+// Field at observation points (lib_mie_ms_get_field, FoggySim/src/lib/mie_theory/
+// lib_mie_multi_sphere.f90:379-434, per sphere lib_mie_ss_get_field,
+// lib_mie_single_sphere.f90:1397-1582) with the vector spherical wave functions of
+// lib_math_vector_spherical_harmonics_components_real_xu
+// (libmath/src/math/lib_math_vector_spherical_harmonics.f90:132-419):
+//   M_nm = (0, i pi_nm z_n, -tau_nm z_n) e^{im phi}
+//   N_nm = (n(n+1) P_n^m z_n / rho, tau_nm xi_n'/rho, i pi_nm xi_n'/rho) e^{im phi},
+// rho = k r, xi_n = rho z_n, xi_n' = (xi_{n-1} + z_n - xi_{n+1}) / 2 (lib_math_bessel.f90:2115-2143),
+// Legendre functions without the Condon-Shortley phase.  Components (rho, theta, phi).
+// ------------------------------------------------------------------------------------------
+void vswf(double theta, double phi, double r, double k, int nmax, int z, cd* M, cd* N) {
+    double rho = k * r;
+    std::vector<cd> zn(nmax + 2);
+    sph_z(z, rho, nmax + 1, zn.data());
+    std::vector<double> pi((nmax + 1) * (nmax + 1)), tau((nmax + 1) * (nmax + 1)), P((nmax + 1) * (nmax + 1));
+    pi_tau_table(theta, nmax, 0, pi.data(), tau.data());
+    legendre_table(std::cos(theta), nmax, P.data());
+    for (int n = 1; n <= nmax; ++n) {
+        cd xid = (rho * zn[n - 1] + zn[n] - rho * zn[n + 1]) / 2.0;
+        for (int m = -n; m <= n; ++m) {
+            int t = n * (n + 1) + m;
+            cd e(std::cos(m * phi), std::sin(m * phi));
+            size_t o = 3 * (size_t)(n * n - 1 + n + m);
+            M[o + 0] = 0.0;
+            M[o + 1] = cd(0.0, pi[t]) * zn[n] * e;
+            M[o + 2] = -tau[t] * zn[n] * e;
+            N[o + 0] = (double)(n * (n + 1)) * P[t] / rho * zn[n] * e;
+            N[o + 1] = tau[t] * (xid * e / rho);
+            N[o + 2] = cd(0.0, pi[t]) * (xid * e / rho);
+        }
+    }
+}
+
+// E and H of the scattered field of all spheres at one point (zero inside any sphere); the
+// coefficients x in the reference layout, the global degree range for every sphere.
+void field_at(const Problem& P, const cd* x, const double* pt, double e0, cd* E, cd* H) {
+    const double c0 = 299792458.0;
+    for (int c = 0; c < 3; ++c) E[c] = H[c] = 0.0;
+    int C = P.cnt();
+    int nmax = P.n2;
+    std::vector<cd> M(3 * (size_t)C), N(3 * (size_t)C);
+    for (int j = 0; j < P.N; ++j) {
+        double d[3];
+        for (int c = 0; c < 3; ++c) d[c] = pt[c] - P.centres[3 * j + c];
+        double r, th, ph;
+        to_spherical(d, &r, &th, &ph);
+        if (!(r > P.radius[P.pidx[j]])) {
+            for (int c = 0; c < 3; ++c) E[c] = H[c] = 0.0;
+            return;
+        }
+        if (!(e0 > 1e-200)) continue;
+        vswf(th, ph, r, P.k, nmax, 3, M.data(), N.data());
+        const cd* a = x + (size_t)2 * C * j;
+        const cd* b = a + C;
+        cd es[3] = {0.0, 0.0, 0.0}, hs[3] = {0.0, 0.0, 0.0};
+        for (int n = 1; n <= nmax; ++n) {
+            cd en[3] = {0.0, 0.0, 0.0}, hn[3] = {0.0, 0.0, 0.0};
+            for (int m = -n; m <= n; ++m) {
+                int o = blk(P.n1, n, m);
+                cd f = std::fabs(e0) * (2.0 * n + 1.0) * nmm_over_npm(n, m) * ipow(n);
+                size_t q = 3 * (size_t)(n * n - 1 + n + m);
+                for (int c = 0; c < 3; ++c) {
+                    en[c] += cd(0.0, 1.0) * f * (a[o] * N[q + c] + b[o] * M[q + c]);
+                    hn[c] += f * (b[o] * N[q + c] + a[o] * M[q + c]);
+                }
+            }
+            for (int c = 0; c < 3; ++c) { es[c] += en[c]; hs[c] += hn[c]; }
+        }
+        double ct = std::cos(th), st = std::sin(th), cp = std::cos(ph), sp = std::sin(ph);
+        cd ex = es[0] * (st * cp) + es[1] * (ct * cp) - es[2] * sp;
+        cd ey = es[0] * (st * sp) + es[1] * (ct * sp) + es[2] * cp;
+        cd ez = es[0] * ct - es[1] * st;
+        cd hx = hs[0] * (st * cp) + hs[1] * (ct * cp) - hs[2] * sp;
+        cd hy = hs[0] * (st * sp) + hs[1] * (ct * sp) + hs[2] * cp;
+        cd hz = hs[0] * ct - hs[1] * st;
+        double fh = P.n_medium / c0;
+        E[0] += ex; E[1] += ey; E[2] += ez;
+        H[0] += fh * hx; H[1] += fh * hy; H[2] += fh * hz;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // ML-FMM operator of the reference: libmlfmm/src/lib/lib_ml_fmm.f90 (upward pass :387-640,
 // downward pass :656-982, final summation :994-1204) with the Mie handles of
 // FoggySim/src/lib/mie_theory/lib_mie_ms_ml_fmm_interface.f90 (get_u_B_i :259-379,
@@ -1372,6 +1454,23 @@ int orc_tree_domain(int N, const double* centres, int l_max_fixed, int l, int64_
     if (kind == 4) v = fmmo::i4(n, l);
     if (out) for (int i = 0; i < (int)v.size() && i < cap; ++i) out[i] = v[i];
     return (int)v.size();
+}
+
+
+// M_nm, N_nm (see vswf) for n = 1..nmax: 3 complex components per (n, m) at index n^2-1+n+m
+int orc_vswf(double theta, double phi, double r, double k, int nmax, int z, double* M, double* N) {
+    vswf(theta, phi, r, k, nmax, z, reinterpret_cast<cd*>(M), reinterpret_cast<cd*>(N));
+    return 0;
+}
+
+// scattered E and H (3 complex each per point) of coefficient vector x at npts points
+int orc_field(void* p, const double* x, int npts, const double* pts, double e0, double* E, double* H) {
+    Problem* P = static_cast<Problem*>(p);
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < npts; ++i)
+        field_at(*P, reinterpret_cast<const cd*>(x), pts + 3 * (size_t)i, e0,
+                 reinterpret_cast<cd*>(E) + 3 * (size_t)i, reinterpret_cast<cd*>(H) + 3 * (size_t)i);
+    return 0;
 }
 
 }  // extern "C"

@@ -287,3 +287,33 @@ def tree_domain(centres, l_max, l, n, kind):
     out = np.zeros(max(cnt, 1), np.int64)
     L.orc_tree_domain(len(c) // 3, c, int(l_max), int(l), int(n), int(kind), out.ctypes.data, cnt)
     return out[:cnt]
+
+
+def vswf(theta, phi, r, k, nmax, z=3):
+    """M_nm, N_nm (n = 1..nmax, m = -n..n) as complex arrays [(n, m), (rho, theta, phi)]."""
+    L = lib()
+    if not getattr(L, "_vswf_sig", False):
+        L.orc_vswf.argtypes = [C.c_double] * 4 + [C.c_int, C.c_int, dp, dp]
+        L._vswf_sig = True
+    cnt = (nmax + 1) ** 2 - 1
+    M = np.zeros(6 * cnt)
+    N = np.zeros(6 * cnt)
+    L.orc_vswf(theta, phi, r, k, nmax, z, M, N)
+    return M.view(np.complex128).reshape(cnt, 3), N.view(np.complex128).reshape(cnt, 3)
+
+
+def _field(self, x, points, e0=1.0):
+    """Scattered E, H (complex, shape (npoints, 3)) of coefficients x (reference layout)."""
+    L = lib()
+    if not getattr(L, "_field_sig", False):
+        L.orc_field.argtypes = [C.c_void_p, dp, C.c_int, dp, C.c_double, dp, dp]
+        L._field_sig = True
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1)
+    n = len(pts) // 3
+    E = np.zeros(6 * n)
+    H = np.zeros(6 * n)
+    L.orc_field(self.h, _c(x), n, pts, float(e0), E, H)
+    return E.view(np.complex128).reshape(n, 3), H.view(np.complex128).reshape(n, 3)
+
+
+Problem.field = _field

@@ -11,6 +11,9 @@ golden values of the reference's Fortran unit tests (read as text, never compile
       FoggySim/ground_truth/lib_math_vector_spherical_harmonics/ (x=2, theta=0.5, phi=0.5 and
       phi=2*pi-0.5, n,nu <= 5, z=3; consumed at
       libmath/src/math/lib_math_vector_spherical_harmonics.f90:2876-3168)
+  * ground_truth_M_mn.csv, ground_truth_N_mn.csv
+      same folder (theta=0.2, phi=0, k=2 pi, r=50, z=3, n <= 4; consumed at
+      libmath/src/math/lib_math_vector_spherical_harmonics.f90:2443-2575, tolerance 1e-13)
   * inline_goldens.json with
       wigner_3j          libmath/src/math/lib_math_wigner.f90:140-164
       ab_xu_cruzan       libmath/src/math/lib_math_vector_spherical_harmonics.f90:2799-2875
@@ -53,7 +56,8 @@ def data_block(path, a, b, name):
 
 def main(ref):
     vsh = os.path.join(ref, "FoggySim/ground_truth/lib_math_vector_spherical_harmonics")
-    for fn in ("ground_truth_AB_mnmunu.csv", "ground_truth_AB_mnmunu_minus_phi.csv"):
+    for fn in ("ground_truth_AB_mnmunu.csv", "ground_truth_AB_mnmunu_minus_phi.csv", "ground_truth_M_mn.csv",
+               "ground_truth_N_mn.csv"):
         shutil.copyfile(os.path.join(vsh, fn), os.path.join(HERE, fn))
 
     g = {}
