@@ -138,12 +138,82 @@ module foggy_gpu_f
             integer(c_int32_t), value :: j1, j2, j3, m1, m2, m3
             real(c_double) :: w
         end function
+        function foggy_last_error(h) result(msg) bind(c, name="foggy_last_error")
+            import :: c_ptr
+            type(c_ptr), value :: h
+            type(c_ptr) :: msg                ! NUL-terminated C string owned by the library
+        end function
+        function foggy_set_params(h, p) result(rc) bind(c, name="foggy_set_params")
+            import :: c_ptr, c_int32_t, foggy_params
+            type(c_ptr), value :: h
+            type(foggy_params), intent(in) :: p
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_get_mie_coefficients(h, ip, a, b) result(rc) bind(c, name="foggy_get_mie_coefficients")
+            import :: c_ptr, c_int32_t, c_double_complex
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: ip
+            complex(c_double_complex), intent(out) :: a(*), b(*)
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_get_vector_b(h, b, mem) result(rc) bind(c, name="foggy_get_vector_b")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: h, b
+            integer(c_int32_t), value :: mem
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_build_tree(h, uindex, order, l_min, l_max) result(rc) bind(c, name="foggy_build_tree")
+            import :: c_ptr, c_int32_t, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int64_t), intent(out) :: uindex(*)
+            integer(c_int32_t), intent(out) :: order(*), l_min, l_max
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_universal_index(n, points, l, out) result(rc) bind(c, name="foggy_universal_index")
+            import :: c_int32_t, c_int64_t, c_double
+            integer(c_int32_t), value :: n, l
+            real(c_double), intent(in) :: points(3, *)
+            integer(c_int64_t), intent(out) :: out(*)
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_tree_boxes(h, l, boxes, count) result(rc) bind(c, name="foggy_tree_boxes")
+            import :: c_ptr, c_int32_t, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: l
+            type(c_ptr), value :: boxes         ! c_loc(boxes(1)), or c_null_ptr to query count
+            integer(c_int32_t), intent(inout) :: count
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_tree_domain(h, l, n, kind, out, count) result(rc) bind(c, name="foggy_tree_domain")
+            import :: c_ptr, c_int32_t, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: l, kind
+            integer(c_int64_t), value :: n
+            type(c_ptr), value :: out           ! c_loc(out(1)), or c_null_ptr to query count
+            integer(c_int32_t), intent(inout) :: count
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_get_field(h, x, mem, npoints, points, e_field_0, e_out, h_out) result(rc) &
+                bind(c, name="foggy_get_field")
+            import :: c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h, x, points, e_out, h_out
+            integer(c_int32_t), value :: mem, npoints
+            real(c_double), value :: e_field_0
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_matvec_static(h, x, y) result(rc) bind(c, name="foggy_matvec_static")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: h, x, y       ! device pointers
+            integer(c_int32_t) :: rc
+        end function
     end interface
 
     public :: foggy_default_params, foggy_create, foggy_destroy, foggy_set_spheres
     public :: foggy_set_plane_waves, foggy_vector_length, foggy_matvec, foggy_solve
     public :: foggy_get_backward_error, foggy_cross_sections, foggy_translation_coefficients
-    public :: foggy_wigner_3j
+    public :: foggy_wigner_3j, foggy_last_error, foggy_set_params, foggy_get_mie_coefficients
+    public :: foggy_get_vector_b, foggy_build_tree, foggy_universal_index, foggy_tree_boxes
+    public :: foggy_tree_domain, foggy_get_field, foggy_matvec_static
     public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
     public :: foggy_ms_get_backward_error, foggy_ms_destructor
 

@@ -101,3 +101,10 @@ def test_argument_errors_are_reported(native):
     p.n_range[1] = 5
     p.gmres_restart = 500
     assert native.foggy_create(C.byref(p), 0, C.byref(h)) == _native.FOGGY_ERR_ARGUMENT
+
+
+def test_fortran_module_binds_every_header_symbol():
+    """The iso_c_binding module declares a bind(c) interface for every entry point of the header."""
+    with open(os.path.join(ROOT, "itofoggysim_b200", "fortran", "foggy_gpu_f.f90")) as f:
+        bound = set(re.findall(r'name="(foggy_[a-z0-9_]+)"', f.read()))
+    assert set(declared_functions()) - bound == set()
