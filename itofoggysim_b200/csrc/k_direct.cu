@@ -58,6 +58,7 @@ namespace foggy {
 
 namespace {
 constexpr int kThreads = 256;
+constexpr int kPrefetch5 = 4;   // coaxial entries loaded ahead per thread
 
 // offset of degree j in the folded [+ 0..j | - 0..j] layout (2(j+1) entries per degree)
 __host__ __device__ __forceinline__ int off2(int j) { return (j - 1) * (j + 2); }
@@ -355,7 +356,7 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
             const double c1m = (mu - 1 >= lo) ? x * 2.0 * (mu - 1) * c.dt.rs[mu * W + k] / (2.0 * mu - 1.0) : 0.0;
             const double c2p = (mu + 1 <= pl) ? x * 2.0 * (mu + 2) * c.dt.rs[(mu + 1) * W + k] / (2.0 * mu + 3.0) : 0.0;
             const double bk2 = 2.0 * k * x;
-            cplx* w = s.B + 4 * t;
+            cplx* w = s.B + t;   // four planes of `items` entries: a'(+k), b'(+k), a'(-k), b'(-k)
 #pragma unroll
             for (int sg = 0; sg < 2; ++sg) {
                 const int kk = sg ? -k : k;
@@ -372,8 +373,8 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
                 // wa = c0 a + i (bs b + c1m a_- - c2p a_+),  wb = c0 b + i (bs a + c1m b_- - c2p b_+)
                 const cplx ia = bs * bv[1] + c1m * av[0] - c2p * av[2];
                 const cplx ib = bs * av[1] + c1m * bv[0] - c2p * bv[2];
-                w[2 * sg] = mk(c0 * av[1].x - ia.y, c0 * av[1].y + ia.x);
-                w[2 * sg + 1] = mk(c0 * bv[1].x - ib.y, c0 * bv[1].y + ib.x);
+                w[2 * sg * items] = mk(c0 * av[1].x - ia.y, c0 * av[1].y + ia.x);
+                w[(2 * sg + 1) * items] = mk(c0 * bv[1].x - ib.y, c0 * bv[1].y + ib.x);
             }
         }
     }
@@ -382,6 +383,7 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
     {
         // rows(k) = pj - max(1, k) + 1: k = 0 and k = 1 both have pj rows
         const int rows_tot = pj + (kmax >= 1 ? kmax * pj - (kmax - 1) * kmax / 2 : 0);
+        const int NW = (kmax + 1) * (pl + 2) - kmax * (kmax + 1) / 2;   // w plane stride
         const int M2 = max(pj, pl) + 2;
         for (int t = tid; t < rows_tot; t += kThreads) {
             int k = 0, rem = t;
@@ -392,19 +394,35 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
                 ++k;
             }
             const int n = max(1, k) + rem;
-            const cplx* w = s.B + 4 * (k * (pl + 2) - k * (k - 1) / 2);
+            const cplx* w = s.B + (k * (pl + 2) - k * (k - 1) / 2);
             const int cnt = pl + 2 - k;
             double r0x = 0, r0y = 0, r1x = 0, r1y = 0, r2x = 0, r2y = 0, r3x = 0, r3y = 0;
             if (tabs) {
                 const int Wk = M2 - k;
-                const cplx* sp = pair_s + pair_block_offset(k, M2, M2) + (n - k);
-                for (int q = 0; q < cnt; ++q) {
-                    const double2 sv = __ldcg(reinterpret_cast<const double2*>(sp + q * Wk));
+                const double2* sp = reinterpret_cast<const double2*>(pair_s + pair_block_offset(k, M2, M2) + (n - k));
+                // kPrefetch5 coaxial entries in flight per thread: the rows come from L2, so the loop
+                // is bounded by how many loads overlap, not by the multiply-adds
+                int q = 0;
+                for (; q + kPrefetch5 <= cnt; q += kPrefetch5) {
+                    double2 sv[kPrefetch5];
+#pragma unroll
+                    for (int u = 0; u < kPrefetch5; ++u) sv[u] = __ldcg(sp + (q + u) * Wk);
+#pragma unroll
+                    for (int u = 0; u < kPrefetch5; ++u) {
+                        const cplx S = mk(sv[u].x, sv[u].y);
+                        cmac(r0x, r0y, S, w[q + u]);
+                        cmac(r1x, r1y, S, w[NW + q + u]);
+                        cmac(r2x, r2y, S, w[2 * NW + q + u]);
+                        cmac(r3x, r3y, S, w[3 * NW + q + u]);
+                    }
+                }
+                for (; q < cnt; ++q) {
+                    const double2 sv = __ldcg(sp + q * Wk);
                     const cplx S = mk(sv.x, sv.y);
-                    cmac(r0x, r0y, S, w[4 * q]);
-                    cmac(r1x, r1y, S, w[4 * q + 1]);
-                    cmac(r2x, r2y, S, w[4 * q + 2]);
-                    cmac(r3x, r3y, S, w[4 * q + 3]);
+                    cmac(r0x, r0y, S, w[q]);
+                    cmac(r1x, r1y, S, w[NW + q]);
+                    cmac(r2x, r2y, S, w[2 * NW + q]);
+                    cmac(r3x, r3y, S, w[3 * NW + q]);
                 }
             } else {
                 const int W = c.g.NM - k + 1;
@@ -422,10 +440,10 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
                         sy += gq * s.zeta[p].y;
                     }
                     const cplx S = mk(sx, sy);
-                    cmac(r0x, r0y, S, w[4 * q]);
-                    cmac(r1x, r1y, S, w[4 * q + 1]);
-                    cmac(r2x, r2y, S, w[4 * q + 2]);
-                    cmac(r3x, r3y, S, w[4 * q + 3]);
+                    cmac(r0x, r0y, S, w[q]);
+                    cmac(r1x, r1y, S, w[NW + q]);
+                    cmac(r2x, r2y, S, w[2 * NW + q]);
+                    cmac(r3x, r3y, S, w[3 * NW + q]);
                 }
             }
             const double f = sgn(k) / (2.0 * n * (n + 1.0));

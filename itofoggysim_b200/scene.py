@@ -166,3 +166,75 @@ def random_cluster(n, seed, p=None, box=None, radii=None, z_coupling=3, referenc
     sc = make_scene(radii, box, seed, n_max=p, m=m, z_coupling=z_coupling,
                     reference_row_rule=bool(reference_row_rule), **kw)
     return sc
+
+
+# ---- hcp lattice scenes (FoggySim/src/lib/scene/lib_scene_generator.f90:53-280) -------------
+
+def hcp_lattice(i, j, k, sphere_radius):
+    """Centre of hcp site (i, j, k) for spheres of the given radius
+    (lib_scene_gerator_hcp_lattice, lib_scene_generator.f90:53-67)."""
+    x = 2.0 * i + math.fmod(float(j + k), 2.0)
+    y = math.sqrt(3.0) * (j + math.fmod(float(k), 2.0) / 3.0)
+    z = 2.0 * math.sqrt(6.0) * k / 3.0
+    return np.array([x, y, z]) * sphere_radius
+
+
+def hcp_fill_cuboid(size_x, size_y, size_z, sphere_radius):
+    """hcp sites filling a cuboid, centred on the origin, in the reference's (i, j, k) order
+    (lib_scene_generator_hcp_lattice_fill_cuboid, lib_scene_generator.f90:69-135)."""
+    r = sphere_radius
+    max_k = max(int(math.floor((size_z - 2.0 * r) / r * 3.0 / (2.0 * math.sqrt(6.0)))), 0)
+    max_j = max(int(math.floor((size_y - 2.0 * r) / r / math.sqrt(3.0) - math.fmod(float(max_k), 2.0) / 3.0)), 0)
+    max_i = max(int(math.floor(((size_x - 2.0 * r) / r - math.fmod(float(max_j + max_k), 2.0)) / 2.0)), 0)
+    offset = -hcp_lattice(max_i, max_j, max_k, r) / 2.0
+    out = np.empty(((max_i + 1) * (max_j + 1) * (max_k + 1), 3))
+    x = 0
+    for i in range(max_i + 1):
+        for j in range(max_j + 1):
+            for k in range(max_k + 1):
+                out[x] = hcp_lattice(i, j, k, r) + offset
+                x += 1
+    return out
+
+
+def hcp_fill_sphere(sphere_radius, lattice_sphere_radius, cap_plane_point=None, cap_plane_normal=None):
+    """hcp sites inside a sphere (optionally the cap on the negative side of a plane), as the mask
+    the reference keeps beside the cuboid lattice (lib_scene_generator_hcp_lattice_fill_sphere,
+    lib_scene_generator.f90:137-203): a site is inside when |c| < R - r/2 and, with a cap plane,
+    (c - point) . normal < 0 (the normal as given, not normalised, as the reference uses it)."""
+    cub = hcp_fill_cuboid(2.0 * sphere_radius, 2.0 * sphere_radius, 2.0 * sphere_radius, lattice_sphere_radius)
+    rho = np.sqrt(np.sum(cub * cub, axis=1))
+    inside = rho < sphere_radius - lattice_sphere_radius / 2.0
+    if cap_plane_point is not None and cap_plane_normal is not None:
+        dist = (cub - np.asarray(cap_plane_point, np.float64)) @ np.asarray(cap_plane_normal, np.float64)
+        inside &= dist < 0.0
+    return cub, inside
+
+
+def hcp_sphere_scene(sphere_radius, lattice_sphere_radius=0.0076, particle_radius=0.0075,
+                     n_particle=complex(2.5287, 0.0), lambda_0=0.55):
+    """The scene of the reference's hcp benchmark (lib_mie_ms_benchmark, calculate_sphere_scene,
+    FoggySim/src/lib/mie_theory/lib_mie_multi_sphere.f90:3717-4164), in micrometres: particles of
+    radius 7.5 nm, refractive index 2.5287, on an hcp lattice of 7.6 nm spheres filling the half
+    (z < 0) of a sphere of the given radius; n_medium = 1, lambda = 550 nm; one plane wave along +z
+    from (0, 0, -10 um), linear polarisation rotated by pi/4; z = j_n for the coupling.
+    n_max = ceil(1.2 n_c) with the reference's n_c = ceil(x + 4.05 x^(1/3) + 2), the degree its
+    convergence test (lib_mie_ss_test_convergence_plane_wave, lib_mie_single_sphere.f90:1604-1674)
+    returns for these absolutely convergent Rayleigh-size series."""
+    cub, inside = hcp_fill_sphere(sphere_radius, lattice_sphere_radius, (0.0, 0.0, 0.0), (0.0, 0.0, 1.0))
+    centres = cub[inside]
+    n_medium = 1.0
+    x = 2.0 * math.pi * n_medium * particle_radius / lambda_0
+    n_c = int(math.ceil(x + 4.05 * x ** (1.0 / 3.0) + 2.0))
+    n_max = int(math.ceil(n_c * 1.2))
+    c = math.cos(math.pi / 4.0)
+    s = math.sin(math.pi / 4.0)
+    waves = dict(wave_theta=np.array([0.0]), wave_phi=np.array([0.0]),
+                 jones=np.array([[c, 0.0, s, 0.0]]), wave_g=np.array([1.0]),
+                 wave_phase=np.array([0.0]), wave_d0=np.array([[0.0, 0.0, -10.0]]))
+    n = len(centres)
+    return Scene(lambda_0=lambda_0, n_medium=n_medium, centres=np.ascontiguousarray(centres),
+                 param_index=np.zeros(n, np.int32), refractive_index=np.array([n_particle], np.complex128),
+                 radius=np.array([particle_radius]), n_range_param=np.array([[1, n_max]], np.int32),
+                 n_range=(1, n_max), z_coupling=1, reference_row_rule=True, gmres_restart=10,
+                 gmres_tolerance=1e-6, name="hcp_sphere_%g" % sphere_radius, **waves)
