@@ -163,11 +163,69 @@ class MultiSphereSolver:
         N.check(rc, self.h)
         return self.last_stats
 
-    def calculate_scattering_coefficients_ab_nm(self):
-        """lib_mie_ms_calculate_scattering_coefficients_ab_nm: solve and split the solution into
-        per-sphere a_nm, b_nm arrays (n = 1..n_max, m = -n..n flattened)."""
-        x, st = self.solve()
-        return self.split(x), st
+    def set_n_range(self, n_range):
+        """lib_mie_ms_solver_set_n_range (lib_mie_ms_solver_interface.f90:174-189): the global degree
+        range; each sphere is truncated at the smaller of its own and the global n_max."""
+        self.params.n_range[0] = int(n_range[0])
+        self.params.n_range[1] = int(n_range[1])
+        self._set()
+        self.n = int(self.L.foggy_vector_length(self.h))
+
+    def n_range(self):
+        return int(self.params.n_range[0]), int(self.params.n_range[1])
+
+    @staticmethod
+    def embed(x, n_spheres, n_from, n_to):
+        """Coefficients of degree range (1, n_from) in the layout of (1, n_to): common degrees
+        copied, the rest zero, as lib_mie_ms_solver_get_vector_x_all rebuilds the initial guess
+        from the stored per-sphere a_nm, b_nm (lib_mie_ms_solver_interface.f90:467-520)."""
+        cf = (n_from + 1) ** 2 - 1
+        ct = (n_to + 1) ** 2 - 1
+        cm = min(cf, ct)
+        src = np.asarray(x).reshape(n_spheres, 2, cf)
+        out = np.zeros((n_spheres, 2, ct), np.complex128)
+        out[:, :, :cm] = src[:, :, :cm]
+        return out.reshape(-1)
+
+    def calculate_scattering_coefficients_ab_nm(self, update_initial_guess_with_n_max=None, step_size=None,
+                                                dynamic_step_size=False):
+        """lib_mie_ms_calculate_scattering_coefficients_ab_nm
+        (FoggySim/src/lib/mie_theory/lib_mie_multi_sphere.f90:162-371): solve, optionally first at a
+        lower n_max whose solution seeds the next solve (n_max continuation), and split the solution
+        into per-sphere a_nm, b_nm arrays (n = 1..n_max, m = -n..n flattened).  Each stage's
+        solution is the next stage's initial guess when the handle uses initial guesses (the
+        reference stores every run's solution in its sphere list and reads it back only then).
+        The stages run are listed in self.continuation_log as dicts (n_max, max_iterations,
+        iterations, backward_error)."""
+        n_org = self.n_range()
+        max_it_org = int(self.params.gmres_max_iterations)
+        state = {"x": None, "n": None}
+        self.continuation_log = []
+
+        def run(n_max, max_iterations):
+            if n_max != self.n_range()[1]:
+                self.set_n_range((n_org[0], n_max))
+            if max_iterations is not None:
+                self.set_max_iterations(max_iterations)
+            x0 = None
+            if self.params.use_initial_guess and state["x"] is not None:
+                x0 = self.embed(state["x"], self.scene.n_spheres, state["n"], n_max)
+            x, st = self.solve(x0, raise_on_error=False)
+            state["x"], state["n"] = x, n_max
+            self.continuation_log.append(dict(n_max=n_max, max_iterations=int(self.params.gmres_max_iterations),
+                                              iterations=st["iterations"], backward_error=st["backward_error"]))
+            return st["backward_error"]
+
+        try:
+            continuation_stages(run, n_org[1], update_initial_guess_with_n_max, step_size, dynamic_step_size)
+        finally:
+            if self.n_range() != n_org:
+                self.set_n_range(n_org)
+            self.set_max_iterations(max_it_org)
+        st = self.last_stats
+        if st["status"] != 0:
+            N.check(st["status"], self.h)
+        return self.split(state["x"]), st
 
     def split(self, x):
         c = (self.scene.n_range[1] + 1) ** 2 - 1
@@ -246,3 +304,58 @@ def universal_index(points, level):
     out = np.zeros(len(pts) // 3, np.int64)
     N.check(N.load().foggy_universal_index(len(out), N.ptr(pts), int(level), N.ptr(out, C.c_int64)))
     return out
+
+
+def continuation_stages(run, n_org, n_start=None, step_size=None, dynamic=False):
+    """The stage sequence of lib_mie_ms_calculate_scattering_coefficients_ab_nm
+    (FoggySim/src/lib/mie_theory/lib_mie_multi_sphere.f90:162-371) over run(n_max, max_iterations)
+    -> backward error (max_iterations None keeps the current setting):
+      no n_start            one solve at n_org;
+      n_start, no step      n_start with 100 iterations, then n_org with 1000;
+      n_start, step         n_start, n_start + step, ... up to n_org - step with 100 each, then
+                            n_org with 1000 (calc_with_steps, :238-266);
+      n_start, step, dynamic  calc_with_dynmaic_step_size (:268-369): solve at n_start, then
+                            repeatedly try the next degree with one iteration and accept the step
+                            when the backward error stays below 1e-3, else halve it.  As in the
+                            reference, an accepted trial (and every step of size 1) advances n_max
+                            by the step a second time before the full solve, and a rejected trial
+                            keeps the degree it tried."""
+    if n_start is None:
+        run(n_org, None)
+        return
+    if step_size is None:
+        run(n_start, 100)
+        run(n_org, 1000)
+        return
+    if not dynamic:
+        for n in range(n_start, n_org - step_size + 1, step_size):
+            run(n, 100)
+        run(n_org, 1000)
+        return
+    m_step = step_size
+    n = n_start
+    run(n, None)
+    state = "test"
+    for _ in range(100000):
+        if state == "test":
+            n = n_org if n + m_step >= n_org else n + m_step
+            if m_step > 1:
+                berr = run(n, 1)
+                if berr < 1e-3:
+                    n = n_org if n + m_step >= n_org else n + m_step
+                    state = "calculate"
+                else:
+                    state = "too_big" if m_step > 1 else "calculate"
+            else:
+                n = n_org if n + m_step >= n_org else n + m_step
+                state = "calculate"
+        elif state == "calculate":
+            run(n, 1000)
+            m_step = step_size
+            state = "finish" if n == n_org else "test"
+        elif state == "too_big":
+            m_step = int(m_step / 2.0) if int(m_step / 2.0) > 1 else 1
+            state = "test"
+        else:
+            return
+    raise RuntimeError("continuation did not finish")
