@@ -525,6 +525,172 @@ void scale_points(int n, const double* c, double* out, double* D_out, double* xm
 
 // ------------------------------------------------------------------------------------------
 // the multi-sphere problem (FoggySim/src/lib/mie_theory/lib_mie_type.f90:43-99)
+
+// ------------------------------------------------------------------------------------------
+// Gaussian beams in the plane-wave approximation (lib_mie_illumination.f90:781-918 case 3,
+// 1022-1050; lib_field_gaussian_beam.f90:111-891).  The localised-approximation branches of the
+// reference (cases 1 and 2) are commented out there and have no restatement.
+// ------------------------------------------------------------------------------------------
+// lib_math_get_matrix_rot, Euler x-convention (lib_math_type_operator.f90:1768-1810)
+void rot3(double phi, double theta, double psi, double R[9]) {
+    const double cph = std::cos(phi), sph = std::sin(phi), cth = std::cos(theta), sth = std::sin(theta);
+    const double cps = std::cos(psi), sps = std::sin(psi);
+    R[0] = cps * cph - cth * sph * sps;  R[1] = cps * sph + cth * cph * sps;  R[2] = sps * sth;
+    R[3] = -sps * cph - cth * sph * cps; R[4] = -sps * sph + cth * cph * cps; R[5] = cps * sth;
+    R[6] = sth * sph;                    R[7] = -sth * cph;                   R[8] = cth;
+}
+void mul3(const double R[9], const double v[3], double o[3]) {
+    const double a = v[0], b = v[1], c = v[2];
+    o[0] = R[0] * a + R[1] * b + R[2] * c;
+    o[1] = R[3] * a + R[4] * b + R[5] * c;
+    o[2] = R[6] * a + R[7] * b + R[8] * c;
+}
+// physicists' Hermite polynomial H_n (lib_math_hermite.f90:93-127): H_0 = 1, H_1 = 2x,
+// H_{k+1} = 2x H_k - 2k H_{k-1}
+double hermite(int n, double x) {
+    double h0 = 1.0, h1 = 2.0 * x;
+    if (n == 0) return h0;
+    for (int k = 1; k < n; ++k) {
+        const double h2 = 2.0 * x * h1 - 2.0 * k * h0;
+        h0 = h1;
+        h1 = h2;
+    }
+    return h1;
+}
+double factorial(int n) {
+    double f = 1.0;
+    for (int i = 2; i <= n; ++i) f *= i;
+    return f;
+}
+struct GBeam {
+    double e0, lambda0, n_medium, phase, wx0, wy0;
+    int tem_m, tem_n;
+    cd jx, jy;
+    double theta, phi;
+    int convention;
+    double g, d0[3];
+};
+// lib_field_gaussian_beam_rayleigh_length / _waist / _curvature (:817-891)
+double gb_zr(double w0, const GBeam& b) { return PI * w0 * w0 * b.n_medium / b.lambda0; }
+double gb_w(double w0, double zr, double z) { return w0 * std::sqrt(1.0 + (z / zr) * (z / zr)); }
+double gb_c(double zr, double z) { return z / (z * z + zr * zr); }
+bool gb_rotated(const GBeam& b) { return b.phi != 0.0 || b.theta != 0.0; }
+// world point relative to the beam origin -> beam frame (:127-133)
+void gb_to_beam(const GBeam& b, const double x[3], double o[3]) {
+    if (gb_rotated(b)) {
+        double R[9];
+        rot3(PI / 2.0 + b.phi, b.theta, PI / 2.0 + b.phi, R);
+        mul3(R, x, o);
+    } else {
+        o[0] = x[0]; o[1] = x[1]; o[2] = x[2];
+    }
+}
+// lib_fiel_gaussian_beam_hermite_scalar (:401-507) at a beam-frame point
+cd gb_scalar(const GBeam& b, const double x[3]) {
+    const double k = 2.0 * PI * b.n_medium / b.lambda0;
+    const double zrx = gb_zr(b.wx0, b), wx = gb_w(b.wx0, zrx, x[2]), crx = gb_c(zrx, x[2]);
+    const double zry = gb_zr(b.wy0, b), wy = gb_w(b.wy0, zry, x[2]), cry = gb_c(zry, x[2]);
+    const double hx = hermite(b.tem_m, x[0] * std::sqrt(2.0) / wx), hy = hermite(b.tem_n, x[1] * std::sqrt(2.0) / wy);
+    cd c = std::sqrt(b.wx0 / wx) * hx * std::exp(-x[0] * x[0] / (wx * wx)) *
+           std::exp(cd(0, -k * x[0] * x[0] * crx / 2.0));
+    c = std::sqrt(b.wy0 / wy) * hy * std::exp(-x[1] * x[1] / (wy * wy)) * std::exp(cd(0, -k * x[1] * x[1] * cry / 2.0)) * c;
+    const double amp = b.e0 * std::sqrt(1.0 / (std::pow(2.0, b.tem_m + b.tem_n) * factorial(b.tem_m) *
+                                               factorial(b.tem_n) * PI));
+    c = amp * std::exp(cd(0, -k * x[2] + b.phase)) * c;
+    c = std::exp(cd(0, (b.tem_m + 0.5) * std::atan2(x[2], zrx) + (b.tem_n + 0.5) * std::atan2(x[2], zry))) * c;
+    return b.convention == 2 ? std::conj(c) : c;
+}
+// get_derivative_xy (:573-595), get_derivative_z (:597-679)
+double gb_dxy(const GBeam& b, double w0, double xy, double z) {
+    if (xy == 0.0 || z == 0.0) return 0.0;
+    return -2.0 * PI * b.lambda0 * xy * z * b.n_medium /
+           ((PI * b.n_medium) * (PI * b.n_medium) * std::pow(w0, 4.0) + (b.lambda0 * z) * (b.lambda0 * z));
+}
+double gb_dz(const GBeam& b, double x, double y, double z) {
+    const double pn2 = (PI * b.n_medium) * (PI * b.n_medium), lz2 = (b.lambda0 * z) * (b.lambda0 * z);
+    const double wx2 = b.wx0 * b.wx0, wx4 = wx2 * wx2, wy2 = b.wy0 * b.wy0, wy4 = wy2 * wy2;
+    double rv = (2.0 * b.tem_m * wx2 + 2.0 * x * x) / (pn2 * wx4 + lz2);
+    rv += (2.0 * b.tem_n * wy2 + 2.0 * y * y) / (pn2 * wy4 + lz2);
+    rv += -4.0 * pn2 * x * x * wx4 / ((pn2 * wx4 + lz2) * (pn2 * wx4 + lz2));
+    rv += -4.0 * pn2 * y * y * wy4 / ((pn2 * wy4 + lz2) * (pn2 * wy4 + lz2));
+    rv = rv * b.lambda0 * b.lambda0 / 2.0 - 2.0;
+    return PI * b.n_medium * rv / b.lambda0;
+}
+// lib_field_gaussian_beam_hermite_get_propagation_direction (:191-225, :546-571), world frame
+void gb_direction(const GBeam& b, const double xw[3], double kv[3]) {
+    double x[3];
+    gb_to_beam(b, xw, x);
+    double k[3] = {-gb_dxy(b, b.wx0, x[0], x[2]), -gb_dxy(b, b.wy0, x[1], x[2]), -gb_dz(b, x[0], x[1], x[2])};
+    const double a = std::sqrt(k[0] * k[0] + k[1] * k[1] + k[2] * k[2]);
+    for (double& v : k) v /= a;
+    if (gb_rotated(b)) {
+        double R[9];
+        rot3(-PI / 2.0 - b.phi, -b.theta, -PI / 2.0 - b.phi, R);
+        mul3(R, k, kv);
+    } else {
+        kv[0] = k[0]; kv[1] = k[1]; kv[2] = k[2];
+    }
+}
+// get_absolute_value_and_argument (:681-799) at a beam-frame point
+void gb_abs_arg(const GBeam& b, const double x[3], double* absolute, double* argument) {
+    const double k = 2.0 * PI * b.n_medium / b.lambda0;
+    const double kz = std::fmod(k * x[2], 2.0 * PI);
+    const double zrx = gb_zr(b.wx0, b), zry = gb_zr(b.wy0, b);
+    const double wx = gb_w(b.wx0, zrx, x[2]), wy = gb_w(b.wy0, zry, x[2]);
+    const double crx = gb_c(zrx, x[2]), cry = gb_c(zry, x[2]);
+    double arg = -std::fmod(k * crx * x[0] * x[0] / 2.0, 2.0 * PI);
+    arg = arg - std::fmod(k * cry * x[1] * x[1] / 2.0, 2.0 * PI);
+    arg = arg - kz + b.phase;
+    arg = arg + (b.tem_m + 0.5) * std::atan2(x[2], zrx);
+    arg = arg + (b.tem_n + 0.5) * std::atan2(x[2], zry);
+    const double hx = hermite(b.tem_m, x[0] * std::sqrt(2.0) / wx), hy = hermite(b.tem_n, x[1] * std::sqrt(2.0) / wy);
+    if (hx * hy < 0.0) arg = arg - PI;
+    arg = std::fmod(arg, 2.0 * PI);
+    if (b.convention == 2) arg = -arg;
+    if (arg < 0.0) arg = 2.0 * PI + arg;
+    *argument = arg;
+    const double a = std::sqrt(b.wx0 / wx) * hx * std::exp(-(x[0] / wx) * (x[0] / wx)) * std::sqrt(b.wy0 / wy) * hy *
+                     std::exp(-(x[1] / wy) * (x[1] / wy)) * b.e0 *
+                     std::sqrt(1.0 / ((double)(1 << (b.tem_m + b.tem_n)) * factorial(b.tem_m) * factorial(b.tem_n) * PI));
+    *absolute = std::fabs(a);
+}
+// lib_field_gaussian_beam_hermite_get_plane_wave_approximation (:256-358): the plane wave that
+// stands in for the beam at world point xw (relative to the beam origin); its amplitude is
+// returned but, as in the reference, not used by the plane-wave coefficients
+Wave gb_plane_wave(const GBeam& b, const double xw[3], double* amplitude) {
+    double x[3], kv[3], rho, th, ph;
+    gb_to_beam(b, xw, x);
+    gb_direction(b, xw, kv);
+    to_spherical(kv, &rho, &th, &ph);
+    double absolute, argument;
+    gb_abs_arg(b, x, &absolute, &argument);
+    double phase = argument + std::fmod(2.0 * PI * x[2] / b.lambda0, 2.0 * PI);
+    phase = std::fmod(phase, 2.0 * PI);
+    if (phase < 0.0) phase = 2.0 * PI + phase;
+    double ax[3] = {1, 0, 0}, ay[3] = {0, 1, 0};
+    if (ph != 0.0 || th != 0.0) {
+        double R[9], t[3];
+        rot3(PI / 2.0 + b.phi, b.theta, PI / 2.0 + b.phi, R);
+        mul3(R, ax, t); ax[0] = t[0]; ax[1] = t[1]; ax[2] = t[2];
+        mul3(R, ay, t); ay[0] = t[0]; ay[1] = t[1]; ay[2] = t[2];
+    }
+    cd px = b.jx * std::fabs(ax[0]) + b.jy * std::fabs(ay[0]);
+    cd py = b.jy * std::fabs(ay[1]) + b.jx * std::fabs(ax[1]);
+    const double nrm = std::sqrt(std::norm(px) + std::norm(py));
+    px /= nrm;
+    py /= nrm;
+    Wave w;
+    w.theta = th;
+    w.phi = ph;
+    w.jre = px.real(); w.jim = px.imag();
+    w.yre = py.real(); w.yim = py.imag();
+    // case 3 scales by g twice: once as the plane wave's own g, once per beam (:864-877)
+    w.g = b.g * b.g;
+    w.phase = phase;
+    for (int d = 0; d < 3; ++d) w.d0[d] = b.d0[d];
+    if (amplitude) *amplitude = absolute;
+    return w;
+}
 // ------------------------------------------------------------------------------------------
 struct Problem {
     double lambda0, n_medium, k;
@@ -537,6 +703,7 @@ struct Problem {
     std::vector<int> nr;
     std::vector<std::vector<cd>> an, bn;   // per parameter, index n - nr1
     std::vector<Wave> waves;
+    std::vector<GBeam> beams;
     int cnt() const { return (n2 + 1) * (n2 + 1) - n1 * n1; }
     // cache of translation blocks per ordered pair (geometry only, bit-identical to recomputing)
     std::vector<std::vector<cd>> cacheA, cacheB;
@@ -555,8 +722,20 @@ void sphere_range(const Problem& P, int j, int* a, int* b) {
 void vector_b(const Problem& P, cd* b, cd* pq_out) {
     int C = P.cnt();
     std::vector<cd> p(C), q(C);
+    std::vector<cd> pb(C), qb(C);
     for (int j = 0; j < P.N; ++j) {
         pq_multi(P.waves, P.lambda0, P.n_medium, &P.centres[3 * j], P.n1, P.n2, p.data(), q.data());
+        // Gaussian beams: each sphere sees its own local plane wave (lib_mie_illumination.f90:232-247)
+        for (const GBeam& b : P.beams) {
+            const double xw[3] = {P.centres[3 * j] - b.d0[0], P.centres[3 * j + 1] - b.d0[1],
+                                  P.centres[3 * j + 2] - b.d0[2]};
+            std::vector<Wave> one{gb_plane_wave(b, xw, nullptr)};
+            pq_multi(one, P.lambda0, P.n_medium, &P.centres[3 * j], P.n1, P.n2, pb.data(), qb.data());
+            for (int i = 0; i < C; ++i) {
+                p[i] += pb[i];
+                q[i] += qb[i];
+            }
+        }
         int ip = P.pidx[j];
         int a0 = P.nr[2 * ip];
         int ja, jb;
@@ -1470,6 +1649,61 @@ int orc_field(void* p, const double* x, int npts, const double* pts, double e0, 
     for (int i = 0; i < npts; ++i)
         field_at(*P, reinterpret_cast<const cd*>(x), pts + 3 * (size_t)i, e0,
                  reinterpret_cast<cd*>(E) + 3 * (size_t)i, reinterpret_cast<cd*>(H) + 3 * (size_t)i);
+    return 0;
+}
+
+// Gaussian beams of a problem (replace any set before); per beam: waist x0, y0, TEM m, n, theta,
+// phi, Jones (re x, im x, re y, im y), g, phase, origin, convention; e_field_0 = 1 and the
+// problem's wavelength and medium
+int orc_set_gaussian_beams(void* p, int nb, const double* waist, const int* tem, const double* theta,
+                           const double* phi, const double* jones, const double* g, const double* phase,
+                           const double* d0, const int* convention) {
+    Problem* P = static_cast<Problem*>(p);
+    P->beams.clear();
+    for (int i = 0; i < nb; ++i) {
+        GBeam b;
+        b.e0 = 1.0;
+        b.lambda0 = P->lambda0;
+        b.n_medium = P->n_medium;
+        b.phase = phase ? phase[i] : 0.0;
+        b.wx0 = waist[2 * i];
+        b.wy0 = waist[2 * i + 1];
+        b.tem_m = tem[2 * i];
+        b.tem_n = tem[2 * i + 1];
+        b.jx = cd(jones[4 * i], jones[4 * i + 1]);
+        b.jy = cd(jones[4 * i + 2], jones[4 * i + 3]);
+        b.theta = theta[i];
+        b.phi = phi[i];
+        b.convention = convention ? convention[i] : 1;
+        b.g = g[i];
+        for (int d = 0; d < 3; ++d) b.d0[d] = d0 ? d0[3 * i + d] : 0.0;
+        P->beams.push_back(b);
+    }
+    return 0;
+}
+
+// one beam's scalar field, |E| and arg E at beam-frame points, and its local plane wave at world
+// points (theta, phi, Jones x re/im, y re/im, phase, amplitude per point)
+int orc_gaussian_probe(double lambda0, double n_medium, double wx0, double wy0, int tem_m, int tem_n,
+                       const double* jones, double theta, double phi, double phase, int convention, int npts,
+                       const double* pts, double* scalar, double* absarg, double* wave) {
+    GBeam b;
+    b.e0 = 1.0; b.lambda0 = lambda0; b.n_medium = n_medium; b.phase = phase; b.wx0 = wx0; b.wy0 = wy0;
+    b.tem_m = tem_m; b.tem_n = tem_n; b.jx = cd(jones[0], jones[1]); b.jy = cd(jones[2], jones[3]);
+    b.theta = theta; b.phi = phi; b.convention = convention; b.g = 1.0;
+    b.d0[0] = b.d0[1] = b.d0[2] = 0.0;
+    for (int i = 0; i < npts; ++i) {
+        const double* x = pts + 3 * i;
+        cd f = gb_scalar(b, x);
+        scalar[2 * i] = f.real();
+        scalar[2 * i + 1] = f.imag();
+        gb_abs_arg(b, x, absarg + 2 * i, absarg + 2 * i + 1);
+        double amp = 0.0;
+        Wave w = gb_plane_wave(b, x, &amp);
+        double* o = wave + 8 * i;
+        o[0] = w.theta; o[1] = w.phi; o[2] = w.jre; o[3] = w.jim; o[4] = w.yre; o[5] = w.yim; o[6] = w.phase;
+        o[7] = amp;
+    }
     return 0;
 }
 

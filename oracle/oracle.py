@@ -317,3 +317,41 @@ def _field(self, x, points, e0=1.0):
 
 
 Problem.field = _field
+
+
+def _set_gaussian_beams(self, waist, tem, theta, phi, jones, g, phase=None, d0=None, convention=None):
+    """Gaussian beams of the problem (plane-wave approximation, the reference's calculation_type 3)."""
+    L = lib()
+    nb = len(theta)
+    arr = lambda a, t=np.float64: np.ascontiguousarray(a, t).reshape(-1)
+    w, tm, th, ph, jo, gg = arr(waist), arr(tem, np.int32), arr(theta), arr(phi), arr(jones), arr(g)
+    pa = arr(phase) if phase is not None else np.zeros(nb)
+    dd = arr(d0) if d0 is not None else np.zeros(3 * nb)
+    cv = arr(convention, np.int32) if convention is not None else np.ones(nb, np.int32)
+    self._beams = (w, tm, th, ph, jo, gg, pa, dd, cv)
+    L.orc_set_gaussian_beams(C.c_void_p(self.h), int(nb), w.ctypes.data_as(C.c_void_p),
+                             tm.ctypes.data_as(C.c_void_p), th.ctypes.data_as(C.c_void_p),
+                             ph.ctypes.data_as(C.c_void_p), jo.ctypes.data_as(C.c_void_p),
+                             gg.ctypes.data_as(C.c_void_p), pa.ctypes.data_as(C.c_void_p),
+                             dd.ctypes.data_as(C.c_void_p), cv.ctypes.data_as(C.c_void_p))
+
+
+Problem.set_gaussian_beams = _set_gaussian_beams
+
+
+def gaussian_probe(lambda0, n_medium, waist, tem, jones, theta, phi, phase, convention, points):
+    """One Gaussian beam at points (beam origin at 0): scalar field (beam frame), (|E|, arg E) and
+    the local plane wave (theta, phi, Jones x re/im, y re/im, phase, amplitude) per point."""
+    L = lib()
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1)
+    n = len(pts) // 3
+    sc = np.zeros(2 * n)
+    aa = np.zeros(2 * n)
+    wv = np.zeros(8 * n)
+    jo = np.ascontiguousarray(jones, np.float64)
+    L.orc_gaussian_probe(C.c_double(lambda0), C.c_double(n_medium), C.c_double(waist[0]), C.c_double(waist[1]),
+                         C.c_int(tem[0]), C.c_int(tem[1]), jo.ctypes.data_as(C.c_void_p), C.c_double(theta),
+                         C.c_double(phi), C.c_double(phase), C.c_int(convention), C.c_int(n),
+                         pts.ctypes.data_as(C.c_void_p), sc.ctypes.data_as(C.c_void_p),
+                         aa.ctypes.data_as(C.c_void_p), wv.ctypes.data_as(C.c_void_p))
+    return sc.view(np.complex128), aa.reshape(n, 2), wv.reshape(n, 8)
