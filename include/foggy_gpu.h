@@ -152,6 +152,21 @@ int32_t foggy_set_plane_waves(foggy_handle h, int32_t nw, const double* theta, c
                               const double* jones, const double* g, const double* phase,
                               const double* d_0_i);
 
+/* Gaussian beams illuminating the cluster, added to the plane waves (lib_mie_illumination_get_p_q_j_j,
+ * lib_mie_illumination.f90:206-250); nb = 0 removes them.  The reference's working beam model,
+ * the plane-wave approximation (calculation_type 3, lib_mie_illumination_get_p_q_gaussian_beam,
+ * lib_mie_illumination.f90:781-918, with lib_field_gaussian_beam_hermite_get_plane_wave_approximation,
+ * FoggySim/src/lib/field/lib_field_gaussian_beam.f90:256-358): each sphere sees the plane wave
+ * along the beam's local phase gradient, with its local phase and projected polarisation.  Per
+ * beam: waist radii x0, y0 (waist[2 nb]), Hermite-Gaussian mode m, n (tem[2 nb], 0..30), axis
+ * direction theta, phi, Jones vector (jones[4 nb]: re x, im x, re y, im y), weight g (applied
+ * twice, as the reference does), phase (NULL = 0), origin d_0_i[3 nb] (NULL = 0) and time
+ * convention (convention[nb], 1 or 2; NULL = 1).  The beams use the handle's lambda_0 and
+ * n_medium.  Setting plane waves with nw = 0 leaves only the beams. */
+int32_t foggy_set_gaussian_beams(foggy_handle h, int32_t nb, const double* waist, const int32_t* tem,
+                                 const double* theta, const double* phi, const double* jones, const double* g,
+                                 const double* phase, const double* d_0_i, const int32_t* convention);
+
 /* Number of complex entries of one coefficient vector in the reference layout. */
 int64_t foggy_vector_length(foggy_handle h);
 

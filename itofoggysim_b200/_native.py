@@ -35,7 +35,7 @@ EXPORTS = [
     "foggy_get_vector_b", "foggy_matvec", "foggy_solve", "foggy_get_backward_error",
     "foggy_cross_sections", "foggy_translation_coefficients", "foggy_wigner_3j", "foggy_build_tree",
     "foggy_universal_index", "foggy_tree_boxes", "foggy_matvec_static", "foggy_tree_domain",
-    "foggy_get_field",
+    "foggy_get_field", "foggy_set_gaussian_beams",
 ]
 
 
@@ -124,6 +124,7 @@ def load():
         "foggy_matvec_static": (i32, [vp, vp, vp]),
         "foggy_tree_domain": (i32, [vp, i32, i64, i32, pi64, pi32]),
         "foggy_get_field": (i32, [vp, vp, i32, i32, vp, dbl, vp, vp]),
+        "foggy_set_gaussian_beams": (i32, [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

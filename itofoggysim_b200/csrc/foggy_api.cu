@@ -82,6 +82,7 @@ struct foggy_handle_s {
     int nbuckets = 0, cmax = 1;
     // waves and right-hand side
     std::vector<WaveDev> waves;
+    std::vector<GaussDev> beams;
     bool rhs_ready = false;
     cplx* d_b = nullptr;
     cplx* d_pq = nullptr;
@@ -656,24 +657,40 @@ int apply_operator(foggy_handle h, const cplx* x, cplx* y) {
 int ensure_rhs(foggy_handle h) {
     if (h->rhs_ready) return FOGGY_OK;
     if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
-    if (h->waves.empty()) return fail(h, FOGGY_ERR_STATE, "no plane waves set");
-    int nw = (int)h->waves.size();
-    WaveDev* d_w = nullptr;
-    double *d_pi = nullptr, *d_tau = nullptr;
-    size_t S = (size_t)(h->pmax + 1) * (h->pmax + 1);
-    CK(h, cudaMalloc(&d_w, nw * sizeof(WaveDev)));
-    CK(h, cudaMalloc(&d_pi, nw * S * sizeof(double)));
-    CK(h, cudaMalloc(&d_tau, nw * S * sizeof(double)));
-    CK(h, cudaMemcpyAsync(d_w, h->waves.data(), nw * sizeof(WaveDev), cudaMemcpyHostToDevice, h->stream));
-    k_pitau<<<nw, h->pmax + 1, 0, h->stream>>>(nw, d_w, h->pmax, d_pi, d_tau);
-    k_rhs<<<h->N, 128, 0, h->stream>>>(scene_view(h), nw, d_w, h->pmax, d_pi, d_tau, h->d_b, h->d_pq);
-    h->launches += 2;
-    cudaError_t e = cudaStreamSynchronize(h->stream);
-    cudaFree(d_w);
-    cudaFree(d_pi);
-    cudaFree(d_tau);
+    if (h->waves.empty() && h->beams.empty()) return fail(h, FOGGY_ERR_STATE, "no plane waves or beams set");
+    const int nw = (int)h->waves.size(), nb = (int)h->beams.size();
+    const size_t nl = (size_t)h->N * nb;   // local plane waves of the beams, per sphere
+    const size_t S = (size_t)(h->pmax + 1) * (h->pmax + 1);
+    // one allocation: waves, local waves, beams, then the pi / tau tables of both
+    const size_t nwav = (size_t)nw + nl;
+    const size_t bytes = nwav * sizeof(WaveDev) + (size_t)nb * sizeof(GaussDev) + 2 * nwav * S * sizeof(double);
+    void* buf = nullptr;
+    CK(h, cudaMalloc(&buf, bytes));
+    WaveDev* d_w = static_cast<WaveDev*>(buf);
+    WaveDev* d_l = d_w + nw;
+    GaussDev* d_g = reinterpret_cast<GaussDev*>(d_l + nl);
+    double* d_pi = reinterpret_cast<double*>(d_g + nb);
+    double* d_tau = d_pi + nwav * S;
+    cudaError_t e = cudaSuccess;
+    if (nw) e = cudaMemcpyAsync(d_w, h->waves.data(), nw * sizeof(WaveDev), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && nb)
+        e = cudaMemcpyAsync(d_g, h->beams.data(), nb * sizeof(GaussDev), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && nb) {
+        k_gauss_local<<<(unsigned)((nl + 127) / 128), 128, 0, h->stream>>>(scene_view(h), nb, d_g, h->prm.lambda_0,
+                                                                           h->prm.n_medium, d_l);
+        h->launches += 1;
+    }
+    if (e == cudaSuccess) {
+        // pi / tau of the shared waves and of the local waves are one table set
+        k_pitau<<<(unsigned)nwav, h->pmax + 1, 0, h->stream>>>((int)nwav, d_w, h->pmax, d_pi, d_tau);
+        k_rhs<<<h->N, 128, 0, h->stream>>>(scene_view(h), nw, d_w, h->pmax, d_pi, d_tau, nb, d_l, d_pi + nw * S,
+                                           d_tau + nw * S, h->d_b, h->d_pq);
+        h->launches += 2;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(buf);
     if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("rhs: ") + cudaGetErrorString(e));
-    CKL(h);
     h->rhs_ready = true;
     return FOGGY_OK;
 }
@@ -1090,7 +1107,8 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
 int32_t foggy_set_plane_waves(foggy_handle h, int32_t nw, const double* theta, const double* phi,
                               const double* jones, const double* g, const double* phase, const double* d_0_i) {
     if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
-    if (nw < 1 || !theta || !phi || !jones || !g) return fail(h, FOGGY_ERR_ARGUMENT, "empty or NULL wave input");
+    if (nw < 0 || (nw > 0 && (!theta || !phi || !jones || !g)))
+        return fail(h, FOGGY_ERR_ARGUMENT, "negative count or NULL wave input");
     h->waves.clear();
     double k = wavenumber(h->prm);
     for (int i = 0; i < nw; ++i) {
@@ -1112,6 +1130,41 @@ int32_t foggy_set_plane_waves(foggy_handle h, int32_t nw, const double* theta, c
         for (int d = 0; d < 3; ++d) w.d0[d] = d_0_i ? d_0_i[3 * i + d] : 0.0;
         h->waves.push_back(w);
     }
+    h->rhs_ready = false;
+    return FOGGY_OK;
+}
+
+int32_t foggy_set_gaussian_beams(foggy_handle h, int32_t nb, const double* waist, const int32_t* tem,
+                                 const double* theta, const double* phi, const double* jones, const double* g,
+                                 const double* phase, const double* d_0_i, const int32_t* convention) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (nb < 0 || (nb > 0 && (!waist || !tem || !theta || !phi || !jones || !g)))
+        return fail(h, FOGGY_ERR_ARGUMENT, "negative count or NULL beam input");
+    std::vector<GaussDev> v;
+    for (int i = 0; i < nb; ++i) {
+        GaussDev b{};
+        b.wx0 = waist[2 * i];
+        b.wy0 = waist[2 * i + 1];
+        b.tem_m = tem[2 * i];
+        b.tem_n = tem[2 * i + 1];
+        if (!(b.wx0 > 0.0) || !(b.wy0 > 0.0) || b.tem_m < 0 || b.tem_n < 0 || b.tem_m > 30 || b.tem_n > 30)
+            return fail(h, FOGGY_ERR_ARGUMENT, "beam waist must be > 0 and TEM orders in 0..30");
+        b.jxr = jones[4 * i];
+        b.jxi = jones[4 * i + 1];
+        b.jyr = jones[4 * i + 2];
+        b.jyi = jones[4 * i + 3];
+        if (b.jxr == 0.0 && b.jxi == 0.0 && b.jyr == 0.0 && b.jyi == 0.0)
+            return fail(h, FOGGY_ERR_ARGUMENT, "beam Jones vector is zero");
+        b.theta = theta[i];
+        b.phi = phi[i];
+        b.phase = phase ? phase[i] : 0.0;
+        b.g = g[i];
+        for (int d = 0; d < 3; ++d) b.d0[d] = d_0_i ? d_0_i[3 * i + d] : 0.0;
+        b.convention = convention ? convention[i] : 1;
+        if (b.convention != 1 && b.convention != 2) return fail(h, FOGGY_ERR_ARGUMENT, "beam convention must be 1 or 2");
+        v.push_back(b);
+    }
+    h->beams = v;
     h->rhs_ready = false;
     return FOGGY_OK;
 }

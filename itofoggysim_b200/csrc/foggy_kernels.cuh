@@ -18,6 +18,20 @@ struct WaveDev {
     double d0[3];        // origin of the wave's coordinate system
 };
 
+// Hermite-Gaussian beam (lib_field_gaussian_beam_hermite_type, lib_field_gaussian_beam.f90:40-56,
+// inside lib_mie_illumination_gaussian_beam_parameter, lib_mie_illumination.f90:58-93); its
+// wavelength and medium are the solver's, e_field_0 = 1
+struct GaussDev {
+    double wx0, wy0;             // waist radii along x and y
+    int tem_m, tem_n;            // Hermite-Gaussian mode
+    double jxr, jxi, jyr, jyi;   // Jones vector
+    double theta, phi;           // propagation direction of the beam axis
+    double phase;                // extra phase
+    double g;                    // amplitude weight
+    double d0[3];                // origin of the beam coordinate system
+    int convention;              // 1: exp(-i(kz - wt)), 2: exp(i(kz - wt))
+};
+
 // k_scene.cu
 __global__ void k_mie_ab(int n_param, const double* size_param, const double* m_re, const double* m_im,
                          const int* p_of_param, int pstride, cplx* an_out, cplx* bn_out);
@@ -25,7 +39,10 @@ __global__ void k_gather_an(int n, const int* pidx, int pstride, const cplx* an_
                             cplx* an_s, cplx* bn_s);
 __global__ void k_pitau(int nw, const WaveDev* waves, int pmax, double* pi_out, double* tau_out);
 __global__ void k_rhs(SceneView sc, int nw, const WaveDev* waves, int pmax, const double* pi_tab,
-                      const double* tau_tab, cplx* b, cplx* pq);
+                      const double* tau_tab, int nl, const WaveDev* lwaves, const double* lpi_tab,
+                      const double* ltau_tab, cplx* b, cplx* pq);
+__global__ void k_gauss_local(SceneView sc, int nb, const GaussDev* beams, double lambda0, double n_medium,
+                              WaveDev* out);
 __global__ void k_unpack(SceneView sc, int pg, const double* g, const cplx* xref, cplx* xdev);
 __global__ void k_pack(SceneView sc, int pg, const double* g, const cplx* ydev, const cplx* identity_ref,
                        cplx* yref);

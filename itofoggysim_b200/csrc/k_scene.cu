@@ -141,8 +141,41 @@ __global__ void k_pitau(int nw, const WaveDev* waves, int pmax, double* pi_out, 
 // plane-wave coefficients of lib_mie_illumination.f90:392-478 (several waves, Jones vector,
 // TE swaps p and q) and :636-763 (p = tau e^{-i m beta}/(n(n+1)) e^{i(k.d + phase)}).
 // One block per sphere; pq keeps the incident coefficients for the cross-sections. --------
+namespace {
+// p, q of one plane wave W at degree n, order m of a sphere centred at cj (pi_s, tau_s its scaled
+// Legendre values there), times W.g, added to pv, qv
+__device__ __forceinline__ void add_wave(const WaveDev& W, const double* cj, int m, double rn, double pi_s,
+                                         double tau_s, cplx& pv, cplx& qv) {
+    double d0 = cj[0] - W.d0[0], d1 = cj[1] - W.d0[1], d2 = cj[2] - W.d0[2];
+    double dn = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    double kd = W.kc[0] * d0 + W.kc[1] * d1 + W.kc[2] * d2;
+    if (W.alpha == 0.0 && m != 1 && m != -1) { pi_s = 0.0; tau_s = 0.0; }
+    double sb, cbv;
+    sincos(-m * W.beta, &sb, &cbv);
+    cplx base = mk(rn * cbv, rn * sb);
+    cplx tp = mk(0, 0), tq = mk(0, 0);
+    if (W.ax > 0) {
+        cplx e = mk(1, 0);
+        if (dn > 0.0 || W.phx != 0.0) { double ss, cc; sincos(kd + W.phx, &ss, &cc); e = mk(cc, ss); }
+        tp = tp + W.ax * (e * (tau_s * base));
+        tq = tq + W.ax * (e * (pi_s * base));
+    }
+    if (W.ay > 0) {
+        cplx e = mk(1, 0);
+        if (dn > 0.0 || W.phy != 0.0) { double ss, cc; sincos(kd + W.phy, &ss, &cc); e = mk(cc, ss); }
+        tp = tp + W.ay * (e * (pi_s * base));    // TE: p and q swap
+        tq = tq + W.ay * (e * (tau_s * base));
+    }
+    pv = pv + W.g * tp;
+    qv = qv + W.g * tq;
+}
+}  // namespace
+
+// nw waves shared by all spheres (tables [w][S]) and nl local waves per sphere (waves[j nl + l],
+// tables [(j nl + l)][S]), the plane waves that stand in for Gaussian beams at each sphere
 __global__ void k_rhs(SceneView sc, int nw, const WaveDev* waves, int pmax, const double* pi_tab,
-                      const double* tau_tab, cplx* b, cplx* pq) {
+                      const double* tau_tab, int nl, const WaveDev* lwaves, const double* lpi_tab,
+                      const double* ltau_tab, cplx* b, cplx* pq) {
     int j = blockIdx.x;
     int pj = sc.p[j];
     int Pj = pj * (pj + 2);
@@ -156,38 +189,133 @@ __global__ void k_rhs(SceneView sc, int nw, const WaveDev* waves, int pmax, cons
         int m = t + 1 - n * n - n;
         cplx pv = mk(0, 0), qv = mk(0, 0);
         double rn = 1.0 / (double)(n * (n + 1));
-        for (int w = 0; w < nw; ++w) {
-            const WaveDev& W = waves[w];
-            double d0 = cj[0] - W.d0[0], d1 = cj[1] - W.d0[1], d2 = cj[2] - W.d0[2];
-            double dn = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-            double kd = W.kc[0] * d0 + W.kc[1] * d1 + W.kc[2] * d2;
-            double pi_s = pi_tab[(size_t)w * S + n * (n + 1) + m];
-            double tau_s = tau_tab[(size_t)w * S + n * (n + 1) + m];
-            if (W.alpha == 0.0 && m != 1 && m != -1) { pi_s = 0.0; tau_s = 0.0; }
-            double sb, cbv;
-            sincos(-m * W.beta, &sb, &cbv);
-            cplx base = mk(rn * cbv, rn * sb);
-            cplx tp = mk(0, 0), tq = mk(0, 0);
-            if (W.ax > 0) {
-                cplx e = mk(1, 0);
-                if (dn > 0.0 || W.phx != 0.0) { double ss, cc; sincos(kd + W.phx, &ss, &cc); e = mk(cc, ss); }
-                tp = tp + W.ax * (e * (tau_s * base));
-                tq = tq + W.ax * (e * (pi_s * base));
-            }
-            if (W.ay > 0) {
-                cplx e = mk(1, 0);
-                if (dn > 0.0 || W.phy != 0.0) { double ss, cc; sincos(kd + W.phy, &ss, &cc); e = mk(cc, ss); }
-                tp = tp + W.ay * (e * (pi_s * base));    // TE: p and q swap
-                tq = tq + W.ay * (e * (tau_s * base));
-            }
-            pv = pv + W.g * tp;
-            qv = qv + W.g * tq;
+        const int e = n * (n + 1) + m;
+        for (int w = 0; w < nw; ++w)
+            add_wave(waves[w], cj, m, rn, pi_tab[(size_t)w * S + e], tau_tab[(size_t)w * S + e], pv, qv);
+        for (int l = 0; l < nl; ++l) {
+            const size_t wl = (size_t)j * nl + l;
+            add_wave(lwaves[wl], cj, m, rn, lpi_tab[wl * S + e], ltau_tab[wl * S + e], pv, qv);
         }
         pq[o + t] = pv;
         pq[o + Pj + t] = qv;
         b[o + t] = sc.an[(size_t)j * sc.pmax + n - 1] * pv;
         b[o + Pj + t] = sc.bn[(size_t)j * sc.pmax + n - 1] * qv;
     }
+}
+
+// ---- Gaussian beams in the plane-wave approximation (lib_mie_illumination.f90:781-918,
+// calculation_type 3, and 1022-1050; beam functions of
+// FoggySim/src/lib/field/lib_field_gaussian_beam.f90:111-891).  At each sphere the beam is replaced
+// by the plane wave with the direction of its phase gradient, its phase (shifted back to the
+// beam origin by 2 pi z / lambda_0) and its polarisation projected on the rotated beam axes; the
+// local amplitude does not enter the coefficients (lib_mie_illumination.f90:392-478 uses only
+// g, the Jones vector and the phase), and the beam's g scales them twice (:864-877). --------
+namespace {
+// Euler rotation, x-convention (lib_math_get_matrix_rot, lib_math_type_operator.f90:1768-1810), applied to v
+__device__ void euler_apply(double phi, double theta, double psi, const double v[3], double o[3]) {
+    double sph, cph, sth, cth, sps, cps;
+    sincos(phi, &sph, &cph);
+    sincos(theta, &sth, &cth);
+    sincos(psi, &sps, &cps);
+    const double a = v[0], b = v[1], c = v[2];
+    o[0] = (cps * cph - cth * sph * sps) * a + (cps * sph + cth * cph * sps) * b + (sps * sth) * c;
+    o[1] = (-sps * cph - cth * sph * cps) * a + (-sps * sph + cth * cph * cps) * b + (cps * sth) * c;
+    o[2] = (sth * sph) * a + (-sth * cph) * b + cth * c;
+}
+// physicists' Hermite polynomial by its three-term recurrence
+__device__ double hermite_h(int n, double x) {
+    double h0 = 1.0, h1 = 2.0 * x;
+    if (n == 0) return h0;
+    for (int k = 1; k < n; ++k) {
+        const double h2 = 2.0 * x * h1 - 2.0 * k * h0;
+        h0 = h1;
+        h1 = h2;
+    }
+    return h1;
+}
+}  // namespace
+
+__global__ void k_gauss_local(SceneView sc, int nb, const GaussDev* beams, double lambda0, double n_medium,
+                              WaveDev* out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= sc.n * nb) return;
+    const int j = t / nb;
+    const GaussDev B = beams[t - j * nb];
+    const double PI_ = 3.14159265358979323846;
+    const double xw[3] = {sc.centres[3 * (size_t)j] - B.d0[0], sc.centres[3 * (size_t)j + 1] - B.d0[1],
+                          sc.centres[3 * (size_t)j + 2] - B.d0[2]};
+    const bool rot = B.phi != 0.0 || B.theta != 0.0;
+    double x[3] = {xw[0], xw[1], xw[2]};
+    if (rot) euler_apply(PI_ / 2.0 + B.phi, B.theta, PI_ / 2.0 + B.phi, xw, x);
+    // propagation direction: minus the phase gradient in the beam frame, normalised, rotated back
+    // (get_derivative_xy / get_derivative_z, lib_field_gaussian_beam.f90:573-679)
+    const double pn2 = (PI_ * n_medium) * (PI_ * n_medium), lz2 = (lambda0 * x[2]) * (lambda0 * x[2]);
+    const double wx2 = B.wx0 * B.wx0, wx4 = wx2 * wx2, wy2 = B.wy0 * B.wy0, wy4 = wy2 * wy2;
+    auto dxy = [&](double w4, double xy) {
+        return (xy == 0.0 || x[2] == 0.0) ? 0.0 : -2.0 * PI_ * lambda0 * xy * x[2] * n_medium / (pn2 * w4 + lz2);
+    };
+    double dz = (2.0 * B.tem_m * wx2 + 2.0 * x[0] * x[0]) / (pn2 * wx4 + lz2);
+    dz += (2.0 * B.tem_n * wy2 + 2.0 * x[1] * x[1]) / (pn2 * wy4 + lz2);
+    dz += -4.0 * pn2 * x[0] * x[0] * wx4 / ((pn2 * wx4 + lz2) * (pn2 * wx4 + lz2));
+    dz += -4.0 * pn2 * x[1] * x[1] * wy4 / ((pn2 * wy4 + lz2) * (pn2 * wy4 + lz2));
+    dz = PI_ * n_medium * (dz * lambda0 * lambda0 / 2.0 - 2.0) / lambda0;
+    double kb[3] = {-dxy(wx4, x[0]), -dxy(wy4, x[1]), -dz};
+    const double kn = sqrt(kb[0] * kb[0] + kb[1] * kb[1] + kb[2] * kb[2]);
+    kb[0] /= kn;
+    kb[1] /= kn;
+    kb[2] /= kn;
+    double kv[3] = {kb[0], kb[1], kb[2]};
+    if (rot) euler_apply(-PI_ / 2.0 - B.phi, -B.theta, -PI_ / 2.0 - B.phi, kb, kv);
+    const double kr = sqrt(kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2]);
+    const double th = (kr == 0.0) ? 0.0 : acos(kv[2] / kr);
+    const double ph = (kv[0] == 0.0 && kv[1] == 0.0) ? 0.0 : atan2(kv[1], kv[0]);
+    // argument of the beam at the point (get_absolute_value_and_argument, :681-799)
+    const double k = 2.0 * PI_ * n_medium / lambda0, two_pi = 2.0 * PI_;
+    const double zrx = PI_ * wx2 * n_medium / lambda0, zry = PI_ * wy2 * n_medium / lambda0;
+    const double wx = B.wx0 * sqrt(1.0 + (x[2] / zrx) * (x[2] / zrx)), wy = B.wy0 * sqrt(1.0 + (x[2] / zry) * (x[2] / zry));
+    const double crx = x[2] / (x[2] * x[2] + zrx * zrx), cry = x[2] / (x[2] * x[2] + zry * zry);
+    double arg = -fmod(k * crx * x[0] * x[0] / 2.0, two_pi);
+    arg = arg - fmod(k * cry * x[1] * x[1] / 2.0, two_pi);
+    arg = arg - fmod(k * x[2], two_pi) + B.phase;
+    arg = arg + (B.tem_m + 0.5) * atan2(x[2], zrx);
+    arg = arg + (B.tem_n + 0.5) * atan2(x[2], zry);
+    const double hx = hermite_h(B.tem_m, x[0] * sqrt(2.0) / wx), hy = hermite_h(B.tem_n, x[1] * sqrt(2.0) / wy);
+    if (hx * hy < 0.0) arg = arg - PI_;
+    arg = fmod(arg, two_pi);
+    if (B.convention == 2) arg = -arg;
+    if (arg < 0.0) arg = two_pi + arg;
+    double phase = fmod(arg + fmod(two_pi * x[2] / lambda0, two_pi), two_pi);
+    if (phase < 0.0) phase = two_pi + phase;
+    // polarisation on the rotated beam axes (:329-352)
+    double ax[3] = {1.0, 0.0, 0.0}, ay[3] = {0.0, 1.0, 0.0};
+    if (ph != 0.0 || th != 0.0) {
+        const double ex[3] = {1.0, 0.0, 0.0}, ey[3] = {0.0, 1.0, 0.0};
+        euler_apply(PI_ / 2.0 + B.phi, B.theta, PI_ / 2.0 + B.phi, ex, ax);
+        euler_apply(PI_ / 2.0 + B.phi, B.theta, PI_ / 2.0 + B.phi, ey, ay);
+    }
+    const double pxr = B.jxr * fabs(ax[0]) + B.jyr * fabs(ay[0]), pxi = B.jxi * fabs(ax[0]) + B.jyi * fabs(ay[0]);
+    const double pyr = B.jyr * fabs(ay[1]) + B.jxr * fabs(ax[1]), pyi = B.jyi * fabs(ay[1]) + B.jxi * fabs(ax[1]);
+    const double nrm = sqrt(pxr * pxr + pxi * pxi + pyr * pyr + pyi * pyi);
+    // the plane wave as the right-hand side takes it (direction through its cartesian round trip)
+    WaveDev W;
+    double st_, ct_, sp_, cp_;
+    sincos(th, &st_, &ct_);
+    sincos(ph, &sp_, &cp_);
+    W.kc[0] = k * st_ * cp_;
+    W.kc[1] = k * st_ * sp_;
+    W.kc[2] = k * ct_;
+    const double r2 = sqrt(W.kc[0] * W.kc[0] + W.kc[1] * W.kc[1] + W.kc[2] * W.kc[2]);
+    W.alpha = (r2 == 0.0) ? 0.0 : acos(W.kc[2] / r2);
+    W.beta = (W.kc[0] == 0.0 && W.kc[1] == 0.0) ? 0.0 : atan2(W.kc[1], W.kc[0]);
+    W.ax = hypot(pxr / nrm, pxi / nrm);
+    W.phx = atan2(pxi / nrm, pxr / nrm) + phase;
+    W.ay = hypot(pyr / nrm, pyi / nrm);
+    W.phy = atan2(pyi / nrm, pyr / nrm) + phase;
+    W.g = B.g * B.g;
+    W.d0[0] = B.d0[0];
+    W.d0[1] = B.d0[1];
+    W.d0[2] = B.d0[2];
+    out[t] = W;
 }
 
 // ---- layout conversion ---------------------------------------------------------------------

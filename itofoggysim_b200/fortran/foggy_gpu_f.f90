@@ -201,6 +201,17 @@ module foggy_gpu_f
             real(c_double), value :: e_field_0
             integer(c_int32_t) :: rc
         end function
+        function foggy_set_gaussian_beams(h, nb, waist, tem, theta, phi, jones, g, phase, d_0_i, convention) &
+                result(rc) bind(c, name="foggy_set_gaussian_beams")
+            import :: c_ptr, c_int32_t, c_double, c_double_complex
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: nb
+            real(c_double), intent(in) :: waist(2, *), theta(*), phi(*), g(*)
+            integer(c_int32_t), intent(in) :: tem(2, *)
+            complex(c_double_complex), intent(in) :: jones(2, *)
+            type(c_ptr), value :: phase, d_0_i, convention   ! c_loc(...) or c_null_ptr for defaults
+            integer(c_int32_t) :: rc
+        end function
         function foggy_matvec_static(h, x, y) result(rc) bind(c, name="foggy_matvec_static")
             import :: c_ptr, c_int32_t
             type(c_ptr), value :: h, x, y       ! device pointers
@@ -213,7 +224,7 @@ module foggy_gpu_f
     public :: foggy_get_backward_error, foggy_cross_sections, foggy_translation_coefficients
     public :: foggy_wigner_3j, foggy_last_error, foggy_set_params, foggy_get_mie_coefficients
     public :: foggy_get_vector_b, foggy_build_tree, foggy_universal_index, foggy_tree_boxes
-    public :: foggy_tree_domain, foggy_get_field, foggy_matvec_static
+    public :: foggy_tree_domain, foggy_get_field, foggy_matvec_static, foggy_set_gaussian_beams
     public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
     public :: foggy_ms_get_backward_error, foggy_ms_destructor
 

@@ -171,6 +171,28 @@ class MultiSphereSolver:
         self._set()
         self.n = int(self.L.foggy_vector_length(self.h))
 
+    def set_gaussian_beams(self, waist, tem, theta, phi, jones, g, phase=None, d_0_i=None, convention=None):
+        """Gaussian beams added to the plane waves (foggy_set_gaussian_beams; the reference's
+        lib_mie_illumination_gaussian_beam_parameter list with calculation_type 3).  waist (nb, 2),
+        tem (nb, 2), theta, phi, g, phase (nb,), jones (nb, 4) re x, im x, re y, im y,
+        d_0_i (nb, 3), convention (nb,)."""
+        nb = len(np.atleast_1d(theta))
+        arrs = [N.as_f64(waist).reshape(-1), N.as_i32(tem).reshape(-1), N.as_f64(theta), N.as_f64(phi),
+                N.as_f64(jones).reshape(-1), N.as_f64(g),
+                N.as_f64(phase) if phase is not None else None,
+                N.as_f64(d_0_i).reshape(-1) if d_0_i is not None else None,
+                N.as_i32(convention) if convention is not None else None]
+        self._beams = arrs
+        ptrs = [(a.ctypes.data if a is not None else None) for a in arrs]
+        N.check(self.L.foggy_set_gaussian_beams(self.h, nb, *ptrs), self.h)
+
+    def set_plane_waves(self, theta, phi, jones, g, phase, d_0_i):
+        """Replace the plane waves (an empty list leaves only the Gaussian beams)."""
+        w = [N.as_f64(theta), N.as_f64(phi), N.as_f64(jones).reshape(-1), N.as_f64(g), N.as_f64(phase),
+             N.as_f64(d_0_i).reshape(-1)]
+        self._waves = w
+        N.check(self.L.foggy_set_plane_waves(self.h, len(w[0]), *[N.ptr(a) for a in w]), self.h)
+
     def n_range(self):
         return int(self.params.n_range[0]), int(self.params.n_range[1])
 
