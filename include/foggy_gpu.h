@@ -279,6 +279,88 @@ int32_t foggy_tree_domain(foggy_handle h, int32_t l, int64_t n, int32_t kind, in
  * finished on the handle's stream. */
 int32_t foggy_matvec_static(foggy_handle h, const double* x, double* y);
 
+/* ---- several right-hand sides --------------------------------------------------------- */
+
+/* One solve per plane wave set on the handle (nrhs must equal that count; no Gaussian beams):
+ * right-hand side r is the incidence of wave r alone, as the reference obtains it by running
+ * lib_mie_ms_solver_run once per illumination (lib_mie_ms_solver_interface.f90:143-154).  The
+ * operator and its pair tables are built once and shared.  x (and x0, if not NULL) hold nrhs
+ * vectors of foggy_vector_length entries one after the other; cross_sections (NULL to skip)
+ * receives {C_sca, C_ext, C_abs} per right-hand side.  stats sums iterations, restarts,
+ * matvecs and times over the solves, with the largest backward error; the status is that of the
+ * first solve that did not converge, or FOGGY_OK. */
+int32_t foggy_solve_rhs(foggy_handle h, int32_t nrhs, const double* x0, double* x, int32_t mem, foggy_stats* stats,
+                        double* cross_sections);
+
+/* ---- serving ------------------------------------------------------------------------- */
+
+/* A solve server on one GPU: requests of differing sphere counts, truncation orders and
+ * right-hand-side counts are queued first in, first out and admitted when their device footprint
+ * (scene, operator slabs, Krylov workspace, staging and, when they fit an equal share of the
+ * budget, pair tables) fits beside the requests already running; up to max_concurrent run at
+ * once, each on its own handle and CUDA stream, so each result equals the one its request gets
+ * alone.  A request larger than the whole budget is refused (FOGGY_REQ_REFUSED,
+ * FOGGY_ERR_NOMEM).  memory_budget <= 0 takes 85 % of the free device memory.  The reference has
+ * no serving layer; each request runs lib_mie_ms_solver_run with the direct operator. */
+typedef struct foggy_server_s* foggy_server;
+
+#define FOGGY_REQ_QUEUED    0
+#define FOGGY_REQ_RUNNING   1
+#define FOGGY_REQ_DONE      2
+#define FOGGY_REQ_FAILED    3
+#define FOGGY_REQ_CANCELLED 4
+#define FOGGY_REQ_REFUSED   5
+
+/* One request; every array is copied at submission (layouts as foggy_set_spheres and
+ * foggy_set_plane_waves; phase and d_0_i may be NULL).  rhs_per_wave = 1 solves one right-hand
+ * side per plane wave (foggy_solve_rhs), 0 one right-hand side of all waves together. */
+typedef struct foggy_request {
+    const foggy_params* params;
+    int32_t n_spheres;
+    const double* centres;
+    const int32_t* param_index;
+    int32_t n_param;
+    const double* refractive_index;
+    const double* radius;
+    const int32_t* n_range;
+    int32_t nw;
+    const double* theta;
+    const double* phi;
+    const double* jones;
+    const double* g;
+    const double* phase;
+    const double* d_0_i;
+    int32_t rhs_per_wave;
+} foggy_request;
+
+typedef struct foggy_request_info {
+    int32_t state;               /* FOGGY_REQ_*                                              */
+    int32_t status;              /* FOGGY_OK or the solve's error                            */
+    int32_t nrhs;
+    int32_t reserved;
+    int64_t x_len;               /* doubles in the result: nrhs vectors, 2 per complex entry  */
+    int64_t footprint;           /* device bytes the request was admitted with               */
+    double  ms_queued;           /* submission to start (or to now / to the end if it never ran) */
+    double  ms_solve;            /* start to end                                             */
+    double  ms_latency;          /* submission to end (or to now)                            */
+    foggy_stats stats;
+    char    error[256];
+} foggy_request_info;
+
+int32_t foggy_server_start(int32_t device, int32_t max_concurrent, int64_t memory_budget, foggy_server* out);
+int32_t foggy_server_submit(foggy_server s, const foggy_request* request, int64_t* id);
+/* State of a request; wait_ms > 0 waits up to that long for it to finish, < 0 without limit.
+ * When it is done, copies the solutions into x (x_len doubles at least; NULL to skip) and the
+ * cross-sections into cross_sections (3 nrhs doubles; NULL to skip). */
+int32_t foggy_server_poll(foggy_server s, int64_t id, int32_t wait_ms, foggy_request_info* info, double* x,
+                          int64_t x_len, double* cross_sections);
+/* Removes a queued request (FOGGY_ERR_STATE once it runs). */
+int32_t foggy_server_cancel(foggy_server s, int64_t id);
+/* Frees a finished request's results. */
+int32_t foggy_server_release(foggy_server s, int64_t id);
+/* Cancels the queued requests, waits for the running ones and frees the server. */
+int32_t foggy_server_stop(foggy_server s);
+
 #ifdef __cplusplus
 }
 #endif

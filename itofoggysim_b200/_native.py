@@ -35,7 +35,9 @@ EXPORTS = [
     "foggy_get_vector_b", "foggy_matvec", "foggy_solve", "foggy_get_backward_error",
     "foggy_cross_sections", "foggy_translation_coefficients", "foggy_wigner_3j", "foggy_build_tree",
     "foggy_universal_index", "foggy_tree_boxes", "foggy_matvec_static", "foggy_tree_domain",
-    "foggy_get_field", "foggy_set_gaussian_beams",
+    "foggy_get_field", "foggy_set_gaussian_beams", "foggy_solve_rhs", "foggy_server_start",
+    "foggy_server_submit", "foggy_server_poll", "foggy_server_cancel", "foggy_server_release",
+    "foggy_server_stop",
 ]
 
 
@@ -77,6 +79,46 @@ class FoggyStats(C.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class FoggyRequest(C.Structure):
+    _fields_ = [
+        ("params", C.POINTER(FoggyParams)),
+        ("n_spheres", C.c_int32),
+        ("centres", C.c_void_p),
+        ("param_index", C.c_void_p),
+        ("n_param", C.c_int32),
+        ("refractive_index", C.c_void_p),
+        ("radius", C.c_void_p),
+        ("n_range", C.c_void_p),
+        ("nw", C.c_int32),
+        ("theta", C.c_void_p),
+        ("phi", C.c_void_p),
+        ("jones", C.c_void_p),
+        ("g", C.c_void_p),
+        ("phase", C.c_void_p),
+        ("d_0_i", C.c_void_p),
+        ("rhs_per_wave", C.c_int32),
+    ]
+
+
+class FoggyRequestInfo(C.Structure):
+    _fields_ = [
+        ("state", C.c_int32),
+        ("status", C.c_int32),
+        ("nrhs", C.c_int32),
+        ("reserved", C.c_int32),
+        ("x_len", C.c_int64),
+        ("footprint", C.c_int64),
+        ("ms_queued", C.c_double),
+        ("ms_solve", C.c_double),
+        ("ms_latency", C.c_double),
+        ("stats", FoggyStats),
+        ("error", C.c_char * 256),
+    ]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED, REQ_REFUSED = range(6)
 
 
 class FoggyError(RuntimeError):
@@ -125,6 +167,13 @@ def load():
         "foggy_tree_domain": (i32, [vp, i32, i64, i32, pi64, pi32]),
         "foggy_get_field": (i32, [vp, vp, i32, i32, vp, dbl, vp, vp]),
         "foggy_set_gaussian_beams": (i32, [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+        "foggy_solve_rhs": (i32, [vp, i32, vp, vp, i32, C.POINTER(FoggyStats), vp]),
+        "foggy_server_start": (i32, [i32, i32, i64, C.POINTER(vp)]),
+        "foggy_server_submit": (i32, [vp, C.POINTER(FoggyRequest), pi64]),
+        "foggy_server_poll": (i32, [vp, i64, i32, C.POINTER(FoggyRequestInfo), vp, i64, vp]),
+        "foggy_server_cancel": (i32, [vp, i64]),
+        "foggy_server_release": (i32, [vp, i64]),
+        "foggy_server_stop": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -1350,6 +1351,120 @@ int32_t foggy_get_field(foggy_handle h, const double* x, int32_t mem, int32_t np
     return FOGGY_OK;
 }
 
+int32_t foggy_solve_rhs(foggy_handle h, int32_t nrhs, const double* x0, double* x, int32_t mem, foggy_stats* stats,
+                        double* cross_sections) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!x) return fail(h, FOGGY_ERR_ARGUMENT, "x is NULL");
+    if (nrhs < 1 || nrhs != (int)h->waves.size())
+        return fail(h, FOGGY_ERR_ARGUMENT, "nrhs must equal the number of plane waves set (one right-hand side each)");
+    if (!h->beams.empty()) return fail(h, FOGGY_ERR_ARGUMENT, "one right-hand side per plane wave excludes Gaussian beams");
+    const size_t len = (size_t)foggy_vector_length(h);
+    const std::vector<WaveDev> all = h->waves;
+    foggy_stats tot{};
+    int status = FOGGY_OK;
+    for (int r = 0; r < nrhs && status != FOGGY_ERR_CUDA; ++r) {
+        h->waves.assign(1, all[r]);
+        h->rhs_ready = false;
+        foggy_stats st{};
+        double* xr = x + 2 * len * r;
+        const double* x0r = x0 ? x0 + 2 * len * r : nullptr;
+        const int rc = foggy_solve(h, x0r, xr, mem, &st);
+        if (rc == FOGGY_ERR_CUDA || rc == FOGGY_ERR_ARGUMENT || rc == FOGGY_ERR_STATE || rc == FOGGY_ERR_NOMEM ||
+            rc == FOGGY_ERR_UNSUPPORTED) {
+            h->waves = all;
+            h->rhs_ready = false;
+            return rc;
+        }
+        if (rc != FOGGY_OK && status == FOGGY_OK) status = rc;
+        if (cross_sections) {
+            const int rc2 = foggy_cross_sections(h, xr, mem, cross_sections + 3 * r);
+            if (rc2 != FOGGY_OK) {
+                h->waves = all;
+                h->rhs_ready = false;
+                return rc2;
+            }
+        }
+        tot.iterations += st.iterations;
+        tot.restarts += st.restarts;
+        tot.matvecs += st.matvecs;
+        tot.backward_error = std::max(tot.backward_error, st.backward_error);
+        tot.ms_total += st.ms_total;
+        tot.ms_matvec += st.ms_matvec;
+        tot.ms_setup += st.ms_setup;
+        tot.kernel_launches += st.kernel_launches;
+    }
+    h->waves = all;
+    h->rhs_ready = false;
+    tot.status = status;
+    if (stats) *stats = tot;
+    return status;
+}
+
+}  // extern "C"
+
+namespace foggy {
+void raise_smem_ceiling(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> ceiling;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& c = ceiling[{func, dev}];
+    if (bytes > c && cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess)
+        c = bytes;
+}
+
+// Device bytes a direct-operator solve of this scene holds at its peak, from the same plan the
+// handle follows (scene arrays, operator slabs, Krylov workspace, host staging, pair tables).
+int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_index, int NP, const int* n_range,
+                             int pair_tables, int64_t* table_bytes_out) {
+    const int pg = prm.n_range[1];
+    std::vector<int> pp(NP);
+    for (int i = 0; i < NP; ++i) pp[i] = std::max(1, std::min(n_range[2 * i + 1], pg));
+    int64_t n_unk = 0;
+    int pmax = 1;
+    const int bounds[] = {0, 4, 8, 12, 16, 20, 24, 28, 32};
+    std::vector<int64_t> bucket(9, 0), cnt(34, 0);
+    for (int j = 0; j < N; ++j) {
+        const int p = pp[param_index[j]];
+        n_unk += 2 * (int64_t)p * (p + 2);
+        pmax = std::max(pmax, p);
+        cnt[std::min(p, 33)]++;
+        for (int b = 1; b < 9; ++b)
+            if (p > bounds[b - 1] && p <= bounds[b]) bucket[b]++;
+    }
+    int nbuckets = 0, cmax = 1;
+    for (int b = 1; b < 9; ++b)
+        if (bucket[b]) {
+            ++nbuckets;
+            cmax = std::max(cmax, (int)std::max<int64_t>(1, std::min<int64_t>(32, (148 * 6 + bucket[b] - 1) / bucket[b])));
+        }
+    const int64_t C = (int64_t)(pg + 1) * (pg + 1) - 1, len = 2 * C * N;
+    const int64_t v = (int64_t)sizeof(cplx);
+    int64_t bytes = 0;
+    bytes += (int64_t)N * 64 + (int64_t)(N + NP) * pmax * 2 * v + 4 * n_unk * v;     // scene, b, pq, scratch
+    bytes += (int64_t)nbuckets * cmax * n_unk * v;                                        // operator slabs
+    bytes += (int64_t)(prm.gmres_restart + 4) * n_unk * v + (int64_t)(prm.gmres_restart + 2) * 2048 * v;
+    bytes += 2 * len * v;                                                                 // host staging
+    const int64_t q = 2 * pmax + 2;
+    bytes += 256 * q * q * q + ((int64_t)64 << 20);                                      // order tables
+    int64_t tb = 0;
+    if (pair_tables >= 0 && N > 1) {
+        for (int a = 1; a <= 32; ++a)
+            for (int b = a; b <= 32; ++b) {
+                if (!cnt[a] || !cnt[b]) continue;
+                const int64_t pairs = (a == b) ? cnt[a] * (cnt[a] - 1) / 2 : cnt[a] * cnt[b];
+                tb += pairs * pair_block_size(a, b) * v;
+            }
+        tb += (int64_t)N * (N - 1) / 2 * 16 + 16;
+    }
+    if (table_bytes_out) *table_bytes_out = tb;
+    return bytes + (pair_tables == 1 ? tb : 0);
+}
+}  // namespace foggy
+
+extern "C" {
+
 int32_t foggy_cross_sections(foggy_handle h, const double* x, int32_t mem, double* out) {
     if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
     if (!x || !out) return fail(h, FOGGY_ERR_ARGUMENT, "x or out is NULL");
@@ -1418,7 +1533,7 @@ int32_t foggy_translation_coefficients(double x, double theta, double phi, const
     cudaMalloc(&dA, (size_t)Pn * Pnu * sizeof(cplx));
     cudaMalloc(&dB, (size_t)Pn * Pnu * sizeof(cplx));
     size_t smem = translation_pair_smem_bytes(pmax);
-    cudaFuncSetAttribute(k_translation_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    raise_smem_ceiling(reinterpret_cast<const void*>(k_translation_pair), smem);
     k_translation_pair<<<1, 256, smem, h->stream>>>(ax, dtabs(h), x, theta, phi, pn, pnu, z_selector, dA, dB);
     std::vector<cplx> hA((size_t)Pn * Pnu), hB((size_t)Pn * Pnu);
     cudaError_t e = cudaMemcpyAsync(hA.data(), dA, hA.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);

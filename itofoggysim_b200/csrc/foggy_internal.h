@@ -28,6 +28,14 @@ void build_axial_tables_qmajor(const AxialTables& t, std::vector<int64_t>& koff,
 void build_scalar_gaunt_qmajor(int NM, std::vector<int64_t>& koff, std::vector<double>& gs);
 void build_g_table(int pmax, std::vector<double>& g);
 void build_delta_table(int pmax, std::vector<double>& out);
+// Raises a kernel's dynamic shared-memory ceiling to at least `bytes` on the current device.  The
+// ceiling is a process-wide attribute of the function: handles launching the same kernel from
+// several threads only ever raise it, under one lock, so no launch finds it lowered by another.
+void raise_smem_ceiling(const void* func, size_t bytes);
+// device bytes a direct solve will hold; pair tables counted when pair_tables == 1 (their size in
+// *table_bytes either way)
+int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_index, int NP, const int* n_range,
+                             int pair_tables, int64_t* table_bytes);
 
 // ---- host: octree lists of the ML-FMM (fmm_tree.cpp) ----------------------------------------
 // Boxes of all levels l_min..l_max with a global id (level by level, ascending Morton code).

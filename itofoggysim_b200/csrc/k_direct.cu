@@ -631,7 +631,7 @@ size_t direct_smem_bytes(int pp, bool tabs) { return smem_bytes(pp, tabs); }
 void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s) {
     size_t smem = direct_smem_bytes(b.pp, a.pt.stab != nullptr);
     dim3 grid(b.ntargets, b.chunks);
-    cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    raise_smem_ceiling(reinterpret_cast<const void*>(k_direct), smem);
     k_direct<<<grid, kThreads, smem, s>>>(a, b);
 }
 
@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
 void launch_translate(const TransArgs& a, int ntargets, cudaStream_t s) {
     if (ntargets <= 0) return;
     size_t smem = smem_bytes(a.pp, false);
-    cudaFuncSetAttribute(k_translate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    raise_smem_ceiling(reinterpret_cast<const void*>(k_translate), smem);
     k_translate<<<ntargets, kThreads, smem, s>>>(a);
 }
 

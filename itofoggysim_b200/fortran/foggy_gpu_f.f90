@@ -56,6 +56,26 @@ module foggy_gpu_f
         integer(c_int64_t) :: kernel_launches
     end type foggy_stats
 
+    ! one solve request of the server (foggy_request): every pointer is c_loc of a contiguous array
+    type, bind(c), public :: foggy_request
+        type(c_ptr) :: params
+        integer(c_int32_t) :: n_spheres
+        type(c_ptr) :: centres, param_index
+        integer(c_int32_t) :: n_param
+        type(c_ptr) :: refractive_index, radius, n_range
+        integer(c_int32_t) :: nw
+        type(c_ptr) :: theta, phi, jones, g, phase, d_0_i
+        integer(c_int32_t) :: rhs_per_wave
+    end type foggy_request
+
+    type, bind(c), public :: foggy_request_info
+        integer(c_int32_t) :: state, status, nrhs, reserved
+        integer(c_int64_t) :: x_len, footprint
+        real(c_double) :: ms_queued, ms_solve, ms_latency
+        type(foggy_stats) :: stats
+        character(kind=c_char) :: error(256)
+    end type foggy_request_info
+
     interface
         subroutine foggy_default_params(p) bind(c, name="foggy_default_params")
             import :: foggy_params
@@ -212,6 +232,54 @@ module foggy_gpu_f
             type(c_ptr), value :: phase, d_0_i, convention   ! c_loc(...) or c_null_ptr for defaults
             integer(c_int32_t) :: rc
         end function
+        function foggy_solve_rhs(h, nrhs, x0, x, mem, stats, cross_sections) result(rc) bind(c, name="foggy_solve_rhs")
+            import :: c_ptr, c_int32_t, foggy_stats
+            type(c_ptr), value :: h, x0, x, cross_sections
+            integer(c_int32_t), value :: nrhs, mem
+            type(foggy_stats), intent(out) :: stats
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_server_start(device, max_concurrent, memory_budget, s) result(rc) &
+                bind(c, name="foggy_server_start")
+            import :: c_ptr, c_int32_t, c_int64_t
+            integer(c_int32_t), value :: device, max_concurrent
+            integer(c_int64_t), value :: memory_budget
+            type(c_ptr), intent(out) :: s
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_server_submit(s, request, id) result(rc) bind(c, name="foggy_server_submit")
+            import :: c_ptr, c_int32_t, c_int64_t, foggy_request
+            type(c_ptr), value :: s
+            type(foggy_request), intent(in) :: request
+            integer(c_int64_t), intent(out) :: id
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_server_poll(s, id, wait_ms, info, x, x_len, cross_sections) result(rc) &
+                bind(c, name="foggy_server_poll")
+            import :: c_ptr, c_int32_t, c_int64_t, foggy_request_info
+            type(c_ptr), value :: s, x, cross_sections
+            integer(c_int64_t), value :: id, x_len
+            integer(c_int32_t), value :: wait_ms
+            type(foggy_request_info), intent(out) :: info
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_server_cancel(s, id) result(rc) bind(c, name="foggy_server_cancel")
+            import :: c_ptr, c_int32_t, c_int64_t
+            type(c_ptr), value :: s
+            integer(c_int64_t), value :: id
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_server_release(s, id) result(rc) bind(c, name="foggy_server_release")
+            import :: c_ptr, c_int32_t, c_int64_t
+            type(c_ptr), value :: s
+            integer(c_int64_t), value :: id
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_server_stop(s) result(rc) bind(c, name="foggy_server_stop")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: s
+            integer(c_int32_t) :: rc
+        end function
         function foggy_matvec_static(h, x, y) result(rc) bind(c, name="foggy_matvec_static")
             import :: c_ptr, c_int32_t
             type(c_ptr), value :: h, x, y       ! device pointers
@@ -225,6 +293,8 @@ module foggy_gpu_f
     public :: foggy_wigner_3j, foggy_last_error, foggy_set_params, foggy_get_mie_coefficients
     public :: foggy_get_vector_b, foggy_build_tree, foggy_universal_index, foggy_tree_boxes
     public :: foggy_tree_domain, foggy_get_field, foggy_matvec_static, foggy_set_gaussian_beams
+    public :: foggy_solve_rhs, foggy_server_start, foggy_server_submit, foggy_server_poll
+    public :: foggy_server_cancel, foggy_server_release, foggy_server_stop
     public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
     public :: foggy_ms_get_backward_error, foggy_ms_destructor
 

@@ -155,6 +155,23 @@ class MultiSphereSolver:
             N.check(rc, self.h)
         return x, self.last_stats
 
+    def solve_rhs(self, x0=None, raise_on_error=True):
+        """One solve per plane wave (foggy_solve_rhs): x of shape (nrhs, n), cross-sections
+        (nrhs, 3) as {C_sca, C_ext, C_abs}, summed stats."""
+        nrhs = self.scene.n_waves
+        x = np.zeros(nrhs * self.n, np.complex128)
+        cs = np.zeros(3 * nrhs)
+        st = N.FoggyStats()
+        x0p = None
+        if x0 is not None:
+            x0 = N.as_c128(np.asarray(x0).reshape(-1))
+            x0p = x0.ctypes.data
+        rc = self.L.foggy_solve_rhs(self.h, nrhs, x0p, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), cs.ctypes.data)
+        self.last_stats = st.as_dict()
+        if raise_on_error:
+            N.check(rc, self.h)
+        return x.reshape(nrhs, self.n), cs.reshape(nrhs, 3), self.last_stats
+
     def solve_device(self, x_ptr, x0_ptr=None):
         st = N.FoggyStats()
         rc = self.L.foggy_solve(self.h, C.c_void_p(x0_ptr) if x0_ptr else None, C.c_void_p(x_ptr),
