@@ -282,6 +282,55 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args):
+    """A seeded Poisson stream of solve requests (itofoggysim_b200.scene.serving_request) submitted
+    at their arrival times to the solve server; value = requests completed per second of the
+    stream's makespan, latency = submission to completion per request.  The same stream run one
+    request at a time gives the plain-path comparison."""
+    from itofoggysim_b200 import scene as S
+    from itofoggysim_b200.server import SolveServer
+    rng = np.random.default_rng(42)
+    reqs = [S.serving_request(rng) for _ in range(args.warmup + args.steps)]
+    gaps = np.random.default_rng(43).exponential(1.0 / 50.0, len(reqs))
+
+    def stream(concurrent):
+        with SolveServer(max_concurrent=concurrent) as srv:
+            for sc in reqs[:args.warmup]:
+                srv.wait(srv.submit(sc, rhs_per_wave=True))
+            t0 = time.perf_counter()
+            ids, t_arr = [], t0
+            for sc, gap in zip(reqs[args.warmup:], gaps[args.warmup:]):
+                t_arr += gap
+                dt = t_arr - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(srv.submit(sc, rhs_per_wave=True))
+            infos = [srv.wait(i)[0] for i in ids]
+            span = time.perf_counter() - t0
+        ok = [i for i in infos if i["state"] == 2]
+        lat = [i["ms_latency"] for i in ok]
+        return dict(solves_s=len(ok) / span, p50_ms=percentile(lat, 50), p99_ms=percentile(lat, 99),
+                    done=len(ok), failed=len(infos) - len(ok), makespan_s=span,
+                    rhs=int(sum(i["nrhs"] for i in ok)), iterations=int(sum(i["stats"]["iterations"] for i in ok)))
+
+    co = stream(args.concurrent)
+    one = stream(1)
+    timed = reqs[args.warmup:]
+    line = {
+        "metric": METRIC, "value": co["solves_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": co["makespan_s"] * 1e3 / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "serving stream (config 5, sphere counts scaled to 50-500)", "requests": args.steps,
+                   "arrivals": "Poisson, 50 per s", "spheres": [int(min(r.n_spheres for r in timed)),
+                                                                 int(max(r.n_spheres for r in timed))],
+                   "rhs_total": co["rhs"], "gmres_tolerance": 1e-6, "concurrent": args.concurrent,
+                   "admission": "FIFO by device footprint"},
+        "latency_ms": {"p50": co["p50_ms"], "p99": co["p99_ms"]},
+        "serving": co, "one_at_a_time": one,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def config_of(sc, args):
     p = sc.p_of_sphere()
     return {"workload": sc.name, "spheres": sc.n_spheres, "p_max": int(p.max()), "p_median": float(np.median(p)),
@@ -300,7 +349,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="medium", choices=["medium", "small"])
+    ap.add_argument("--workload", default="medium", choices=["medium", "small", "serving"],
+                    help="serving: a request stream through the solve server (its own JSON line)")
+    ap.add_argument("--concurrent", type=int, default=3, help="co-resident requests of the serving workload")
     ap.add_argument("--operator", default="direct", choices=["direct", "mlfmm"],
                     help="mlfmm: the ML-FMM passes (fmm_convention below) instead of all pairs")
     ap.add_argument("--fmm-convention", type=int, default=0, choices=[0, 1])
@@ -312,6 +363,13 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.workload == "serving":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving layer"}), flush=True)
+        elif rank == 0:
+            run_serving(args)
+        return
 
     if args.impl == "reference":
         if not args.matvecs_per_solve and not MATVECS_PER_SOLVE[args.workload]:

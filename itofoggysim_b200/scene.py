@@ -238,3 +238,27 @@ def hcp_sphere_scene(sphere_radius, lattice_sphere_radius=0.0076, particle_radiu
                  radius=np.array([particle_radius]), n_range_param=np.array([[1, n_max]], np.int32),
                  n_range=(1, n_max), z_coupling=1, reference_row_rule=True, gmres_restart=10,
                  gmres_tolerance=1e-6, name="hcp_sphere_%g" % sphere_radius, **waves)
+
+
+# ---- serving stream ----------------------------------------------------------------------------
+
+def serving_request(rng, n_lo=50, n_hi=500):
+    """One request of the serving stream: sphere count log-uniform in [n_lo, n_hi], lognormal radii
+    (median uniform in 0.4-0.8 um, sigma_ln 0.3, clipped to 0.2-1.2 um so that every truncation
+    order stays within the direct operator's 32), m = 1.33 + 1e-8 i, wavelength uniform in
+    0.45-0.65 um, volume fraction uniform in 1-5 % (cube edge (N E[V] / vf)^(1/3)), 1-16
+    right-hand sides along random directions, x-polarised (TM), GMRES(30) to 1e-6."""
+    n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+    med = rng.uniform(0.4, 0.8)
+    radii = np.clip(med * np.exp(0.3 * rng.standard_normal(n)), 0.2, 1.2)
+    lam = rng.uniform(0.45, 0.65)
+    vf = rng.uniform(0.01, 0.05)
+    box = (np.sum(4.0 / 3.0 * math.pi * radii ** 3) / vf) ** (1.0 / 3.0)
+    nr = int(rng.integers(1, 17))
+    th = np.arccos(rng.uniform(-1.0, 1.0, nr))
+    ph = rng.uniform(0.0, 2.0 * math.pi, nr)
+    waves = dict(wave_theta=th, wave_phi=ph, jones=np.tile([1.0, 0.0, 0.0, 0.0], (nr, 1)), wave_g=np.ones(nr),
+                 wave_phase=np.zeros(nr), wave_d0=np.zeros((nr, 3)))
+    return make_scene(radii, box, int(rng.integers(1 << 30)), lambda_0=lam, waves=waves, z_coupling=3,
+                      reference_row_rule=False, gmres_restart=30, gmres_tolerance=1e-6,
+                      name="serving_%d" % n)
