@@ -251,6 +251,17 @@ def cpu_sample(sc, budget_s=15.0, seed=0):
     return per_pair * N * (N - 1), done, elapsed
 
 
+def job_rate(local_ms, units, world, torch, dev, dist):
+    """Whole-job rate of replicas: every rank processed `units` in local_ms of its own device
+    time; the job's time is the slowest rank's, so rate = world * units / max over ranks.
+    Returns (rate per second, max_ms)."""
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    return world * units / (max_ms * 1e-3), max_ms
+
+
 def percentile(v, q):
     return float(np.percentile(np.asarray(v), q)) if len(v) else None
 
@@ -422,11 +433,7 @@ def main():
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * args.steps / (max_ms * 1e-3)
+    value, max_ms = job_rate(total_ms, args.steps, world, torch, dev, dist)
     x_dev = xbuf.cpu().numpy().view(np.complex128)
     berr = s.get_backward_error()
     tree = s.build_tree() if fmm else None
@@ -449,10 +456,7 @@ def main():
     h2d = (sc.centres.nbytes + sc.param_index.nbytes + sc.refractive_index.nbytes + sc.radius.nbytes
            + sc.n_range_param.nbytes + 6 * 8 * sc.n_waves)
     d2h = xh.nbytes
-    e2e_t = torch.tensor([float(np.mean(e2e_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world / (float(e2e_t.item()) * 1e-3)
+    e2e_value, _ = job_rate(float(np.mean(e2e_ms)), 1, world, torch, dev, dist)
 
     result = None
     if rank == 0:
