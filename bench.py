@@ -342,6 +342,50 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def fibonacci_waves(n_dir):
+    """n_dir incidence directions on a Fibonacci sphere (z_i = 1 - (2i+1)/n, phi_i = i pi (3 - sqrt 5))
+    times the two polarisations TM (Jones (1, 0)) and TE (Jones (0, 1))."""
+    i = np.arange(n_dir)
+    th = np.arccos(1.0 - (2.0 * i + 1.0) / n_dir)
+    ph = np.mod(i * math.pi * (3.0 - math.sqrt(5.0)), 2.0 * math.pi)
+    th2, ph2 = np.repeat(th, 2), np.repeat(ph, 2)
+    jones = np.tile([[1.0, 0.0, 0.0, 0.0], [0.0, 0.0, 1.0, 0.0]], (n_dir, 1))
+    n = 2 * n_dir
+    return dict(wave_theta=th2, wave_phi=ph2, jones=jones, wave_g=np.ones(n), wave_phase=np.zeros(n),
+                wave_d0=np.zeros((n, 3)))
+
+
+def run_multi_rhs(args):
+    """Several right-hand sides of one scene through foggy_solve_rhs: the 64-sphere cluster (the
+    small workload) under 64 Fibonacci directions x 2 polarisations = 128 right-hand sides, GMRES
+    to 1e-6; value = right-hand sides solved per second (device time)."""
+    import torch
+    from itofoggysim_b200 import scene as S, solver
+    sc = S.small_cluster()
+    sc = S.Scene(**{**sc.__dict__, **fibonacci_waves(64), "gmres_tolerance": 1e-6, "name": "small_cluster_64_rhs128"})
+    with solver.MultiSphereSolver(sc) as s:
+        for _ in range(args.warmup):
+            s.solve_rhs()
+        torch.cuda.synchronize()
+        tot_ms, iters = 0.0, 0
+        for _ in range(args.steps):
+            x, cs, st = s.solve_rhs()
+            tot_ms += st["ms_total"]
+            iters += st["iterations"]
+    nrhs = sc.n_waves
+    line = {
+        "metric": METRIC, "value": nrhs * args.steps / (tot_ms * 1e-3), "unit": "rhs solves/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "64-sphere cluster x 128 right-hand sides (config 4 scaled: 64 Fibonacci "
+                               "directions x TM/TE)", "rhs": nrhs, "gmres_tolerance": 1e-6,
+                   "solver": "one GMRES per right-hand side on a shared operator and pair tables"},
+        "iterations_per_rhs": iters / (args.steps * nrhs),
+        "c_ext_range": [float(cs[:, 1].min()), float(cs[:, 1].max())],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def config_of(sc, args):
     p = sc.p_of_sphere()
     return {"workload": sc.name, "spheres": sc.n_spheres, "p_max": int(p.max()), "p_median": float(np.median(p)),
@@ -360,7 +404,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="medium", choices=["medium", "small", "serving"],
+    ap.add_argument("--workload", default="medium", choices=["medium", "small", "serving", "multi_rhs"],
                     help="serving: a request stream through the solve server (its own JSON line)")
     ap.add_argument("--concurrent", type=int, default=3, help="co-resident requests of the serving workload")
     ap.add_argument("--operator", default="direct", choices=["direct", "mlfmm"],
@@ -374,6 +418,14 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.workload == "multi_rhs":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "CPU reference arm times the single-RHS workloads"}),
+                  flush=True)
+        elif rank == 0:
+            run_multi_rhs(args)
+        return
 
     if args.workload == "serving":
         if args.impl == "reference":
