@@ -292,6 +292,11 @@ int32_t foggy_matvec_static(foggy_handle h, const double* x, double* y);
 int32_t foggy_solve_rhs(foggy_handle h, int32_t nrhs, const double* x0, double* x, int32_t mem, foggy_stats* stats,
                         double* cross_sections);
 
+/* y_v = A x_v for nrhs vectors one after the other (reference layout, foggy_vector_length entries
+ * each): lib_mie_ms_solver_calculate_vector_b (lib_mie_ms_solver_interface.f90:739-783) for several
+ * vectors in one call; each y_v equals foggy_matvec of x_v. */
+int32_t foggy_matvec_rhs(foggy_handle h, int32_t nrhs, const double* x, double* y, int32_t mem);
+
 /* ---- serving ------------------------------------------------------------------------- */
 
 /* A solve server on one GPU: requests of differing sphere counts, truncation orders and

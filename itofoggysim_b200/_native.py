@@ -37,7 +37,7 @@ EXPORTS = [
     "foggy_universal_index", "foggy_tree_boxes", "foggy_matvec_static", "foggy_tree_domain",
     "foggy_get_field", "foggy_set_gaussian_beams", "foggy_solve_rhs", "foggy_server_start",
     "foggy_server_submit", "foggy_server_poll", "foggy_server_cancel", "foggy_server_release",
-    "foggy_server_stop",
+    "foggy_server_stop", "foggy_matvec_rhs",
 ]
 
 
@@ -174,6 +174,7 @@ def load():
         "foggy_server_cancel": (i32, [vp, i64]),
         "foggy_server_release": (i32, [vp, i64]),
         "foggy_server_stop": (i32, [vp]),
+        "foggy_matvec_rhs": (i32, [vp, i32, vp, vp, i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1465,6 +1465,15 @@ int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_in
 
 extern "C" {
 
+// y_v = A x_v for nrhs vectors (reference layout, len entries apart), one operator application each
+int32_t foggy_matvec_rhs(foggy_handle h, int32_t nrhs, const double* x, double* y, int32_t mem) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!x || !y || nrhs < 1) return fail(h, FOGGY_ERR_ARGUMENT, "x or y is NULL, or nrhs < 1");
+    const size_t len = (size_t)foggy_vector_length(h);
+    for (int v = 0; v < nrhs; ++v) TRY(foggy_matvec(h, x + 2 * (size_t)v * len, y + 2 * (size_t)v * len, mem));
+    return FOGGY_OK;
+}
+
 int32_t foggy_cross_sections(foggy_handle h, const double* x, int32_t mem, double* out) {
     if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
     if (!x || !out) return fail(h, FOGGY_ERR_ARGUMENT, "x or out is NULL");

@@ -239,6 +239,12 @@ module foggy_gpu_f
             type(foggy_stats), intent(out) :: stats
             integer(c_int32_t) :: rc
         end function
+        function foggy_matvec_rhs(h, nrhs, x, y, mem) result(rc) bind(c, name="foggy_matvec_rhs")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: h, x, y
+            integer(c_int32_t), value :: nrhs, mem
+            integer(c_int32_t) :: rc
+        end function
         function foggy_server_start(device, max_concurrent, memory_budget, s) result(rc) &
                 bind(c, name="foggy_server_start")
             import :: c_ptr, c_int32_t, c_int64_t
@@ -294,7 +300,7 @@ module foggy_gpu_f
     public :: foggy_get_vector_b, foggy_build_tree, foggy_universal_index, foggy_tree_boxes
     public :: foggy_tree_domain, foggy_get_field, foggy_matvec_static, foggy_set_gaussian_beams
     public :: foggy_solve_rhs, foggy_server_start, foggy_server_submit, foggy_server_poll
-    public :: foggy_server_cancel, foggy_server_release, foggy_server_stop
+    public :: foggy_server_cancel, foggy_server_release, foggy_server_stop, foggy_matvec_rhs
     public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
     public :: foggy_ms_get_backward_error, foggy_ms_destructor
 

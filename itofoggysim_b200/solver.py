@@ -155,6 +155,14 @@ class MultiSphereSolver:
             N.check(rc, self.h)
         return x, self.last_stats
 
+    def calculate_vector_b_rhs(self, X):
+        """y_v = A x_v for the rows of X (foggy_matvec_rhs)."""
+        X = N.as_c128(np.asarray(X).reshape(-1))
+        nr = X.size // self.n
+        Y = np.zeros(nr * self.n, np.complex128)
+        N.check(self.L.foggy_matvec_rhs(self.h, nr, X.ctypes.data, Y.ctypes.data, N.FOGGY_MEM_HOST), self.h)
+        return Y.reshape(nr, self.n)
+
     def solve_rhs(self, x0=None, raise_on_error=True):
         """One solve per plane wave (foggy_solve_rhs): x of shape (nrhs, n), cross-sections
         (nrhs, 3) as {C_sca, C_ext, C_abs}, summed stats."""
