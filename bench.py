@@ -386,6 +386,41 @@ def run_multi_rhs(args):
     print(json.dumps(line), flush=True)
 
 
+def run_mixed(args):
+    """The workload solved with the FP32 operator in the Arnoldi steps and FP64 true residuals
+    (SURVEY config 3 on config 2's scene); value = solves/s (device time), with the relative error
+    of the coefficients and of C_ext against one FP64 solve of the same scene."""
+    import torch
+    from itofoggysim_b200 import solver
+    sc = workload_scene(args.workload)
+    with solver.MultiSphereSolver(sc) as s:
+        x64, st64 = s.solve()
+        c64 = s.cross_sections(x64)
+    with solver.MultiSphereSolver(sc, precision=1) as s:
+        for _ in range(args.warmup):
+            s.solve()
+        torch.cuda.synchronize()
+        ms, its, mvs = [], [], []
+        for _ in range(args.steps):
+            x, st = s.solve()
+            ms.append(st["ms_total"])
+            its.append(st["iterations"])
+            mvs.append(st["matvecs"])
+        c = s.cross_sections(x)
+    line = {
+        "metric": METRIC, "value": 1e3 / float(np.mean(ms)), "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": float(np.mean(ms)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 translations, f64 residuals", "data": "synthetic",
+        "config": {"workload": sc.name + " mixed precision (config 3)", "gmres_restart": sc.gmres_restart,
+                   "gmres_tolerance": sc.gmres_tolerance},
+        "fp64": {"ms_per_solve": st64["ms_total"], "iterations": st64["iterations"]},
+        "iterations": its[-1], "matvecs": mvs[-1], "backward_error": st["backward_error"],
+        "rel_coefficient_error": float(np.linalg.norm(x - x64) / np.linalg.norm(x64)),
+        "c_ext_rel_error": float(abs(c[1] - c64[1]) / abs(c64[1])),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def config_of(sc, args):
     p = sc.p_of_sphere()
     return {"workload": sc.name, "spheres": sc.n_spheres, "p_max": int(p.max()), "p_median": float(np.median(p)),
@@ -413,11 +448,22 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU sampling")
     ap.add_argument("--matvecs-per-solve", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: FP32 Arnoldi operator, FP64 true residuals (its own JSON line, with errors "
+                         "against an FP64 solve)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.precision == "mixed":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no mixed-precision solve"}),
+                  flush=True)
+        elif rank == 0:
+            run_mixed(args)
+        return
 
     if args.workload == "multi_rhs":
         if args.impl == "reference":

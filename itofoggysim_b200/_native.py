@@ -60,7 +60,7 @@ class FoggyParams(C.Structure):
         ("pair_tables", C.c_int32),
         ("fmm_convention", C.c_int32),
         ("z_translation_gt_r", C.c_int32),
-        ("reserved", C.c_int32),
+        ("precision", C.c_int32),
     ]
 
 

@@ -68,6 +68,8 @@ struct foggy_handle_s {
     int gs_nm = 0;
     // per-pair scalar coaxial coefficients (geometry only), when they fit the memory budget
     cplx* d_stab = nullptr;
+    cplxf* d_stab32 = nullptr;   // the pair tables in single precision (mixed-precision solves)
+    bool stab32_ready = false;
     int64_t* d_pair_off = nullptr;
     int stab_z = 0;
     bool stab_ready = false;
@@ -76,6 +78,7 @@ struct foggy_handle_s {
     double* d_irs = nullptr;
     double* d_rj = nullptr;
     double* d_delta = nullptr;    // d^j(pi/2), build_delta_table
+    float* d_delta32 = nullptr;   // the same in single precision
     int K = 0;
     // operator launches: (target bucket, source bucket) pairs of truncation-order buckets
     std::vector<DirectBucket> launches_direct;
@@ -230,6 +233,7 @@ int ensure_tables(foggy_handle h, int pmax) {
     dfree(h, h->d_rj);
     dfree(h, h->d_g);
     dfree(h, h->d_delta);
+    dfree(h, h->d_delta32);
     AxialTables t;
     build_axial_tables(pmax, t);
     TRY(dalloc(h, &h->d_axoff, t.offset.size()));
@@ -292,6 +296,9 @@ int ensure_tables(foggy_handle h, int pmax) {
         build_delta_table(pmax, dl);
         TRY(dalloc(h, &h->d_delta, dl.size()));
         CK(h, cudaMemcpy(h->d_delta, dl.data(), dl.size() * sizeof(double), cudaMemcpyHostToDevice));
+        std::vector<float> dl32(dl.begin(), dl.end());
+        TRY(dalloc(h, &h->d_delta32, dl32.size()));
+        CK(h, cudaMemcpy(h->d_delta32, dl32.data(), dl32.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
     std::vector<double> g;
     build_g_table(pmax, g);
@@ -319,6 +326,9 @@ DirectArgs direct_args(foggy_handle h, const cplx* x) {
     a.g = SGaunt{h->d_koffS, h->d_gs, h->gs_nm};
     a.dt = dtabs(h);
     a.pt.stab = h->stab_ready ? h->d_stab : nullptr;
+    a.pt.stab32 = h->stab32_ready ? h->d_stab32 : nullptr;
+    a.delta32 = h->d_delta32;
+    a.fp32 = 0;
     a.pt.pair_off = h->d_pair_off;
     a.z = h->prm.z_coupling;
     a.x = x;
@@ -385,33 +395,42 @@ int plan_direct(foggy_handle h) {
 // and read by every operator application.  Skipped when they do not fit (pair_tables = 0) or
 // when switched off (pair_tables = -1).
 int ensure_pair_tables(foggy_handle h) {
+    const bool mixed = h->prm.precision == 1;
     if (h->prm.pair_tables < 0 || h->N < 2) {
         h->stab_ready = false;
+        h->stab32_ready = false;
         return FOGGY_OK;
     }
-    if (h->stab_ready && h->stab_z == h->prm.z_coupling) return FOGGY_OK;
+    if (h->stab_z == h->prm.z_coupling && (mixed ? h->stab32_ready : h->stab_ready)) return FOGGY_OK;
     const int64_t npairs = (int64_t)h->N * (h->N - 1) / 2;
-    if (!h->d_stab) {
-        // total size from the counts of each truncation order
-        std::vector<int64_t> cnt(h->pmax + 1, 0);
-        for (int j = 0; j < h->N; ++j) cnt[h->p_s[j]]++;
-        int64_t tot = 0;
-        for (int a = 1; a <= h->pmax; ++a)
-            for (int b = a; b <= h->pmax; ++b) {
-                if (!cnt[a] || !cnt[b]) continue;
-                int64_t pairs = (a == b) ? cnt[a] * (cnt[a] - 1) / 2 : cnt[a] * cnt[b];
-                tot += pairs * pair_block_size(a, b);
-            }
-        size_t bytes = (size_t)tot * sizeof(cplx) + (size_t)npairs * 2 * sizeof(int64_t);
-        // keep room for the Krylov basis of the solve and 4 GiB for everything else
-        size_t room = h->budget > h->bytes_in_use ? h->budget - h->bytes_in_use : 0;
-        size_t reserve = (size_t)(h->prm.gmres_restart + 4) * (size_t)h->n_unk * sizeof(cplx) + ((size_t)4 << 30);
-        if (h->prm.pair_tables == 0 && bytes + reserve > room) {
-            h->stab_ready = false;
-            return FOGGY_OK;
+    // total size from the counts of each truncation order
+    std::vector<int64_t> cnt(h->pmax + 1, 0);
+    for (int j = 0; j < h->N; ++j) cnt[h->p_s[j]]++;
+    int64_t tot = 0;
+    for (int a = 1; a <= h->pmax; ++a)
+        for (int b = a; b <= h->pmax; ++b) {
+            if (!cnt[a] || !cnt[b]) continue;
+            int64_t pairs = (a == b) ? cnt[a] * (cnt[a] - 1) / 2 : cnt[a] * cnt[b];
+            tot += pairs * pair_block_size(a, b);
         }
+    // keep room for the Krylov basis of the solve and 4 GiB for everything else; a mixed-precision
+    // solve needs the single-precision tables and keeps the double ones too when both fit (its
+    // true residuals then use them; otherwise they sum S per application)
+    const size_t offb = h->d_pair_off ? 0 : (size_t)npairs * 2 * sizeof(int64_t);
+    const size_t b64 = h->d_stab ? 0 : (size_t)tot * sizeof(cplx);
+    const size_t b32 = h->d_stab32 ? 0 : (size_t)tot * sizeof(cplxf);
+    const size_t room = h->budget > h->bytes_in_use ? h->budget - h->bytes_in_use : 0;
+    const size_t reserve = (size_t)(h->prm.gmres_restart + 4) * (size_t)h->n_unk * sizeof(cplx) + ((size_t)4 << 30);
+    const bool force = h->prm.pair_tables == 1;
+    const bool want32 = mixed && (force || offb + b32 + reserve <= room);
+    const bool want64 = mixed ? (force || offb + b32 + b64 + reserve <= room) : (force || offb + b64 + reserve <= room);
+    if (!want32 && !want64) {
+        h->stab_ready = false;
+        h->stab32_ready = false;
+        return FOGGY_OK;
+    }
+    if (!h->d_pair_off) {
         TRY(dalloc(h, &h->d_pair_off, npairs + 1));
-        TRY(dalloc(h, &h->d_stab, (size_t)tot));
         int64_t* d_sizes = nullptr;
         CK(h, cudaMalloc(&d_sizes, npairs * sizeof(int64_t)));
         k_pair_sizes<<<h->N, 256, 0, h->stream>>>(scene_view(h), d_sizes);
@@ -430,10 +449,19 @@ int ensure_pair_tables(foggy_handle h) {
     SGaunt g{h->d_koffS, h->d_gs, h->gs_nm};
     int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, (148 * 8 + h->N - 1) / h->N));
     dim3 grid(h->N, chunks);
-    k_pair_s<<<grid, 256, 0, h->stream>>>(scene_view(h), g, h->prm.z_coupling, h->d_pair_off, h->d_stab, chunks);
-    h->launches += 1;
+    if (want64) {
+        if (!h->d_stab) TRY(dalloc(h, &h->d_stab, (size_t)tot));
+        launch_pair_s(scene_view(h), g, h->prm.z_coupling, h->d_pair_off, h->d_stab, false, grid, chunks, h->stream);
+        h->launches += 1;
+        h->stab_ready = true;
+    }
+    if (want32) {
+        if (!h->d_stab32) TRY(dalloc(h, &h->d_stab32, (size_t)tot));
+        launch_pair_s(scene_view(h), g, h->prm.z_coupling, h->d_pair_off, h->d_stab32, true, grid, chunks, h->stream);
+        h->launches += 1;
+        h->stab32_ready = true;
+    }
     CKL(h);
-    h->stab_ready = true;
     h->stab_z = h->prm.z_coupling;
     return FOGGY_OK;
 }
@@ -640,10 +668,12 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
 }
 
 // y = A x in the device layout
-int apply_operator(foggy_handle h, const cplx* x, cplx* y) {
+// fp32: the single-precision operator (mixed-precision solves' Arnoldi steps), when its tables exist
+int apply_operator(foggy_handle h, const cplx* x, cplx* y, bool fp32 = false) {
     if (h->prm.matvec_mode == FOGGY_MATVEC_MLFMM) return apply_operator_fmm(h, x, y);
     TRY(ensure_pair_tables(h));
     DirectArgs a = direct_args(h, x);
+    a.fp32 = (fp32 && h->stab32_ready) ? 1 : 0;
     for (const DirectBucket& b : h->launches_direct) {
         launch_direct(a, b, h->stream);
         h->launches += 1;
@@ -709,6 +739,8 @@ void free_scene(foggy_handle h) {
     dfree(h, h->d_pq);
     dfree(h, h->d_partial);
     dfree(h, h->d_stab);
+    dfree(h, h->d_stab32);
+    h->stab32_ready = false;
     dfree(h, h->d_pair_off);
     h->stab_ready = false;
     dfree(h, h->d_tmp_in);
@@ -782,12 +814,15 @@ int gmres(foggy_handle h, foggy_stats* st) {
     double* d_res = h->d_scal + 2;
     double* d_bn = h->d_scal + 3;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> mv_events;
-    auto matvec = [&](const cplx* x, cplx* y) -> int {
+    // Arnoldi steps of a mixed-precision solve use the FP32 operator; the true residuals (start and
+    // every restart) the FP64 one, so the restarts refine the solution to the FP64 tolerance
+    const bool mixed = h->prm.precision == 1;
+    auto matvec = [&](const cplx* x, cplx* y, bool arnoldi) -> int {
         cudaEvent_t a, b;
         cudaEventCreate(&a);
         cudaEventCreate(&b);
         cudaEventRecord(a, h->stream);
-        int r = apply_operator(h, x, y);
+        int r = apply_operator(h, x, y, arnoldi && mixed);
         cudaEventRecord(b, h->stream);
         mv_events.push_back({a, b});
         st->matvecs++;
@@ -804,7 +839,7 @@ int gmres(foggy_handle h, foggy_stats* st) {
         mv_events.clear();
     };
     TRY(norm_dev(h, h->d_b, d_bn));
-    TRY(matvec(h->d_x, h->d_w));
+    TRY(matvec(h->d_x, h->d_w, false));
     k_sub<<<G, 256, 0, h->stream>>>(h->d_b, h->d_w, h->d_r, n);
     h->launches += 1;
     TRY(norm_dev(h, h->d_r, d_beta));
@@ -833,7 +868,7 @@ int gmres(foggy_handle h, foggy_stats* st) {
         for (; k < m && st->iterations < maxit; ++k) {
             cplx* vk = h->d_V + (size_t)k * n;
             cplx* vk1 = h->d_V + (size_t)(k + 1) * n;
-            TRY(matvec(vk, h->d_w));
+            TRY(matvec(vk, h->d_w, true));
             k_dots_partial<<<kRedBlocks, 256, 0, h->stream>>>(h->d_V, n, k + 1, h->d_w, n, h->d_part);
             k_dots_reduce<<<k + 1, 256, 0, h->stream>>>(h->d_part, k + 1, h->d_h, 0);
             k_axpy_multi<<<G, 256, 0, h->stream>>>(h->d_V, n, k + 1, h->d_h, h->d_w, n);
@@ -865,7 +900,7 @@ int gmres(foggy_handle h, foggy_stats* st) {
             h->launches += 2;
         }
         st->restarts++;
-        TRY(matvec(h->d_x, h->d_w));
+        TRY(matvec(h->d_x, h->d_w, false));
         k_sub<<<G, 256, 0, h->stream>>>(h->d_b, h->d_w, h->d_r, n);
         h->launches += 1;
     h->launches += 1;
@@ -925,6 +960,9 @@ static int check_params(foggy_handle h, const foggy_params* p) {
         return fail(h, FOGGY_ERR_ARGUMENT, "fmm_convention must be 0 or 1");
     if (p->z_translation_gt_r < 1 || p->z_translation_gt_r > 4)
         return fail(h, FOGGY_ERR_ARGUMENT, "z_translation_gt_r must be 1..4");
+    if (p->precision != 0 && p->precision != 1) return fail(h, FOGGY_ERR_ARGUMENT, "precision must be 0 (FP64) or 1 (mixed)");
+    if (p->precision == 1 && p->matvec_mode == FOGGY_MATVEC_MLFMM)
+        return fail(h, FOGGY_ERR_UNSUPPORTED, "mixed precision is built for the direct operator only");
     return FOGGY_OK;
 }
 
@@ -1458,6 +1496,7 @@ int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_in
             }
         tb += (int64_t)N * (N - 1) / 2 * 16 + 16;
     }
+    if (prm.precision == 1) tb += tb / 2;   // single-precision tables beside the double ones
     if (table_bytes_out) *table_bytes_out = tb;
     return bytes + (pair_tables == 1 ? tb : 0);
 }

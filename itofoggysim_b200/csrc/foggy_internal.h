@@ -82,6 +82,24 @@ __host__ __device__ __forceinline__ cplx operator*(cplx a, cplx b) {
 }
 __host__ __device__ __forceinline__ cplx operator*(double s, cplx a) { return mk(s * a.x, s * a.y); }
 __host__ __device__ __forceinline__ cplx conjg(cplx a) { return mk(a.x, -a.y); }
+// single-precision complex of the FP32 operator (the translation arithmetic of the mixed-precision
+// solve); scalars of either precision multiply it in single precision
+struct cplxf {
+    float x, y;
+};
+__host__ __device__ __forceinline__ cplxf operator+(cplxf a, cplxf b) { return cplxf{a.x + b.x, a.y + b.y}; }
+__host__ __device__ __forceinline__ cplxf operator-(cplxf a, cplxf b) { return cplxf{a.x - b.x, a.y - b.y}; }
+__host__ __device__ __forceinline__ cplxf operator*(cplxf a, cplxf b) {
+    return cplxf{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+__host__ __device__ __forceinline__ cplxf operator*(float s, cplxf a) { return cplxf{s * a.x, s * a.y}; }
+__host__ __device__ __forceinline__ cplxf operator*(double s, cplxf a) { return (float)s * a; }
+__host__ __device__ __forceinline__ cplxf conjg(cplxf a) { return cplxf{a.x, -a.y}; }
+// complex of type C from two reals
+template <class C>
+__host__ __device__ __forceinline__ C cm(double a, double b) {
+    return C{(decltype(C::x))a, (decltype(C::x))b};
+}
 __host__ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
     // Smith's algorithm
     if (fabs(b.x) >= fabs(b.y)) {

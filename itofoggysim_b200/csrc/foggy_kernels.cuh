@@ -66,6 +66,7 @@ struct DTabs {
 // row-major (S is symmetric in a and b).
 struct PairTabs {
     const cplx* stab;          // nullptr: the operator sums S from the Gaunt table per matvec
+    const cplxf* stab32;       // the same in single precision (FP32 operator)
     const int64_t* pair_off;
 };
 struct SGaunt {
@@ -87,12 +88,13 @@ __host__ __device__ __forceinline__ int64_t pair_block_size(int ps, int pt) {
     return pair_block_offset(km + 1, M2, M2);
 }
 __global__ void k_pair_sizes(SceneView sc, int64_t* sizes);
-__global__ void k_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, cplx* stab, int chunks);
 
 struct DirectArgs {
     SceneView sc;
     DTabs dt;                  // rs[j][k] = sqrt(j^2 - k^2) for the coaxial relation
     const double* delta;       // d^j(pi/2), gaunt.cpp::build_delta_table layout
+    const float* delta32;      // the same in single precision
+    int fp32;                  // 1: the FP32 operator (stab32, delta32), FP64 input and slabs
     SGaunt g;                  // scalar Gaunt sums (no pair tables)
     PairTabs pt;
     int z;                     // radial function selector (1 j_n, 2 y_n, 3 h1, 4 h2)
@@ -111,9 +113,12 @@ struct DirectBucket {
     int chunks;                // CTAs per target (<= cmax)
     int pp;                    // largest degree of the launch (sizes shared memory)
 };
-size_t direct_smem_bytes(int pp, bool tabs);
+size_t direct_smem_bytes(int pp, bool tabs, bool fp32 = false);
 size_t translation_pair_smem_bytes(int pmax);
 void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s);
+// scalar coaxial tables of every pair, in FP64 (stab: cplx*) or FP32 (cplxf*)
+void launch_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, void* stab, bool fp32, dim3 grid,
+                   int chunks, cudaStream_t s);
 // y = x + T (sum of the slab partials) for coupled spheres, y = x otherwise
 __global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial, int slabs, int64_t n_unk,
                                 cplx* y);

@@ -7,12 +7,13 @@
 namespace foggy {
 
 // i^p c
-__device__ __forceinline__ cplx ipow_mul(int p, cplx c) {
+template <class C>
+__device__ __forceinline__ C ipow_mul(int p, C c) {
     switch (p & 3) {
         case 0: return c;
-        case 1: return mk(-c.y, c.x);
-        case 2: return mk(-c.x, -c.y);
-        default: return mk(c.y, -c.x);
+        case 1: return C{-c.y, c.x};
+        case 2: return C{-c.x, -c.y};
+        default: return C{c.y, -c.x};
     }
 }
 // t = n^2 - 1 + n + m (n >= 1, -n <= m <= n) -> (n, m)

@@ -69,14 +69,29 @@ __host__ __device__ inline int szB(int pp) { return 2 * (pp + 1) * (pp + 4); }
 __host__ __device__ inline int szAcc(int pp) { return 2 * pp * (pp + 2); }
 __host__ __device__ inline int szZ(int pp) { return 2 * pp + 4; }
 
+// element types of an operator precision: the complex C of its arithmetic and its real R
+template <class C>
+using real_of = decltype(C::x);
+template <class C>
+struct Vec2T;
+template <>
+struct Vec2T<cplx> {
+    using type = double2;
+};
+template <>
+struct Vec2T<cplxf> {
+    using type = float2;
+};
+
+template <class C>
 struct Bufs {
     short2* nk;    // [pp (pp + 3) / 2] item u -> (degree, order >= 0)
-    cplx* A;       // folded source (1), rotated source x' (3), folded translated field (5)
-    cplx* B;       // folded rotated source (2), w (4), folded rotated field (6)
-    cplx* acc;     // target accumulator (a | b), standard layout
-    cplx* eps;     // [2][pp + 1] e^{i mu (phi + pi/2)}
-    cplx* eth;     // [2][pp + 1] e^{-i s theta}
-    cplx* zeta;    // [2pp + 4] i^p z_p (no pair tables)
+    C* A;          // folded source (1), rotated source x' (3), folded translated field (5)
+    C* B;          // folded rotated source (2), w (4), folded rotated field (6)
+    C* acc;        // target accumulator (a | b), standard layout
+    C* eps;        // [2][pp + 1] e^{i mu (phi + pi/2)}
+    C* eth;        // [2][pp + 1] e^{-i s theta}
+    C* zeta;       // [2pp + 4] i^p z_p (no pair tables)
     double* jb;    // [2][2pp + 4]
     double* yb;    // [2][2pp + 4]
     double* rho;   // [2]
@@ -85,15 +100,17 @@ struct Bufs {
 __host__ __device__ inline int szNK(int pp) { return (pp * (pp + 3) / 2 + 3) & ~3; }
 
 // the radial functions and zeta are only kept when S is summed in the kernel (no pair tables)
+template <class C>
 __host__ __device__ inline size_t smem_bytes(int pp, bool tabs) {
     size_t c = (size_t)szA(pp) + szB(pp) + szAcc(pp) + 4 * (size_t)(pp + 1) + (tabs ? 0 : szZ(pp));
     size_t d = (tabs ? 0 : 4 * (size_t)szZ(pp)) + 2;
-    return c * sizeof(cplx) + d * sizeof(double) + (size_t)szNK(pp) * sizeof(short2);
+    return c * sizeof(C) + d * sizeof(double) + (size_t)szNK(pp) * sizeof(short2);
 }
 
-__device__ inline Bufs carve(double* base, int pp, bool tabs) {
-    Bufs s;
-    cplx* c = reinterpret_cast<cplx*>(base);
+template <class C>
+__device__ inline Bufs<C> carve(double* base, int pp, bool tabs) {
+    Bufs<C> s;
+    C* c = reinterpret_cast<C*>(base);
     s.A = c;           c += szA(pp);
     s.B = c;           c += szB(pp);
     s.acc = c;         c += szAcc(pp);
@@ -109,7 +126,8 @@ __device__ inline Bufs carve(double* base, int pp, bool tabs) {
 }
 
 // r += s w in two fused multiply-adds per component
-__device__ __forceinline__ void cmac(double& rx, double& ry, cplx s, cplx w) {
+template <class C>
+__device__ __forceinline__ void cmac(real_of<C>& rx, real_of<C>& ry, C s, C w) {
     rx = fma(s.x, w.x, rx);
     rx = fma(-s.y, w.y, rx);
     ry = fma(s.x, w.y, ry);
@@ -130,7 +148,8 @@ struct Disp {
 // tid <= pq the azimuthal phases, 64 <= tid <= 64 + pq the polar ones, 100/101 the Bessel
 // functions (only without pair tables), the last thread the distance; with a coaxial block
 // (sblock), 32..63 prefetch its rows into L2.
-__device__ inline void prep_pair(const Bufs& s, const Disp& g, int z, const cplx* sblock, int pj, int pl, int pp,
+template <class C>
+__device__ inline void prep_pair(const Bufs<C>& s, const Disp& g, int z, const C* sblock, int pj, int pl, int pp,
                                  int b, int tid, bool bessel) {
     const int pq = max(pj, pl);
     const bool e1 = tid <= pq;
@@ -141,9 +160,16 @@ __device__ inline void prep_pair(const Bufs& s, const Disp& g, int z, const cplx
         // rows mu = k..pl+1 of each order's square block, read by the coaxial stage of that pair
         const int M2 = pq + 2;
         for (int k = tid - 32; k <= min(pj, pl); k += 32) {
-            const cplx* rows = sblock + pair_block_offset(k, M2, M2);
-            const unsigned bytes = (unsigned)((pl + 2 - k) * (M2 - k) * sizeof(cplx));
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rows), "r"(bytes) : "memory");
+            // the bulk prefetch takes a 16-byte aligned address and a multiple of 16 bytes: the
+            // range is narrowed to the aligned part inside the rows (single-precision entries are
+            // 8 bytes)
+            const uintptr_t b0 = reinterpret_cast<uintptr_t>(sblock + pair_block_offset(k, M2, M2));
+            const uintptr_t b1 = b0 + (uintptr_t)(pl + 2 - k) * (M2 - k) * sizeof(C);
+            const uintptr_t a0 = (b0 + 15) & ~(uintptr_t)15, a1 = b1 & ~(uintptr_t)15;
+            if (a1 > a0) {
+                const unsigned bytes = (unsigned)(a1 - a0);
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"(bytes) : "memory");
+            }
         }
     }
     if (!(e1 || e2 || e3 || e4)) return;
@@ -155,7 +181,7 @@ __device__ inline void prep_pair(const Bufs& s, const Disp& g, int z, const cplx
         const double ph = (d0 == 0.0 && d1 == 0.0) ? 0.0 : atan2(d1, d0);
         double sn, cs;
         sincos((double)tid * ph, &sn, &cs);
-        s.eps[b * (pp + 1) + tid] = ipow_mul(tid, mk(cs, sn));
+        s.eps[b * (pp + 1) + tid] = ipow_mul(tid, cm<C>(cs, sn));
     }
     if (e2) {
         // the reference evaluates its Legendre functions at x = cos(theta) with sqrt(|1 - x^2|) as
@@ -167,7 +193,7 @@ __device__ inline void prep_pair(const Bufs& s, const Disp& g, int z, const cplx
         const int sidx = tid - 64;
         double sn, cs;
         sincos((double)sidx * te, &sn, &cs);
-        s.eth[b * (pp + 1) + sidx] = mk(cs, -sn);
+        s.eth[b * (pp + 1) + sidx] = cm<C>(cs, -sn);
     }
     if (e3) {
         const int P = pj + pl + 1;
@@ -178,15 +204,17 @@ __device__ inline void prep_pair(const Bufs& s, const Disp& g, int z, const cplx
 }
 
 // E = sum over even a, O = sum over odd a of Q[a (j+1) + o] u[a], a = 0..amax, for the two parts
-__device__ __forceinline__ void delta_sum(const double* __restrict__ Q, int j, int o, int amax, const cplx* ua,
-                                          const cplx* ub, cplx& Ea, cplx& Oa, cplx& Eb, cplx& Ob) {
-    double eax = 0, eay = 0, oax = 0, oay = 0, ebx = 0, eby = 0, obx = 0, oby = 0;
+template <class C>
+__device__ __forceinline__ void delta_sum(const real_of<C>* __restrict__ Q, int j, int o, int amax, const C* ua,
+                                          const C* ub, C& Ea, C& Oa, C& Eb, C& Ob) {
+    using R = real_of<C>;
+    R eax = 0, eay = 0, oax = 0, oay = 0, ebx = 0, eby = 0, obx = 0, oby = 0;
     const int st = j + 1;
     int a = 0;
     for (; a + 1 <= amax; a += 2) {
-        const double q0 = __ldg(Q + a * st + o);
-        const double q1 = __ldg(Q + (a + 1) * st + o);
-        const cplx u0 = ua[a], u1 = ua[a + 1], v0 = ub[a], v1 = ub[a + 1];
+        const R q0 = __ldg(Q + a * st + o);
+        const R q1 = __ldg(Q + (a + 1) * st + o);
+        const C u0 = ua[a], u1 = ua[a + 1], v0 = ub[a], v1 = ub[a + 1];
         eax += q0 * u0.x;
         eay += q0 * u0.y;
         oax += q1 * u1.x;
@@ -197,47 +225,49 @@ __device__ __forceinline__ void delta_sum(const double* __restrict__ Q, int j, i
         oby += q1 * v1.y;
     }
     if (a <= amax) {
-        const double q0 = __ldg(Q + a * st + o);
-        const cplx u0 = ua[a], v0 = ub[a];
+        const R q0 = __ldg(Q + a * st + o);
+        const C u0 = ua[a], v0 = ub[a];
         eax += q0 * u0.x;
         eay += q0 * u0.y;
         ebx += q0 * v0.x;
         eby += q0 * v0.y;
     }
-    Ea = mk(eax, eay);
-    Oa = mk(oax, oay);
-    Eb = mk(ebx, eby);
-    Ob = mk(obx, oby);
+    Ea = C{eax, eay};
+    Oa = C{oax, oay};
+    Eb = C{ebx, eby};
+    Ob = C{obx, oby};
 }
 
 // stages 2 and 6: W = Delta u at +-s, times e^{-+i s theta}; stored folded for the transposed
 // product as V = (-1)^s (W'_s +- W'_{-s}) at off2(j) + s and off2(j) + j + 1 + s
-__device__ __forceinline__ void fwd_item(const double* delta, const cplx* src, cplx* dst, int SP, int j, int s_,
-                                         int amax, cplx eth) {
+template <class C>
+__device__ __forceinline__ void fwd_item(const real_of<C>* delta, const C* src, C* dst, int SP, int j, int s_,
+                                         int amax, C eth) {
     const int fold = ((j + s_) & 1) ? j + 1 : 0;
-    const cplx* ua = src + off2(j) + fold;
-    cplx Ea, Oa, Eb, Ob;
+    const C* ua = src + off2(j) + fold;
+    C Ea, Oa, Eb, Ob;
     delta_sum(delta + qoff(j), j, s_, amax, ua, ua + SP, Ea, Oa, Eb, Ob);
-    const double pj_ = sgn(j), ps = sgn(s_);
-    cplx* d = dst + off2(j);
+    const real_of<C> pj_ = sgn(j), ps = sgn(s_);
+    C* d = dst + off2(j);
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
-        const cplx E = part ? Eb : Ea, O = part ? Ob : Oa;
-        const cplx wp = eth * (E + O);
+        const C E = part ? Eb : Ea, O = part ? Ob : Oa;
+        const C wp = eth * (E + O);
         if (s_ == 0) {
             d[part * SP] = wp;
             d[part * SP + j + 1] = wp;
         } else {
-            const cplx wm = conjg(eth) * (pj_ * (E - O));
+            const C wm = conjg(eth) * (pj_ * (E - O));
             d[part * SP + s_] = ps * (wp + wm);
             d[part * SP + j + 1 + s_] = ps * (wp - wm);
         }
     }
 }
 // Shared-memory buffers and tables of one CTA's translations.
+template <class C>
 struct PairCtx {
-    Bufs s;
-    const double* delta;   // d^j(pi/2)
+    Bufs<C> s;
+    const real_of<C>* delta;   // d^j(pi/2)
     DTabs dt;              // rs[j][k] = sqrt(j^2 - k^2)
     SGaunt g;              // scalar Gaunt sums (no coaxial block)
     int z;                 // radial function of the translation
@@ -250,11 +280,13 @@ struct PairCtx {
 // were prepared in buffer cur; next(tid) prepares the following translation into the other
 // buffer while the last stage runs.  Coincident centres (distance 0) add the source unchanged,
 // as the reference does for them.
-template <class Next>
-__device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const cplx* __restrict__ xl,
-                                const cplx* pair_s, int cur, Next next) {
-    const Bufs& s = c.s;
-    const double* delta = c.delta;
+template <class C, class Next>
+__device__ inline void run_pair(const PairCtx<C>& c, int tid, int pj, int pl, const cplx* __restrict__ xl,
+                                const C* pair_s, int cur, Next next) {
+    using R = real_of<C>;
+    using V2 = typename Vec2T<C>::type;
+    const Bufs<C>& s = c.s;
+    const R* delta = c.delta;
     const int pp = c.pp, SP = c.SP, XP = c.XP;
     const bool tabs = c.tabs;
     const int Pj = pj * (pj + 2);
@@ -262,7 +294,7 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
         const int pm = min(pj, pl), Pm = pm * (pm + 2), Pl = pl * (pl + 2);
         for (int t = tid; t < 2 * Pm; t += kThreads) {
             const int part = t >= Pm, e = t - part * Pm;
-            s.acc[part * Pj + e] = s.acc[part * Pj + e] + xl[part * Pl + e];
+            s.acc[part * Pj + e] = s.acc[part * Pj + e] + cm<C>(xl[part * Pl + e].x, xl[part * Pl + e].y);
         }
         next(tid);
         __syncthreads();
@@ -270,8 +302,8 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
     }
     const int Pl = pl * (pl + 2);
     const int kmax = min(pj, pl);
-    const cplx* eps = s.eps + cur * (pp + 1);
-    const cplx* eth = s.eth + cur * (pp + 1);
+    const C* eps = s.eps + cur * (pp + 1);
+    const C* eth = s.eth + cur * (pp + 1);
     // ---- 1. u = e^{i mu (phi + pi/2)} x, folded ------------------------------------------
     {
         const int items = pl * (pl + 3) / 2;
@@ -279,20 +311,20 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
             const short2 d_ = s.nk[t];
             const int nu = d_.x, mu = d_.y;
             const int base = nu * nu - 1 + nu;
-            const cplx e = eps[mu];
-            cplx* U = s.A + off2(nu) + mu;
+            const C e = eps[mu];
+            C* U = s.A + off2(nu) + mu;
             // the four source entries are all in flight before any use
             const double2* xv = reinterpret_cast<const double2*>(xl + base);
             const double2 ap = __ldcg(xv + mu), am = __ldcg(xv - mu);
             const double2 bp = __ldcg(xv + Pl + mu), bm = __ldcg(xv + Pl - mu);
-            const cplx ua = e * mk(ap.x, ap.y), ub = e * mk(bp.x, bp.y);
+            const C ua = e * cm<C>(ap.x, ap.y), ub = e * cm<C>(bp.x, bp.y);
             if (mu == 0) {
                 U[0] = ua;
                 U[nu + 1] = ua;
                 U[SP] = ub;
                 U[SP + nu + 1] = ub;
             } else {
-                const cplx va = conjg(e) * mk(am.x, am.y), vb = conjg(e) * mk(bm.x, bm.y);
+                const C va = conjg(e) * cm<C>(am.x, am.y), vb = conjg(e) * cm<C>(bm.x, bm.y);
                 U[0] = ua + va;
                 U[nu + 1] = ua - va;
                 U[SP] = ub + vb;
@@ -303,7 +335,10 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
             const int P = pj + pl + 1;
             const double* jb = s.jb + cur * szZ(pp);
             const double* yb = s.yb + cur * szZ(pp);
-            for (int p = tid; p <= P; p += kThreads) s.zeta[p] = zeta_of(c.z, p, jb, yb);
+            for (int p = tid; p <= P; p += kThreads) {
+                const cplx z = zeta_of(c.z, p, jb, yb);
+                s.zeta[p] = cm<C>(z.x, z.y);
+            }
         }
     }
     __syncthreads();
@@ -324,15 +359,15 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
             const short2 d_ = s.nk[t];
             const int nu = d_.x, k = d_.y;
             const int fold = ((nu + k) & 1) ? nu + 1 : 0;
-            const cplx* va = s.B + off2(nu) + fold;
-            cplx Ea, Oa, Eb, Ob;
+            const C* va = s.B + off2(nu) + fold;
+            C Ea, Oa, Eb, Ob;
             delta_sum(delta + qoff(nu), nu, k, nu, va, va + SP, Ea, Oa, Eb, Ob);
-            const double f = 2.0 * nu + 1.0;
-            const double pn = sgn(nu);
-            cplx* X = s.A + nu * nu - 1 + nu;
+            const R f = 2.0 * nu + 1.0;
+            const R pn = sgn(nu);
+            C* X = s.A + nu * nu - 1 + nu;
 #pragma unroll
             for (int part = 0; part < 2; ++part) {
-                const cplx E = part ? Eb : Ea, O = part ? Ob : Oa;
+                const C E = part ? Eb : Ea, O = part ? Ob : Oa;
                 X[part * XP + k] = ipow_mul(k, f * (E + O));
                 if (k > 0) X[part * XP - k] = ipow_mul(-k, (f * pn) * (E - O));
             }
@@ -352,29 +387,29 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
             }
             const int mu = k + rem;
             const int lo = max(1, k);
-            const double c0 = 2.0 * mu * (mu + 1.0);
-            const double c1m = (mu - 1 >= lo) ? x * 2.0 * (mu - 1) * c.dt.rs[mu * W + k] / (2.0 * mu - 1.0) : 0.0;
-            const double c2p = (mu + 1 <= pl) ? x * 2.0 * (mu + 2) * c.dt.rs[(mu + 1) * W + k] / (2.0 * mu + 3.0) : 0.0;
-            const double bk2 = 2.0 * k * x;
-            cplx* w = s.B + t;   // four planes of `items` entries: a'(+k), b'(+k), a'(-k), b'(-k)
+            const R c0 = 2.0 * mu * (mu + 1.0);
+            const R c1m = (mu - 1 >= lo) ? x * 2.0 * (mu - 1) * c.dt.rs[mu * W + k] / (2.0 * mu - 1.0) : 0.0;
+            const R c2p = (mu + 1 <= pl) ? x * 2.0 * (mu + 2) * c.dt.rs[(mu + 1) * W + k] / (2.0 * mu + 3.0) : 0.0;
+            const R bk2 = 2.0 * k * x;
+            C* w = s.B + t;   // four planes of `items` entries: a'(+k), b'(+k), a'(-k), b'(-k)
 #pragma unroll
             for (int sg = 0; sg < 2; ++sg) {
                 const int kk = sg ? -k : k;
-                const double bs = sg ? -bk2 : bk2;
-                cplx av[3], bv[3];
+                const R bs = sg ? -bk2 : bk2;
+                C av[3], bv[3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     const int nu = mu - 1 + d;
                     const bool ok = nu >= lo && nu <= pl;
                     const int o = nu * nu - 1 + nu + kk;
-                    av[d] = ok ? s.A[o] : mk(0, 0);
-                    bv[d] = ok ? s.A[XP + o] : mk(0, 0);
+                    av[d] = ok ? s.A[o] : C{0, 0};
+                    bv[d] = ok ? s.A[XP + o] : C{0, 0};
                 }
                 // wa = c0 a + i (bs b + c1m a_- - c2p a_+),  wb = c0 b + i (bs a + c1m b_- - c2p b_+)
-                const cplx ia = bs * bv[1] + c1m * av[0] - c2p * av[2];
-                const cplx ib = bs * av[1] + c1m * bv[0] - c2p * bv[2];
-                w[2 * sg * items] = mk(c0 * av[1].x - ia.y, c0 * av[1].y + ia.x);
-                w[(2 * sg + 1) * items] = mk(c0 * bv[1].x - ib.y, c0 * bv[1].y + ib.x);
+                const C ia = bs * bv[1] + c1m * av[0] - c2p * av[2];
+                const C ib = bs * av[1] + c1m * bv[0] - c2p * bv[2];
+                w[2 * sg * items] = C{c0 * av[1].x - ia.y, c0 * av[1].y + ia.x};
+                w[(2 * sg + 1) * items] = C{c0 * bv[1].x - ib.y, c0 * bv[1].y + ib.x};
             }
         }
     }
@@ -394,22 +429,22 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
                 ++k;
             }
             const int n = max(1, k) + rem;
-            const cplx* w = s.B + (k * (pl + 2) - k * (k - 1) / 2);
+            const C* w = s.B + (k * (pl + 2) - k * (k - 1) / 2);
             const int cnt = pl + 2 - k;
-            double r0x = 0, r0y = 0, r1x = 0, r1y = 0, r2x = 0, r2y = 0, r3x = 0, r3y = 0;
+            R r0x = 0, r0y = 0, r1x = 0, r1y = 0, r2x = 0, r2y = 0, r3x = 0, r3y = 0;
             if (tabs) {
                 const int Wk = M2 - k;
-                const double2* sp = reinterpret_cast<const double2*>(pair_s + pair_block_offset(k, M2, M2) + (n - k));
+                const V2* sp = reinterpret_cast<const V2*>(pair_s + pair_block_offset(k, M2, M2) + (n - k));
                 // kPrefetch5 coaxial entries in flight per thread: the rows come from L2, so the loop
                 // is bounded by how many loads overlap, not by the multiply-adds
                 int q = 0;
                 for (; q + kPrefetch5 <= cnt; q += kPrefetch5) {
-                    double2 sv[kPrefetch5];
+                    V2 sv[kPrefetch5];
 #pragma unroll
                     for (int u = 0; u < kPrefetch5; ++u) sv[u] = __ldcg(sp + (q + u) * Wk);
 #pragma unroll
                     for (int u = 0; u < kPrefetch5; ++u) {
-                        const cplx S = mk(sv[u].x, sv[u].y);
+                        const C S = C{sv[u].x, sv[u].y};
                         cmac(r0x, r0y, S, w[q + u]);
                         cmac(r1x, r1y, S, w[NW + q + u]);
                         cmac(r2x, r2y, S, w[2 * NW + q + u]);
@@ -417,8 +452,8 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
                     }
                 }
                 for (; q < cnt; ++q) {
-                    const double2 sv = __ldcg(sp + q * Wk);
-                    const cplx S = mk(sv.x, sv.y);
+                    const V2 sv = __ldcg(sp + q * Wk);
+                    const C S = C{sv.x, sv.y};
                     cmac(r0x, r0y, S, w[q]);
                     cmac(r1x, r1y, S, w[NW + q]);
                     cmac(r2x, r2y, S, w[2 * NW + q]);
@@ -439,24 +474,24 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
                         sx += gq * s.zeta[p].x;
                         sy += gq * s.zeta[p].y;
                     }
-                    const cplx S = mk(sx, sy);
+                    const C S = cm<C>(sx, sy);
                     cmac(r0x, r0y, S, w[q]);
                     cmac(r1x, r1y, S, w[NW + q]);
                     cmac(r2x, r2y, S, w[2 * NW + q]);
                     cmac(r3x, r3y, S, w[3 * NW + q]);
                 }
             }
-            const double f = sgn(k) / (2.0 * n * (n + 1.0));
-            cplx* U = s.A + off2(n) + k;
+            const R f = sgn(k) / (2.0 * n * (n + 1.0));
+            C* U = s.A + off2(n) + k;
             if (k == 0) {
-                U[0] = mk(f * r0x, f * r0y);
+                U[0] = C{f * r0x, f * r0y};
                 U[n + 1] = U[0];
-                U[SP] = mk(f * r1x, f * r1y);
+                U[SP] = C{f * r1x, f * r1y};
                 U[SP + n + 1] = U[SP];
             } else {
                 // u'_{+k} = i^{-k} y'(+k), u'_{-k} = i^{k} y'(-k)
-                const cplx ap = ipow_mul(-k, mk(f * r0x, f * r0y)), am = ipow_mul(k, mk(f * r2x, f * r2y));
-                const cplx bp = ipow_mul(-k, mk(f * r1x, f * r1y)), bm = ipow_mul(k, mk(f * r3x, f * r3y));
+                const C ap = ipow_mul(-k, C{f * r0x, f * r0y}), am = ipow_mul(k, C{f * r2x, f * r2y});
+                const C bp = ipow_mul(-k, C{f * r1x, f * r1y}), bm = ipow_mul(k, C{f * r3x, f * r3y});
                 U[0] = ap + am;
                 U[n + 1] = ap - am;
                 U[SP] = bp + bm;
@@ -482,15 +517,15 @@ __device__ inline void run_pair(const PairCtx& c, int tid, int pj, int pl, const
             const short2 d_ = s.nk[t];
             const int n = d_.x, m = d_.y;
             const int fold = ((n + m) & 1) ? n + 1 : 0;
-            const cplx* va = s.B + off2(n) + fold;
-            cplx Ea, Oa, Eb, Ob;
+            const C* va = s.B + off2(n) + fold;
+            C Ea, Oa, Eb, Ob;
             delta_sum(delta + qoff(n), n, m, n, va, va + SP, Ea, Oa, Eb, Ob);
-            const double pn = sgn(n);
-            const cplx e = eps[m];
-            cplx* acc = s.acc + n * n - 1 + n;
+            const R pn = sgn(n);
+            const C e = eps[m];
+            C* acc = s.acc + n * n - 1 + n;
 #pragma unroll
             for (int part = 0; part < 2; ++part) {
-                const cplx E = part ? Eb : Ea, O = part ? Ob : Oa;
+                const C E = part ? Eb : Ea, O = part ? Ob : Oa;
                 acc[part * Pj + m] = acc[part * Pj + m] + conjg(e) * (E + O);
                 if (m > 0) acc[part * Pj - m] = acc[part * Pj - m] + e * (pn * (E - O));
             }
@@ -515,7 +550,8 @@ __global__ void k_pair_sizes(SceneView sc, int64_t* sizes) {
 //   S(k; a, b) = sum_q (2p+1)(a b p; -k k 0)(a b p; 0 0 0) i^p z_p(k |d_t - d_s|),  p = a + b - 2q
 // for k = 0..min(p_s, p_t) on the square a, b = k..M+1, M = max(p_s, p_t) (S is symmetric in a, b;
 // the square lets either sphere of the pair read it with its own degree as the fast index).
-__global__ void __launch_bounds__(256) k_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, cplx* stab,
+template <class C>
+__global__ void __launch_bounds__(256) k_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, C* stab,
                                                 int chunks) {
     __shared__ double jb[2 * kMaxDegree + 8], yb[2 * kMaxDegree + 8];
     __shared__ cplx zeta[2 * kMaxDegree + 8];
@@ -540,7 +576,7 @@ __global__ void __launch_bounds__(256) k_pair_s(SceneView sc, SGaunt g, int z, c
         __syncthreads();
         for (int p = threadIdx.x; p <= P; p += blockDim.x) zeta[p] = zeta_of(z, p, jb, yb);
         __syncthreads();
-        cplx* out = stab + pair_off[pair_index(s, t, sc.n)];
+        C* out = stab + pair_off[pair_index(s, t, sc.n)];
         const int km = min(ps, pt);
         const int64_t tot = pair_block_size(ps, pt);
         for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
@@ -560,19 +596,27 @@ __global__ void __launch_bounds__(256) k_pair_s(SceneView sc, SGaunt g, int z, c
                 sx += c * zeta[p].x;
                 sy += c * zeta[p].y;
             }
-            out[e] = mk(sx, sy);
+            out[e] = cm<C>(sx, sy);
         }
         __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------------------------
+// the pair tables and the d(pi/2) table of an operator precision
+__device__ __forceinline__ const cplx* stab_of(const DirectArgs& a, cplx*) { return a.pt.stab; }
+__device__ __forceinline__ const cplxf* stab_of(const DirectArgs& a, cplxf*) { return a.pt.stab32; }
+__device__ __forceinline__ const double* delta_of(const DirectArgs& a, cplx*) { return a.delta; }
+__device__ __forceinline__ const float* delta_of(const DirectArgs& a, cplxf*) { return a.delta32; }
+
+template <class C>
 __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBucket bk) {
     extern __shared__ __align__(16) double smem_d[];
     const SceneView& sc = a.sc;
     const int pp = bk.pp;
-    const bool tabs = a.pt.stab != nullptr;
-    const Bufs s = carve(smem_d, pp, tabs);
+    const C* stab = stab_of(a, (C*)nullptr);
+    const bool tabs = stab != nullptr;
+    const Bufs<C> s = carve<C>(smem_d, pp, tabs);
     const int j = bk.targets[blockIdx.x];
     const int c = blockIdx.y;
     if (!sc.couple[j]) return;
@@ -581,16 +625,16 @@ __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBuck
     const int Pj = pj * (pj + 2);
     const int SP = pp * (pp + 3);   // part stride of the folded buffers
     const int XP = pp * (pp + 2);   // part stride of x'
-    const PairCtx ctx{s, a.delta, a.dt, a.g, a.z, pp, SP, XP, tabs};
-    for (int t = tid; t < 2 * Pj; t += kThreads) s.acc[t] = mk(0, 0);
+    const PairCtx<C> ctx{s, delta_of(a, (C*)nullptr), a.dt, a.g, a.z, pp, SP, XP, tabs};
+    for (int t = tid; t < 2 * Pj; t += kThreads) s.acc[t] = C{0, 0};
     for (int t = tid; t < pp * (pp + 3) / 2; t += kThreads) {
         int n, k;
         decode_nk(t, n, k);
         s.nk[t] = make_short2((short)n, (short)k);
     }
 
-    auto block = [&](int l) -> const cplx* {
-        return tabs ? a.pt.stab + a.pt.pair_off[pair_index(min(j, l), max(j, l), sc.n)] : nullptr;
+    auto block = [&](int l) -> const C* {
+        return tabs ? stab + a.pt.pair_off[pair_index(min(j, l), max(j, l), sc.n)] : nullptr;
     };
     auto disp = [&](int l) {
         return Disp{sc.centres + 3 * (size_t)j, sc.centres + 3 * (size_t)l, sc.k, 1.0, {0.0, 0.0, 0.0}};
@@ -617,7 +661,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBuck
         i = inext;
     }
     cplx* out = a.partial + (size_t)(bk.slab + c) * a.n_unk + sc.off[j];
-    for (int t = tid; t < 2 * Pj; t += kThreads) out[t] = s.acc[t];
+    for (int t = tid; t < 2 * Pj; t += kThreads) out[t] = mk(s.acc[t].x, s.acc[t].y);
     // slabs of this source bucket that launches with fewer chunks leave unused
     if (c == bk.chunks - 1)
         for (int e = c + 1; e < a.cmax; ++e) {
@@ -626,13 +670,29 @@ __global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBuck
         }
 }
 
-size_t direct_smem_bytes(int pp, bool tabs) { return smem_bytes(pp, tabs); }
+size_t direct_smem_bytes(int pp, bool tabs, bool fp32) {
+    return fp32 ? smem_bytes<cplxf>(pp, tabs) : smem_bytes<cplx>(pp, tabs);
+}
 
 void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s) {
-    size_t smem = direct_smem_bytes(b.pp, a.pt.stab != nullptr);
     dim3 grid(b.ntargets, b.chunks);
-    raise_smem_ceiling(reinterpret_cast<const void*>(k_direct), smem);
-    k_direct<<<grid, kThreads, smem, s>>>(a, b);
+    if (a.fp32) {
+        size_t smem = direct_smem_bytes(b.pp, a.pt.stab32 != nullptr, true);
+        raise_smem_ceiling(reinterpret_cast<const void*>(k_direct<cplxf>), smem);
+        k_direct<cplxf><<<grid, kThreads, smem, s>>>(a, b);
+    } else {
+        size_t smem = direct_smem_bytes(b.pp, a.pt.stab != nullptr, false);
+        raise_smem_ceiling(reinterpret_cast<const void*>(k_direct<cplx>), smem);
+        k_direct<cplx><<<grid, kThreads, smem, s>>>(a, b);
+    }
+}
+
+void launch_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, void* stab, bool fp32, dim3 grid,
+                   int chunks, cudaStream_t s) {
+    if (fp32)
+        k_pair_s<cplxf><<<grid, 256, 0, s>>>(sc, g, z, pair_off, static_cast<cplxf*>(stab), chunks);
+    else
+        k_pair_s<cplx><<<grid, 256, 0, s>>>(sc, g, z, pair_off, static_cast<cplx*>(stab), chunks);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -642,14 +702,14 @@ void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s) {
 __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     extern __shared__ __align__(16) double smem_d[];
     const int pp = a.pp;
-    const Bufs s = carve(smem_d, pp, false);
+    const Bufs<cplx> s = carve<cplx>(smem_d, pp, false);
     const int t = a.tbase + blockIdx.x;
     const int tid = threadIdx.x;
     const int pj = a.tgt.p[t];
     const int Pj = pj * (pj + 2);
     const int SP = pp * (pp + 3);
     const int XP = pp * (pp + 2);
-    const PairCtx ctx{s, a.delta, a.dt, a.g, a.z, pp, SP, XP, false};
+    const PairCtx<cplx> ctx{s, a.delta, a.dt, a.g, a.z, pp, SP, XP, false};
     cplx* out = a.out + a.tgt.off[t];
     for (int e = tid; e < 2 * Pj; e += kThreads) s.acc[e] = a.add ? out[e] : mk(0, 0);
     for (int e = tid; e < pp * (pp + 3) / 2; e += kThreads) {
@@ -663,16 +723,16 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     };
     if (i0 < i1) {
         const int l = a.lidx[i0];
-        prep_pair(s, disp(l), a.z, nullptr, pj, a.src.p[l], pp, 0, tid, true);
+        prep_pair(s, disp(l), a.z, (const cplx*)nullptr, pj, a.src.p[l], pp, 0, tid, true);
     }
     __syncthreads();
     int cur = 0;
     for (int i = i0; i < i1; ++i) {
         const int l = a.lidx[i];
-        run_pair(ctx, tid, pj, a.src.p[l], a.x + a.src.off[l], nullptr, cur, [&](int tt) {
+        run_pair(ctx, tid, pj, a.src.p[l], a.x + a.src.off[l], (const cplx*)nullptr, cur, [&](int tt) {
             if (i + 1 < i1) {
                 const int ln = a.lidx[i + 1];
-                prep_pair(s, disp(ln), a.z, nullptr, pj, a.src.p[ln], pp, cur ^ 1, tt, true);
+                prep_pair(s, disp(ln), a.z, (const cplx*)nullptr, pj, a.src.p[ln], pp, cur ^ 1, tt, true);
             }
         });
         cur ^= 1;
@@ -682,7 +742,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
 
 void launch_translate(const TransArgs& a, int ntargets, cudaStream_t s) {
     if (ntargets <= 0) return;
-    size_t smem = smem_bytes(a.pp, false);
+    size_t smem = smem_bytes<cplx>(a.pp, false);
     raise_smem_ceiling(reinterpret_cast<const void*>(k_translate), smem);
     k_translate<<<ntargets, kThreads, smem, s>>>(a);
 }

@@ -41,7 +41,7 @@ module foggy_gpu_f
         integer(c_int32_t) :: pair_tables
         integer(c_int32_t) :: fmm_convention
         integer(c_int32_t) :: z_translation_gt_r
-        integer(c_int32_t) :: reserved
+        integer(c_int32_t) :: precision
     end type foggy_params
 
     type, bind(c), public :: foggy_stats
