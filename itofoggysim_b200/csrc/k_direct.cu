@@ -609,8 +609,20 @@ __device__ __forceinline__ const cplxf* stab_of(const DirectArgs& a, cplxf*) { r
 __device__ __forceinline__ const double* delta_of(const DirectArgs& a, cplx*) { return a.delta; }
 __device__ __forceinline__ const float* delta_of(const DirectArgs& a, cplxf*) { return a.delta32; }
 
+// CTAs per SM the register budget is set for: the FP64 operator needs 80 registers a thread
+// (3 CTAs); the FP32 one fits 64 without spills, so 4 CTAs where shared memory allows
+// (orders up to 28)
 template <class C>
-__global__ void __launch_bounds__(kThreads, 3) k_direct(DirectArgs a, DirectBucket bk) {
+struct DirectOcc {
+    static constexpr int ctas = 3;
+};
+template <>
+struct DirectOcc<cplxf> {
+    static constexpr int ctas = 4;
+};
+
+template <class C>
+__global__ void __launch_bounds__(kThreads, DirectOcc<C>::ctas) k_direct(DirectArgs a, DirectBucket bk) {
     extern __shared__ __align__(16) double smem_d[];
     const SceneView& sc = a.sc;
     const int pp = bk.pp;
