@@ -167,6 +167,14 @@ int fail(foggy_handle h, int code, const std::string& msg) {
             return fail(h, FOGGY_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
     } while (0)
 
+// Host to device on the handle's stream, then wait.  The kernels that read dst run on that
+// non-blocking stream, which a blocking cudaMemcpy on the legacy stream does not order (from
+// pageable memory it may return before the DMA lands), and the source is often a temporary.
+static cudaError_t h2d(foggy_handle h, void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(h->stream) : e;
+}
+
 template <class T>
 int dalloc(foggy_handle h, T** p, size_t count) {
     size_t bytes = count * sizeof(T);
@@ -245,12 +253,12 @@ int ensure_tables(foggy_handle h, int pmax) {
         build_axial_tables_qmajor(t, koff, gab);
         TRY(dalloc(h, &h->d_koff, koff.size()));
         TRY(dalloc(h, &h->d_gab, gab.size()));
-        CK(h, cudaMemcpy(h->d_koff, koff.data(), koff.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
-        CK(h, cudaMemcpy(h->d_gab, gab.data(), gab.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(h, h2d(h, h->d_koff, koff.data(), koff.size() * sizeof(int64_t)));
+        CK(h, h2d(h, h->d_gab, gab.data(), gab.size() * sizeof(double)));
     }
-    CK(h, cudaMemcpy(h->d_axoff, t.offset.data(), t.offset.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_ga, t.ga.data(), t.ga.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_gb, t.gb.data(), t.gb.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, h2d(h, h->d_axoff, t.offset.data(), t.offset.size() * sizeof(int32_t)));
+    CK(h, h2d(h, h->d_ga, t.ga.data(), t.ga.size() * sizeof(double)));
+    CK(h, h2d(h, h->d_gb, t.gb.data(), t.gb.size() * sizeof(double)));
     int K = pmax + 1;   // the scalar-coefficient relation reads sqrt((nu+1)^2 - k^2) at nu = pmax
     {
         std::vector<int64_t> koff;
@@ -260,8 +268,8 @@ int ensure_tables(foggy_handle h, int pmax) {
         dfree(h, h->d_gs);
         TRY(dalloc(h, &h->d_koffS, koff.size()));
         TRY(dalloc(h, &h->d_gs, gs.size()));
-        CK(h, cudaMemcpy(h->d_koffS, koff.data(), koff.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
-        CK(h, cudaMemcpy(h->d_gs, gs.data(), gs.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(h, h2d(h, h->d_koffS, koff.data(), koff.size() * sizeof(int64_t)));
+        CK(h, h2d(h, h->d_gs, gs.data(), gs.size() * sizeof(double)));
         h->gs_nm = pmax + 1;
     }
     std::vector<double> sb((size_t)(K + 1) * (2 * K + 1), 0.0), rs((size_t)(K + 1) * (K + 1), 0.0);
@@ -287,23 +295,23 @@ int ensure_tables(foggy_handle h, int pmax) {
     TRY(dalloc(h, &h->d_rs, rs.size()));
     TRY(dalloc(h, &h->d_irs, irs.size()));
     TRY(dalloc(h, &h->d_rj, rj.size()));
-    CK(h, cudaMemcpy(h->d_sqrt_binom, sb.data(), sb.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_rs, rs.data(), rs.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_irs, irs.data(), irs.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_rj, rj.data(), rj.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, h2d(h, h->d_sqrt_binom, sb.data(), sb.size() * sizeof(double)));
+    CK(h, h2d(h, h->d_rs, rs.data(), rs.size() * sizeof(double)));
+    CK(h, h2d(h, h->d_irs, irs.data(), irs.size() * sizeof(double)));
+    CK(h, h2d(h, h->d_rj, rj.data(), rj.size() * sizeof(double)));
     {
         std::vector<double> dl;
         build_delta_table(pmax, dl);
         TRY(dalloc(h, &h->d_delta, dl.size()));
-        CK(h, cudaMemcpy(h->d_delta, dl.data(), dl.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(h, h2d(h, h->d_delta, dl.data(), dl.size() * sizeof(double)));
         std::vector<float> dl32(dl.begin(), dl.end());
         TRY(dalloc(h, &h->d_delta32, dl32.size()));
-        CK(h, cudaMemcpy(h->d_delta32, dl32.data(), dl32.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(h, h2d(h, h->d_delta32, dl32.data(), dl32.size() * sizeof(float)));
     }
     std::vector<double> g;
     build_g_table(pmax, g);
     TRY(dalloc(h, &h->d_g, g.size()));
-    CK(h, cudaMemcpy(h->d_g, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h, h2d(h, h->d_g, g.data(), g.size() * sizeof(double)));
     h->K = K;
     h->tab_pmax = pmax;
     return FOGGY_OK;
@@ -374,7 +382,7 @@ int plan_direct(foggy_handle h) {
     }
     dfree(h, h->d_bucket_lists);
     TRY(dalloc(h, &h->d_bucket_lists, flat.size()));
-    CK(h, cudaMemcpy(h->d_bucket_lists, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h, h2d(h, h->d_bucket_lists, flat.data(), flat.size() * sizeof(int)));
     h->launches_direct.clear();
     for (int t = 0; t < h->nbuckets; ++t)
         for (int s = 0; s < h->nbuckets; ++s) {
@@ -596,10 +604,10 @@ int ensure_fmm(foggy_handle h) {
     TRY(dalloc(h, &h->d_fmm_C, (size_t)nbox * 2 * Pg));
     TRY(dalloc(h, &h->d_fmm_D, (size_t)nbox * 2 * Pg));
     TRY(dalloc(h, &h->d_fmm_slab, 2 * (size_t)h->n_unk));
-    CK(h, cudaMemcpy(h->d_fmm_list, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_fmm_c, bc.data(), bc.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_fmm_p, bp.data(), bp.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_fmm_off, bo.data(), bo.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+    CK(h, h2d(h, h->d_fmm_list, all.data(), all.size() * sizeof(int)));
+    CK(h, h2d(h, h->d_fmm_c, bc.data(), bc.size() * sizeof(double)));
+    CK(h, h2d(h, h->d_fmm_p, bp.data(), bp.size() * sizeof(int)));
+    CK(h, h2d(h, h->d_fmm_off, bo.data(), bo.size() * sizeof(int64_t)));
     h->fmm_ready = true;
     return FOGGY_OK;
 }
@@ -1043,14 +1051,10 @@ int32_t foggy_set_params(foggy_handle h, const foggy_params* params) {
     return FOGGY_OK;
 }
 
-int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centres, const int32_t* param_index,
+// The scene of foggy_set_spheres on a handle whose previous scene is freed; the input is checked.
+static int32_t load_scene(foggy_handle h, int32_t n_spheres, const double* centres, const int32_t* param_index,
                           int32_t n_param, const double* refractive_index, const double* radius,
                           const int32_t* n_range) {
-    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
-    if (n_spheres < 1 || n_param < 1 || !centres || !param_index || !refractive_index || !radius || !n_range)
-        return fail(h, FOGGY_ERR_ARGUMENT, "empty or NULL sphere input");
-    CK(h, cudaSetDevice(h->device));
-    free_scene(h);
     const int pg = h->prm.n_range[1];
     h->N = n_spheres;
     h->NP = n_param;
@@ -1065,9 +1069,6 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
     for (int i = 0; i < n_param; ++i) {
         h->mre[i] = refractive_index[2 * i] / h->prm.n_medium;
         h->mim[i] = refractive_index[2 * i + 1] / h->prm.n_medium;
-        if (n_range[2 * i] != 1 || n_range[2 * i + 1] < 1)
-            return fail(h, FOGGY_ERR_ARGUMENT, "parameter n_range must be [1, n_max], n_max >= 1");
-        if (!(radius[i] > 0)) return fail(h, FOGGY_ERR_ARGUMENT, "radius must be > 0");
         h->p_param[i] = std::min(n_range[2 * i + 1], pg);
     }
     h->p_s.resize(n_spheres);
@@ -1077,9 +1078,6 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
     int64_t o = 0;
     for (int j = 0; j < n_spheres; ++j) {
         int ip = param_index[j];
-        if (ip < 0 || ip >= n_param) return fail(h, FOGGY_ERR_ARGUMENT, "param_index out of range");
-        for (int d = 0; d < 3; ++d)
-            if (!std::isfinite(centres[3 * (size_t)j + d])) return fail(h, FOGGY_ERR_ARGUMENT, "non-finite centre");
         int p = h->p_param[ip];
         h->p_s[j] = p;
         h->pmax = std::max(h->pmax, p);
@@ -1091,8 +1089,6 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
     }
     h->off[n_spheres] = o;
     h->n_unk = o;
-    if (h->pmax > 32)
-        return fail(h, FOGGY_ERR_UNSUPPORTED, "the direct operator supports truncation orders up to 32");
     TRY(ensure_tables(h, std::max(h->pmax, 1)));
     // device scene
     TRY(dalloc(h, &h->d_centres, 3 * (size_t)n_spheres));
@@ -1109,10 +1105,10 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
     TRY(dalloc(h, &h->d_tmp_out, h->n_unk));
     TRY(plan_direct(h));
     TRY(dalloc(h, &h->d_partial, (size_t)h->nbuckets * h->cmax * h->n_unk));
-    CK(h, cudaMemcpy(h->d_centres, centres, 3 * (size_t)n_spheres * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_p, h->p_s.data(), n_spheres * sizeof(int), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_off, h->off.data(), (n_spheres + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->d_couple, h->couple.data(), n_spheres * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h, h2d(h, h->d_centres, centres, 3 * (size_t)n_spheres * sizeof(double)));
+    CK(h, h2d(h, h->d_p, h->p_s.data(), n_spheres * sizeof(int)));
+    CK(h, h2d(h, h->d_off, h->off.data(), (n_spheres + 1) * sizeof(int64_t)));
+    CK(h, h2d(h, h->d_couple, h->couple.data(), n_spheres * sizeof(int)));
     // Mie coefficients per parameter (FP64, device) then gathered per sphere
     std::vector<double> xs(n_param);
     for (int i = 0; i < n_param; ++i) xs[i] = 2.0 * kPi * h->prm.n_medium * radius[i] / h->prm.lambda_0;
@@ -1124,11 +1120,11 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
     CK(h, cudaMalloc(&d_mi, n_param * sizeof(double)));
     CK(h, cudaMalloc(&d_pp, n_param * sizeof(int)));
     CK(h, cudaMalloc(&d_pidx, n_spheres * sizeof(int)));
-    CK(h, cudaMemcpy(d_x, xs.data(), n_param * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(d_mr, h->mre.data(), n_param * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(d_mi, h->mim.data(), n_param * sizeof(double), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(d_pp, h->p_param.data(), n_param * sizeof(int), cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(d_pidx, param_index, n_spheres * sizeof(int), cudaMemcpyHostToDevice));
+    CK(h, h2d(h, d_x, xs.data(), n_param * sizeof(double)));
+    CK(h, h2d(h, d_mr, h->mre.data(), n_param * sizeof(double)));
+    CK(h, h2d(h, d_mi, h->mim.data(), n_param * sizeof(double)));
+    CK(h, h2d(h, d_pp, h->p_param.data(), n_param * sizeof(int)));
+    CK(h, h2d(h, d_pidx, param_index, n_spheres * sizeof(int)));
     k_mie_ab<<<(n_param + 63) / 64, 64, 0, h->stream>>>(n_param, d_x, d_mr, d_mi, d_pp, h->pmax, h->d_an_p, h->d_bn_p);
     k_gather_an<<<n_spheres, 64, 0, h->stream>>>(n_spheres, d_pidx, h->pmax, h->d_an_p, h->d_bn_p, h->d_an, h->d_bn);
     cudaError_t e = cudaStreamSynchronize(h->stream);
@@ -1141,6 +1137,45 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
     CKL(h);
     h->rhs_ready = false;
     return FOGGY_OK;
+}
+
+int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centres, const int32_t* param_index,
+                          int32_t n_param, const double* refractive_index, const double* radius,
+                          const int32_t* n_range) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (n_spheres < 1 || n_param < 1 || !centres || !param_index || !refractive_index || !radius || !n_range)
+        return fail(h, FOGGY_ERR_ARGUMENT, "empty or NULL sphere input");
+    // all of the input is checked before the handle's scene is touched, so a refused call leaves
+    // the previous scene in place
+    const int pg = h->prm.n_range[1];
+    for (int i = 0; i < n_param; ++i) {
+        if (n_range[2 * i] != 1 || n_range[2 * i + 1] < 1)
+            return fail(h, FOGGY_ERR_ARGUMENT, "parameter n_range must be [1, n_max], n_max >= 1");
+        if (!(radius[i] > 0) || !std::isfinite(radius[i]))
+            return fail(h, FOGGY_ERR_ARGUMENT, "radius must be finite and > 0");
+        if (!std::isfinite(refractive_index[2 * i]) || !std::isfinite(refractive_index[2 * i + 1]))
+            return fail(h, FOGGY_ERR_ARGUMENT, "non-finite refractive index");
+    }
+    int pmax = 0;
+    for (int j = 0; j < n_spheres; ++j) {
+        const int ip = param_index[j];
+        if (ip < 0 || ip >= n_param) return fail(h, FOGGY_ERR_ARGUMENT, "param_index out of range");
+        for (int d = 0; d < 3; ++d)
+            if (!std::isfinite(centres[3 * (size_t)j + d])) return fail(h, FOGGY_ERR_ARGUMENT, "non-finite centre");
+        pmax = std::max(pmax, std::min(n_range[2 * ip + 1], pg));
+    }
+    if (pmax > 32) return fail(h, FOGGY_ERR_UNSUPPORTED, "the direct operator supports truncation orders up to 32");
+    CK(h, cudaSetDevice(h->device));
+    free_scene(h);
+    const int32_t rc = load_scene(h, n_spheres, centres, param_index, n_param, refractive_index, radius, n_range);
+    if (rc != FOGGY_OK) {
+        // a device failure part way: no scene rather than a partial one
+        free_scene(h);
+        h->N = 0;
+        h->NP = 0;
+        h->n_unk = 0;
+    }
+    return rc;
 }
 
 int32_t foggy_set_plane_waves(foggy_handle h, int32_t nw, const double* theta, const double* phi,
@@ -1578,23 +1613,20 @@ int32_t foggy_translation_coefficients(double x, double theta, double phi, const
     AxialView ax{h->tab_pmax, h->d_axoff, h->d_ga, h->d_gb, h->d_koff, reinterpret_cast<const double2*>(h->d_gab)};
     int Pn = pn * (pn + 2), Pnu = pnu * (pnu + 2);
     cplx *dA = nullptr, *dB = nullptr;
-    cudaMalloc(&dA, (size_t)Pn * Pnu * sizeof(cplx));
-    cudaMalloc(&dB, (size_t)Pn * Pnu * sizeof(cplx));
-    size_t smem = translation_pair_smem_bytes(pmax);
-    raise_smem_ceiling(reinterpret_cast<const void*>(k_translation_pair), smem);
-    k_translation_pair<<<1, 256, smem, h->stream>>>(ax, dtabs(h), x, theta, phi, pn, pnu, z_selector, dA, dB);
     std::vector<cplx> hA((size_t)Pn * Pnu), hB((size_t)Pn * Pnu);
-    cudaError_t e = cudaMemcpyAsync(hA.data(), dA, hA.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = cudaMalloc(&dA, hA.size() * sizeof(cplx));
+    if (e == cudaSuccess) e = cudaMalloc(&dB, hB.size() * sizeof(cplx));
+    if (e == cudaSuccess) {
+        size_t smem = translation_pair_smem_bytes(pmax);
+        raise_smem_ceiling(reinterpret_cast<const void*>(k_translation_pair), smem);
+        k_translation_pair<<<1, 256, smem, h->stream>>>(ax, dtabs(h), x, theta, phi, pn, pnu, z_selector, dA, dB);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hA.data(), dA, hA.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hB.data(), dB, hB.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     cudaFree(dA);
     cudaFree(dB);
-    {
-        std::vector<double> dl;
-        build_delta_table(pmax, dl);
-        TRY(dalloc(h, &h->d_delta, dl.size()));
-        CK(h, cudaMemcpy(h->d_delta, dl.data(), dl.size() * sizeof(double), cudaMemcpyHostToDevice));
-    }
     std::vector<double> g;
     build_g_table(pmax, g);
     foggy_destroy(h);

@@ -263,6 +263,30 @@ def test_argument_errors(native):
     assert e.value.code == _native.FOGGY_ERR_ARGUMENT
 
 
+def test_refused_scene_keeps_previous(native):
+    """A foggy_set_spheres call refused for its input leaves the handle's scene as it was."""
+    import ctypes as C
+    sc = S.random_cluster(3, seed=2, p=3)
+    with solver.MultiSphereSolver(sc) as s:
+        b0 = s.get_vector_b()
+        x0, _ = s.solve()
+        c, pi, m, r, nr = s._keep
+        bad = [np.array([0, 5, 0], np.int32), np.array([0, -1, 0], np.int32)]
+        for pidx in bad:
+            rc = s.L.foggy_set_spheres(s.h, sc.n_spheres, _native.ptr(c), _native.ptr(pidx, C.c_int32), sc.n_param,
+                                       _native.ptr(m), _native.ptr(r), _native.ptr(nr, C.c_int32))
+            assert rc == _native.FOGGY_ERR_ARGUMENT
+        cen = c.copy()
+        cen[4] = np.inf
+        rc = s.L.foggy_set_spheres(s.h, sc.n_spheres, _native.ptr(cen), _native.ptr(pi, C.c_int32), sc.n_param,
+                                   _native.ptr(m), _native.ptr(r), _native.ptr(nr, C.c_int32))
+        assert rc == _native.FOGGY_ERR_ARGUMENT
+        assert s.L.foggy_vector_length(s.h) == sc.vector_length()
+        assert np.array_equal(s.get_vector_b(), b0)
+        x1, st = s.solve()
+        assert st["status"] == 0 and np.array_equal(x1, x0)
+
+
 def test_memory_budget_admission(native):
     sc = S.random_cluster(6, seed=2, p=6)
     with pytest.raises(_native.FoggyError) as e:
