@@ -122,7 +122,8 @@ int32_t foggy_create(const foggy_params* params, int32_t device, foggy_handle* o
 /* Replaces lib_mie_ms_solver_destructor (lib_mie_ms_solver_interface.f90:131-141). */
 int32_t foggy_destroy(foggy_handle h);
 
-/* Message of the last failing call on this handle (or of the last failing foggy_create). */
+/* Message of the last failing call on this handle; with h = NULL, of the calling thread's last
+ * failing foggy_create or handle-less call. */
 const char* foggy_last_error(foggy_handle h);
 
 /* Replaces lib_mie_ms_solver_set_n_range / _set_max_iterations / _use_ml_fmm

@@ -19,8 +19,9 @@ using namespace foggy;
 
 namespace {
 const double kPi = 3.14159265358979323846264338327950288;
-std::mutex g_err_mu;
-std::string g_err;   // error of a failing foggy_create / handle-less call
+// error of the calling thread's last failing foggy_create / handle-less call (per thread, as
+// errno, so that threads creating handles side by side read their own message)
+thread_local std::string g_err;
 
 struct DevBuf {
     void* p = nullptr;
@@ -147,7 +148,6 @@ int fail(foggy_handle h, int code, const std::string& msg) {
     if (h) {
         h->err = msg;
     } else {
-        std::lock_guard<std::mutex> lk(g_err_mu);
         g_err = msg;
     }
     return code;
@@ -1018,7 +1018,6 @@ int32_t foggy_destroy(foggy_handle h) {
 
 const char* foggy_last_error(foggy_handle h) {
     if (h) return h->err.c_str();
-    std::lock_guard<std::mutex> lk(g_err_mu);
     return g_err.c_str();
 }
 

@@ -103,6 +103,39 @@ def test_argument_errors_are_reported(native):
     assert native.foggy_create(C.byref(p), 0, C.byref(h)) == _native.FOGGY_ERR_ARGUMENT
 
 
+def test_handle_less_errors_are_per_thread(native):
+    """Threads whose foggy_create calls fail side by side each read their own message."""
+    import threading
+    from itofoggysim_b200 import _native
+
+    def bad_params(kind):
+        p = _native.FoggyParams()
+        native.foggy_default_params(C.byref(p))
+        if kind == 0:
+            p.n_range[1] = 99
+        else:
+            p.lambda_0 = -1.0
+        return p
+
+    expect = [b"n_range", b"lambda_0"]
+    wrong = []
+
+    def run(kind):
+        p = bad_params(kind)
+        h = C.c_void_p()
+        for _ in range(2000):
+            native.foggy_create(C.byref(p), 0, C.byref(h))
+            if expect[kind] not in native.foggy_last_error(None):
+                wrong.append(kind)
+
+    ts = [threading.Thread(target=run, args=(k % 2,)) for k in range(4)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert wrong == []
+
+
 def test_fortran_module_binds_every_header_symbol():
     """The iso_c_binding module declares a bind(c) interface for every entry point of the header."""
     with open(os.path.join(ROOT, "itofoggysim_b200", "fortran", "foggy_gpu_f.f90")) as f:
