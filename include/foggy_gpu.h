@@ -361,6 +361,7 @@ typedef struct foggy_request_info {
 int32_t foggy_server_start(int32_t device, int32_t max_concurrent, int64_t memory_budget, foggy_server* out);
 int32_t foggy_server_submit(foggy_server s, const foggy_request* request, int64_t* id);
 /* State of a request; wait_ms > 0 waits up to that long for it to finish, < 0 without limit.
+ * status, nrhs, x_len, stats and error are filled once the request has finished (zero before).
  * When it is done, copies the solutions into x (x_len doubles at least; NULL to skip) and the
  * cross-sections into cross_sections (3 nrhs doubles; NULL to skip). */
 int32_t foggy_server_poll(foggy_server s, int64_t id, int32_t wait_ms, foggy_request_info* info, double* x,

@@ -238,14 +238,17 @@ int32_t foggy_server_poll(foggy_server S, int64_t id, int32_t wait_ms, foggy_req
     }
     std::memset(info, 0, sizeof(*info));
     info->state = r->state;
-    info->status = r->status;
-    info->nrhs = r->nrhs;
-    info->x_len = (int64_t)r->x.size();
     info->footprint = r->footprint;
     const double t_now = now_ms();
     info->ms_queued = ((r->t_start > 0) ? r->t_start : (terminal(r->state) ? r->t_end : t_now)) - r->t_submit;
     info->ms_solve = (r->t_start > 0) ? ((r->t_end > 0 ? r->t_end : t_now) - r->t_start) : 0.0;
     info->ms_latency = (terminal(r->state) ? r->t_end : t_now) - r->t_submit;
+    // the worker writes the results without the lock while the request runs and publishes them
+    // by setting a terminal state under it, so they are read only from then on
+    if (!terminal(r->state)) return FOGGY_OK;
+    info->status = r->status;
+    info->nrhs = r->nrhs;
+    info->x_len = (int64_t)r->x.size();
     info->stats = r->stats;
     std::strncpy(info->error, r->error.c_str(), sizeof(info->error) - 1);
     if (r->state == FOGGY_REQ_DONE) {
