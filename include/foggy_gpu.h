@@ -235,6 +235,21 @@ int32_t foggy_build_tree(foggy_handle h, int64_t* uindex_out, int32_t* order_out
  * points[3*n] host memory, out[n]. */
 int32_t foggy_universal_index(int32_t n, const double* points, int32_t l, int64_t* out);
 
+/* libtree box arithmetic on universal indices (box n at level l, 0 <= n < 8^l, l = 0..21), on the
+ * host: no handle, no GPU.
+ * foggy_tree_parent: the box `step` levels up (1 <= step <= l), n >> 3 step
+ *   (lib_tree_get_parent, libtree/src/lib/lib_tree.f90:405-431).
+ * foggy_tree_children: the eight boxes 8 n + j, j = 0..7, at level l + 1 (l < 21)
+ *   (lib_tree_get_children, lib_tree.f90:444-453).
+ * foggy_tree_centre_of_box: centre[3] = 2^-l (c + 1/2) in the normalised cube [0,1)^3, c the
+ *   de-interleaved box coordinates (lib_tree_get_centre_of_box, lib_tree.f90:1292-1300).
+ * foggy_tree_neighbours: the boxes at distance 1 inside the domain, ascending, out[26] at most
+ *   (lib_tree_hf_get_neighbour_all_xD with k = 1, lib_tree_helper_functions.f90:914-997). */
+int32_t foggy_tree_parent(int64_t n, int32_t l, int32_t step, int64_t* parent);
+int32_t foggy_tree_children(int64_t n, int32_t l, int64_t* children);
+int32_t foggy_tree_centre_of_box(int64_t n, int32_t l, double* centre);
+int32_t foggy_tree_neighbours(int64_t n, int32_t l, int64_t* out, int32_t* count);
+
 /* Number of boxes at tree level l and their universal indices in ascending order
  * (lib_ml_fmm_hf_create_hierarchy, libmlfmm/src/lib/lib_ml_fmm_helper_functions.f90:366-457).
  * Call with boxes == NULL to query the count. */

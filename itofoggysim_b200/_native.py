@@ -37,7 +37,8 @@ EXPORTS = [
     "foggy_universal_index", "foggy_tree_boxes", "foggy_matvec_static", "foggy_tree_domain",
     "foggy_get_field", "foggy_set_gaussian_beams", "foggy_solve_rhs", "foggy_server_start",
     "foggy_server_submit", "foggy_server_poll", "foggy_server_cancel", "foggy_server_release",
-    "foggy_server_stop", "foggy_matvec_rhs",
+    "foggy_server_stop", "foggy_matvec_rhs", "foggy_tree_parent", "foggy_tree_children",
+    "foggy_tree_centre_of_box", "foggy_tree_neighbours",
 ]
 
 
@@ -175,6 +176,10 @@ def load():
         "foggy_server_release": (i32, [vp, i64]),
         "foggy_server_stop": (i32, [vp]),
         "foggy_matvec_rhs": (i32, [vp, i32, vp, vp, i32]),
+        "foggy_tree_parent": (i32, [i64, i32, i32, pi64]),
+        "foggy_tree_children": (i32, [i64, i32, pi64]),
+        "foggy_tree_centre_of_box": (i32, [i64, i32, pd]),
+        "foggy_tree_neighbours": (i32, [i64, i32, pi64, pi32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1692,6 +1692,49 @@ int32_t foggy_universal_index(int32_t n, const double* points, int32_t l, int64_
     return FOGGY_OK;
 }
 
+// ---- libtree box arithmetic: integer work on universal indices, on the host ------------------
+static int check_box(int64_t n, int32_t l) {
+    if (l < 0 || l > 21) return fail(nullptr, FOGGY_ERR_ARGUMENT, "level must be 0..21");
+    // every non-negative int64 is a level-21 box (8^21 = 2^63)
+    if (n < 0 || (l < 21 && n >= ((int64_t)1 << (3 * l))))
+        return fail(nullptr, FOGGY_ERR_ARGUMENT, "box index outside 0..8^l - 1");
+    return FOGGY_OK;
+}
+
+int32_t foggy_tree_parent(int64_t n, int32_t l, int32_t step, int64_t* parent) {
+    if (!parent) return fail(nullptr, FOGGY_ERR_ARGUMENT, "parent is NULL");
+    TRY(check_box(n, l));
+    if (step < 1 || step > l) return fail(nullptr, FOGGY_ERR_ARGUMENT, "step must be 1..l");
+    *parent = n >> (3 * step);
+    return FOGGY_OK;
+}
+
+int32_t foggy_tree_children(int64_t n, int32_t l, int64_t* children) {
+    if (!children) return fail(nullptr, FOGGY_ERR_ARGUMENT, "children is NULL");
+    TRY(check_box(n, l));
+    if (l == 21) return fail(nullptr, FOGGY_ERR_ARGUMENT, "level 21 boxes have no children");
+    for (int j = 0; j < 8; ++j) children[j] = (n << 3) + j;
+    return FOGGY_OK;
+}
+
+int32_t foggy_tree_centre_of_box(int64_t n, int32_t l, double* centre) {
+    if (!centre) return fail(nullptr, FOGGY_ERR_ARGUMENT, "centre is NULL");
+    TRY(check_box(n, l));
+    box_centre(n, l, centre);
+    return FOGGY_OK;
+}
+
+int32_t foggy_tree_neighbours(int64_t n, int32_t l, int64_t* out, int32_t* count) {
+    if (!out || !count) return fail(nullptr, FOGGY_ERR_ARGUMENT, "out or count is NULL");
+    TRY(check_box(n, l));
+    std::vector<int64_t> nb;
+    tree_i2(n, l, nb);   // own box first, then the neighbours inside the domain
+    std::sort(nb.begin() + 1, nb.end());
+    *count = (int32_t)nb.size() - 1;
+    std::copy(nb.begin() + 1, nb.end(), out);
+    return FOGGY_OK;
+}
+
 int32_t foggy_tree_boxes(foggy_handle h, int32_t l, int64_t* boxes, int32_t* count) {
     if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
     if (!count) return fail(h, FOGGY_ERR_ARGUMENT, "count is NULL");

@@ -196,6 +196,35 @@ module foggy_gpu_f
             integer(c_int64_t), intent(out) :: out(*)
             integer(c_int32_t) :: rc
         end function
+        function foggy_tree_parent(n, l, step, parent) result(rc) bind(c, name="foggy_tree_parent")
+            import :: c_int32_t, c_int64_t
+            integer(c_int64_t), value :: n
+            integer(c_int32_t), value :: l, step
+            integer(c_int64_t), intent(out) :: parent
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_tree_children(n, l, children) result(rc) bind(c, name="foggy_tree_children")
+            import :: c_int32_t, c_int64_t
+            integer(c_int64_t), value :: n
+            integer(c_int32_t), value :: l
+            integer(c_int64_t), intent(out) :: children(8)
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_tree_centre_of_box(n, l, centre) result(rc) bind(c, name="foggy_tree_centre_of_box")
+            import :: c_int32_t, c_int64_t, c_double
+            integer(c_int64_t), value :: n
+            integer(c_int32_t), value :: l
+            real(c_double), intent(out) :: centre(3)
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_tree_neighbours(n, l, out, count) result(rc) bind(c, name="foggy_tree_neighbours")
+            import :: c_int32_t, c_int64_t
+            integer(c_int64_t), value :: n
+            integer(c_int32_t), value :: l
+            integer(c_int64_t), intent(out) :: out(26)
+            integer(c_int32_t), intent(out) :: count
+            integer(c_int32_t) :: rc
+        end function
         function foggy_tree_boxes(h, l, boxes, count) result(rc) bind(c, name="foggy_tree_boxes")
             import :: c_ptr, c_int32_t, c_int64_t
             type(c_ptr), value :: h
@@ -301,6 +330,7 @@ module foggy_gpu_f
     public :: foggy_tree_domain, foggy_get_field, foggy_matvec_static, foggy_set_gaussian_beams
     public :: foggy_solve_rhs, foggy_server_start, foggy_server_submit, foggy_server_poll
     public :: foggy_server_cancel, foggy_server_release, foggy_server_stop, foggy_matvec_rhs
+    public :: foggy_tree_parent, foggy_tree_children, foggy_tree_centre_of_box, foggy_tree_neighbours
     public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
     public :: foggy_ms_get_backward_error, foggy_ms_destructor
 

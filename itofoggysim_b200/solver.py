@@ -354,6 +354,37 @@ def universal_index(points, level):
     return out
 
 
+def tree_parent(n, level, step=1):
+    """lib_tree_get_parent (libtree/src/lib/lib_tree.f90:405-431): the box `step` levels above box
+    n of the given level."""
+    out = C.c_int64()
+    N.check(N.load().foggy_tree_parent(int(n), int(level), int(step), C.byref(out)))
+    return out.value
+
+
+def tree_children(n, level):
+    """lib_tree_get_children (lib_tree.f90:444-453): the eight boxes of level + 1 inside box n."""
+    out = np.zeros(8, np.int64)
+    N.check(N.load().foggy_tree_children(int(n), int(level), N.ptr(out, C.c_int64)))
+    return out
+
+
+def tree_centre_of_box(n, level):
+    """lib_tree_get_centre_of_box (lib_tree.f90:1292-1300): centre of box n in the normalised cube."""
+    out = np.zeros(3)
+    N.check(N.load().foggy_tree_centre_of_box(int(n), int(level), N.ptr(out)))
+    return out
+
+
+def tree_neighbours(n, level):
+    """lib_tree_hf_get_neighbour_all_xD with k = 1 (libtree/src/lib/lib_tree_helper_functions.f90:914-997):
+    the boxes at distance 1 inside the domain, ascending."""
+    out = np.zeros(26, np.int64)
+    cnt = C.c_int32()
+    N.check(N.load().foggy_tree_neighbours(int(n), int(level), N.ptr(out, C.c_int64), C.byref(cnt)))
+    return out[:cnt.value]
+
+
 def continuation_stages(run, n_org, n_start=None, step_size=None, dynamic=False):
     """The stage sequence of lib_mie_ms_calculate_scattering_coefficients_ab_nm
     (FoggySim/src/lib/mie_theory/lib_mie_multi_sphere.f90:162-371) over run(n_max, max_iterations)
