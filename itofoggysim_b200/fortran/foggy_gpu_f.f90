@@ -332,7 +332,7 @@ module foggy_gpu_f
     public :: foggy_server_cancel, foggy_server_release, foggy_server_stop, foggy_matvec_rhs
     public :: foggy_tree_parent, foggy_tree_children, foggy_tree_centre_of_box, foggy_tree_neighbours
     public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
-    public :: foggy_ms_get_backward_error, foggy_ms_destructor
+    public :: foggy_ms_get_backward_error, foggy_ms_destructor, foggy_ms_vector_length
 
     type(c_ptr), save :: m_handle = c_null_ptr
 
@@ -378,6 +378,12 @@ module foggy_gpu_f
         function foggy_ms_get_backward_error() result(e)
             real(c_double) :: e
             e = foggy_get_backward_error(m_handle)
+        end function
+
+        ! entries of a solution vector of the current scene, in the reference's flat layout
+        function foggy_ms_vector_length() result(n)
+            integer(c_int64_t) :: n
+            n = foggy_vector_length(m_handle)
         end function
 
         subroutine foggy_ms_destructor()
