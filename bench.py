@@ -346,7 +346,7 @@ def run_serving(args):
         "metric": METRIC, "value": co["solves_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": co["makespan_s"] * 1e3 / max(1, args.steps),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "serving stream (config 5, sphere counts scaled to 50-500)", "requests": args.steps,
+        "config": {"workload": "serving stream: 50-500 lognormal spheres per request, 1-16 right-hand sides", "requests": args.steps,
                    "arrivals": "Poisson, 50 per s", "spheres": [int(min(r.n_spheres for r in timed)),
                                                                  int(max(r.n_spheres for r in timed))],
                    "rhs_total": co["rhs"], "gmres_tolerance": 1e-6, "concurrent": args.concurrent,
@@ -392,8 +392,8 @@ def run_multi_rhs(args):
         "metric": METRIC, "value": nrhs * args.steps / (tot_ms * 1e-3), "unit": "rhs solves/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "64-sphere cluster x 128 right-hand sides (config 4 scaled: 64 Fibonacci "
-                               "directions x TM/TE)", "rhs": nrhs, "gmres_tolerance": 1e-6,
+        "config": {"workload": "64-sphere cluster x 128 right-hand sides (64 Fibonacci directions "
+                               "x TM/TE)", "rhs": nrhs, "gmres_tolerance": 1e-6,
                    "solver": "one GMRES per right-hand side on a shared operator and pair tables"},
         "iterations_per_rhs": iters / (args.steps * nrhs),
         "c_ext_range": [float(cs[:, 1].min()), float(cs[:, 1].max())],
@@ -403,7 +403,7 @@ def run_multi_rhs(args):
 
 def run_mixed(args):
     """The workload solved with the FP32 operator in the Arnoldi steps and FP64 true residuals
-    (SURVEY config 3 on config 2's scene); value = solves/s (device time), with the relative error
+    (the 2000-sphere lognormal scene); value = solves/s (device time), with the relative error
     of the coefficients and of C_ext against one FP64 solve of the same scene.  The roofline is
     that of the FP32 operator: its mean application time is the operator time of a solve less its
     FP64 residual applications (timed in the FP64 solve), over its Arnoldi steps."""
@@ -452,7 +452,7 @@ def run_mixed(args):
         "metric": METRIC, "value": 1e3 / float(np.mean(ms)), "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": float(np.mean(ms)), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 translations, f64 residuals", "data": "synthetic",
-        "config": {"workload": sc.name + " mixed precision (config 3)", "gmres_restart": sc.gmres_restart,
+        "config": {"workload": sc.name + " mixed precision", "gmres_restart": sc.gmres_restart,
                    "gmres_tolerance": sc.gmres_tolerance,
                    "l2": "Krylov basis exceeds L2; 256 MB L2 flush between steps"},
         "fp64": {"ms_per_solve": st64["ms_total"], "iterations": st64["iterations"],
