@@ -911,7 +911,6 @@ int gmres(foggy_handle h, foggy_stats* st) {
         TRY(matvec(h->d_x, h->d_w, false));
         k_sub<<<G, 256, 0, h->stream>>>(h->d_b, h->d_w, h->d_r, n);
         h->launches += 1;
-    h->launches += 1;
         TRY(norm_dev(h, h->d_r, d_beta));
         CK(h, cudaMemcpyAsync(h->h_pin, h->d_scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CK(h, cudaStreamSynchronize(h->stream));
