@@ -18,11 +18,12 @@ class SolveServer:
         self.h = h
         self._keep = {}
 
-    def submit(self, scene, rhs_per_wave=False, init_with_single_sphere=False, pair_tables=0):
+    def submit(self, scene, rhs_per_wave=False, init_with_single_sphere=False, pair_tables=0, precision=0):
         """Queue one solve of scene (its plane waves summed into one right-hand side, or one
-        right-hand side per wave); returns the request id."""
+        right-hand side per wave); precision 1 solves it in mixed precision (FP32 Arnoldi steps,
+        FP64 residuals).  Returns the request id."""
         s = scene
-        prm = _params(s, False, init_with_single_sphere, 0, pair_tables)
+        prm = _params(s, False, init_with_single_sphere, 0, pair_tables, precision=precision)
         arrs = dict(params=prm, centres=N.as_f64(s.centres).reshape(-1), pidx=N.as_i32(s.param_index),
                     m=N.as_c128(s.refractive_index), r=N.as_f64(s.radius),
                     nr=N.as_i32(s.n_range_param).reshape(-1), th=N.as_f64(s.wave_theta), ph=N.as_f64(s.wave_phi),

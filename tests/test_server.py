@@ -31,6 +31,16 @@ def test_failed_without_device(native):
             assert info["ms_latency"] >= 0
 
 
+def test_request_params_reach_the_handle(native):
+    """A request's precision is checked by the handle it runs on: an invalid value fails the
+    request with the handle's argument error (raised before any device is needed)."""
+    with SolveServer(max_concurrent=2, memory_budget=8 << 30) as srv:
+        rid = srv.submit(S.random_cluster(3, seed=1, p=3), precision=7)
+        info, x, _ = srv.wait(rid)
+        assert info["state"] == N.REQ_FAILED and info["status"] == N.FOGGY_ERR_ARGUMENT and x is None
+        assert "precision" in info["error"]
+
+
 def test_argument_errors(native):
     L = N.load()
     with SolveServer(max_concurrent=1, memory_budget=1 << 20) as srv:
