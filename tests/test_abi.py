@@ -103,6 +103,49 @@ def test_argument_errors_are_reported(native):
     assert native.foggy_create(C.byref(p), 0, C.byref(h)) == _native.FOGGY_ERR_ARGUMENT
 
 
+C_PROGRAM = r"""
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include "foggy_gpu.h"
+
+int main(void) {
+    foggy_params p;
+    foggy_handle h = NULL;
+    int64_t parent = -1, kids[8];
+    double c[3];
+    foggy_default_params(&p);
+    if (p.gmres_restart != 10 || p.gmres_max_iterations != 1000) return 1;
+    if (fabs(foggy_wigner_3j(2, 2, 2, 0, 0, 0) + sqrt(2.0 / 35.0)) > 1e-15) return 2;
+    if (foggy_tree_parent(6, 1, 1, &parent) != FOGGY_OK || parent != 0) return 3;
+    if (foggy_tree_children(1, 1, kids) != FOGGY_OK || kids[0] != 8 || kids[7] != 15) return 4;
+    if (foggy_tree_centre_of_box(1, 1, c) != FOGGY_OK || c[0] != 0.25 || c[2] != 0.75) return 5;
+    p.n_range[1] = 99;
+    if (foggy_create(&p, 0, &h) != FOGGY_ERR_ARGUMENT || h != NULL) return 6;
+    if (strstr(foggy_last_error(NULL), "n_range") == NULL) return 7;
+    puts("ok");
+    return 0;
+}
+"""
+
+
+def test_c_program_links_and_runs(native, tmp_path):
+    """The header is plain C (C99, pedantic) and a C program linked against the library calls it."""
+    import subprocess
+    from itofoggysim_b200 import _native
+    src = tmp_path / "use_abi.c"
+    src.write_text(C_PROGRAM)
+    exe = tmp_path / "use_abi"
+    libdir = os.path.dirname(_native.LIB_PATH)
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+                        "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                        "-L" + libdir, "-l:" + os.path.basename(_native.LIB_PATH), "-Wl,-rpath," + libdir, "-lm"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout, r.stderr)
+
+
 def test_handle_less_errors_are_per_thread(native):
     """Threads whose foggy_create calls fail side by side each read their own message."""
     import threading
