@@ -235,6 +235,15 @@ int32_t foggy_build_tree(foggy_handle h, int64_t* uindex_out, int32_t* order_out
  * points[3*n] host memory, out[n]. */
 int32_t foggy_universal_index(int32_t n, const double* points, int32_t l, int64_t* out);
 
+/* Device bytes a direct-operator solve of this scene holds at its peak, from the plan the handle
+ * follows (scene arrays, operator slabs, Krylov workspace, staging, order tables), into
+ * solve_bytes, and the pair tables' bytes into table_bytes (FP64, plus FP32 when
+ * params->precision = 1).  The solve server admits requests by these.  Host only: no handle, no
+ * GPU. */
+int32_t foggy_estimate_solve_bytes(const foggy_params* params, int32_t n_spheres, const int32_t* param_index,
+                                   int32_t n_param, const int32_t* n_range, int64_t* solve_bytes,
+                                   int64_t* table_bytes);
+
 /* libtree box arithmetic on universal indices (box n at level l, 0 <= n < 8^l, l = 0..21), on the
  * host: no handle, no GPU.
  * foggy_tree_parent: the box `step` levels up (1 <= step <= l), n >> 3 step

@@ -38,7 +38,7 @@ EXPORTS = [
     "foggy_get_field", "foggy_set_gaussian_beams", "foggy_solve_rhs", "foggy_server_start",
     "foggy_server_submit", "foggy_server_poll", "foggy_server_cancel", "foggy_server_release",
     "foggy_server_stop", "foggy_matvec_rhs", "foggy_tree_parent", "foggy_tree_children",
-    "foggy_tree_centre_of_box", "foggy_tree_neighbours",
+    "foggy_tree_centre_of_box", "foggy_tree_neighbours", "foggy_estimate_solve_bytes",
 ]
 
 
@@ -180,6 +180,7 @@ def load():
         "foggy_tree_children": (i32, [i64, i32, pi64]),
         "foggy_tree_centre_of_box": (i32, [i64, i32, pd]),
         "foggy_tree_neighbours": (i32, [i64, i32, pi64, pi32]),
+        "foggy_estimate_solve_bytes": (i32, [C.POINTER(FoggyParams), i32, pi32, i32, pi32, pi64, pi64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1691,6 +1691,26 @@ int32_t foggy_universal_index(int32_t n, const double* points, int32_t l, int64_
     return FOGGY_OK;
 }
 
+int32_t foggy_estimate_solve_bytes(const foggy_params* params, int32_t n_spheres, const int32_t* param_index,
+                                   int32_t n_param, const int32_t* n_range, int64_t* solve_bytes,
+                                   int64_t* table_bytes) {
+    TRY(check_params(nullptr, params));
+    if (n_spheres < 1 || n_param < 1 || !param_index || !n_range || !solve_bytes || !table_bytes)
+        return fail(nullptr, FOGGY_ERR_ARGUMENT, "empty or NULL input");
+    int pmax = 0;
+    for (int i = 0; i < n_param; ++i)
+        if (n_range[2 * i] != 1 || n_range[2 * i + 1] < 1)
+            return fail(nullptr, FOGGY_ERR_ARGUMENT, "parameter n_range must be [1, n_max], n_max >= 1");
+    for (int j = 0; j < n_spheres; ++j) {
+        if (param_index[j] < 0 || param_index[j] >= n_param)
+            return fail(nullptr, FOGGY_ERR_ARGUMENT, "param_index out of range");
+        pmax = std::max(pmax, std::min(n_range[2 * param_index[j] + 1], params->n_range[1]));
+    }
+    if (pmax > 32) return fail(nullptr, FOGGY_ERR_UNSUPPORTED, "the direct operator supports truncation orders up to 32");
+    *solve_bytes = estimate_solve_bytes(*params, n_spheres, param_index, n_param, n_range, 0, table_bytes);
+    return FOGGY_OK;
+}
+
 // ---- libtree box arithmetic: integer work on universal indices, on the host ------------------
 static int check_box(int64_t n, int32_t l) {
     if (l < 0 || l > 21) return fail(nullptr, FOGGY_ERR_ARGUMENT, "level must be 0..21");

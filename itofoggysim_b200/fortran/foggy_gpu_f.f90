@@ -196,6 +196,15 @@ module foggy_gpu_f
             integer(c_int64_t), intent(out) :: out(*)
             integer(c_int32_t) :: rc
         end function
+        function foggy_estimate_solve_bytes(p, n_spheres, param_index, n_param, n_range, solve_bytes, &
+                                            table_bytes) result(rc) bind(c, name="foggy_estimate_solve_bytes")
+            import :: c_int32_t, c_int64_t, foggy_params
+            type(foggy_params), intent(in) :: p
+            integer(c_int32_t), value :: n_spheres, n_param
+            integer(c_int32_t), intent(in) :: param_index(*), n_range(2, *)
+            integer(c_int64_t), intent(out) :: solve_bytes, table_bytes
+            integer(c_int32_t) :: rc
+        end function
         function foggy_tree_parent(n, l, step, parent) result(rc) bind(c, name="foggy_tree_parent")
             import :: c_int32_t, c_int64_t
             integer(c_int64_t), value :: n
@@ -331,6 +340,7 @@ module foggy_gpu_f
     public :: foggy_solve_rhs, foggy_server_start, foggy_server_submit, foggy_server_poll
     public :: foggy_server_cancel, foggy_server_release, foggy_server_stop, foggy_matvec_rhs
     public :: foggy_tree_parent, foggy_tree_children, foggy_tree_centre_of_box, foggy_tree_neighbours
+    public :: foggy_estimate_solve_bytes
     public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
     public :: foggy_ms_get_backward_error, foggy_ms_destructor, foggy_ms_vector_length
 

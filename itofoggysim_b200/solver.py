@@ -354,6 +354,17 @@ def universal_index(points, level):
     return out
 
 
+def estimate_solve_bytes(scene, precision=0):
+    """(solve bytes, pair-table bytes) a direct-operator solve of scene holds on the device at its
+    peak (foggy_estimate_solve_bytes; host only, no GPU)."""
+    p = _params(scene, precision=precision)
+    sb, tb = C.c_int64(), C.c_int64()
+    N.check(N.load().foggy_estimate_solve_bytes(C.byref(p), scene.n_spheres, N.ptr(N.as_i32(scene.param_index), C.c_int32),
+                                               scene.n_param, N.ptr(N.as_i32(scene.n_range_param).reshape(-1), C.c_int32),
+                                               C.byref(sb), C.byref(tb)))
+    return sb.value, tb.value
+
+
 def tree_parent(n, level, step=1):
     """lib_tree_get_parent (libtree/src/lib/lib_tree.f90:405-431): the box `step` levels above box
     n of the given level."""
