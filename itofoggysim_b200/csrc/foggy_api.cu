@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "foggy_kernels.cuh"
 
 using namespace foggy;
@@ -26,6 +28,16 @@ thread_local std::string g_err;
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+};
+
+// NVTX range over a scope: the phases of a solve (scene, pair tables, operator applications,
+// ML-FMM passes) on a profiler's timeline, as the reference's _TRACE_ timings per pass
+// (libmlfmm/src/lib/lib_ml_fmm.f90:339-372).  Without a tool attached it costs a branch.
+struct Trace {
+    explicit Trace(const char* name) { nvtxRangePushA(name); }
+    ~Trace() { nvtxRangePop(); }
+    Trace(const Trace&) = delete;
+    Trace& operator=(const Trace&) = delete;
 };
 
 }  // namespace
@@ -454,6 +466,7 @@ int ensure_pair_tables(foggy_handle h) {
         cudaFree(d_sizes);
         if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("pair offsets: ") + cudaGetErrorString(e));
     }
+    Trace tr("pair tables");
     SGaunt g{h->d_koffS, h->d_gs, h->gs_nm};
     int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, (148 * 8 + h->N - 1) / h->N));
     dim3 grid(h->N, chunks);
@@ -653,21 +666,37 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
         launch_translate(a, ntgt, h->stream);
         if (ntgt > 0) h->launches += 1;
     };
+    Trace tr("ML-FMM operator");
     // upward: aggregation at the leaves, then M2M level by level
-    pass(B, S, x, h->d_fmm_C, 0, 1, leaf0, nbox - leaf0, sts, z_reg, 0, false);
-    for (int li = nlev - 2; li >= 0; --li)
-        pass(B, B, h->d_fmm_C, h->d_fmm_C, 2, 3, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
-             z_reg, 0, false);
+    {
+        Trace tp("aggregation");
+        pass(B, S, x, h->d_fmm_C, 0, 1, leaf0, nbox - leaf0, sts, z_reg, 0, false);
+    }
+    {
+        Trace tp("M2M");
+        for (int li = nlev - 2; li >= 0; --li)
+            pass(B, B, h->d_fmm_C, h->d_fmm_C, 2, 3, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
+                 z_reg, 0, false);
+    }
     // downward: M2L on every level, then L2L from the coarsest level down
-    for (int li = 0; li < nlev; ++li)
-        pass(B, B, h->d_fmm_C, h->d_fmm_D, 4, 5, t.level_base[li], t.level_base[li + 1] - t.level_base[li], sts, zi,
-             0, false);
-    for (int li = 1; li < nlev; ++li)
-        pass(B, B, h->d_fmm_D, h->d_fmm_D, 6, 7, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
-             z_reg, 1, false);
+    {
+        Trace tp("M2L");
+        for (int li = 0; li < nlev; ++li)
+            pass(B, B, h->d_fmm_C, h->d_fmm_D, 4, 5, t.level_base[li], t.level_base[li + 1] - t.level_base[li], sts,
+                 zi, 0, false);
+    }
+    {
+        Trace tp("L2L");
+        for (int li = 1; li < nlev; ++li)
+            pass(B, B, h->d_fmm_D, h->d_fmm_D, 6, 7, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
+                 z_reg, 1, false);
+    }
     // final summation: box to sphere, near field, then y = x + T (both)
-    pass(S, B, h->d_fmm_D, h->d_fmm_slab, 8, 9, 0, h->N, sts, z_dor, 0, conv == 0);
-    pass(S, S, x, h->d_fmm_slab + h->n_unk, 10, 11, 0, h->N, 1.0, zi, 0, false);
+    {
+        Trace tp("box to sphere, near field");
+        pass(S, B, h->d_fmm_D, h->d_fmm_slab, 8, 9, 0, h->N, sts, z_dor, 0, conv == 0);
+        pass(S, S, x, h->d_fmm_slab + h->n_unk, 10, 11, 0, h->N, 1.0, zi, 0, false);
+    }
     CKL(h);
     k_direct_finish<<<h->N, 256, 0, h->stream>>>(sv, x, h->d_fmm_slab, 2, h->n_unk, y);
     h->launches += 1;
@@ -682,6 +711,7 @@ int apply_operator(foggy_handle h, const cplx* x, cplx* y, bool fp32 = false) {
     TRY(ensure_pair_tables(h));
     DirectArgs a = direct_args(h, x);
     a.fp32 = (fp32 && h->stab32_ready) ? 1 : 0;
+    Trace tr(a.fp32 ? "operator (FP32)" : "operator (FP64)");
     for (const DirectBucket& b : h->launches_direct) {
         launch_direct(a, b, h->stream);
         h->launches += 1;
@@ -1163,6 +1193,7 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
         pmax = std::max(pmax, std::min(n_range[2 * ip + 1], pg));
     }
     if (pmax > 32) return fail(h, FOGGY_ERR_UNSUPPORTED, "the direct operator supports truncation orders up to 32");
+    Trace tr("foggy_set_spheres");
     CK(h, cudaSetDevice(h->device));
     free_scene(h);
     const int32_t rc = load_scene(h, n_spheres, centres, param_index, n_param, refractive_index, radius, n_range);
@@ -1311,6 +1342,7 @@ int32_t foggy_solve(foggy_handle h, const double* x0, double* x, int32_t mem, fo
     if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
     if (!x) return fail(h, FOGGY_ERR_ARGUMENT, "x is NULL");
     if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    Trace tr("foggy_solve");
     CK(h, cudaSetDevice(h->device));
     foggy_stats st{};
     h->launches = 0;
@@ -1378,6 +1410,7 @@ int32_t foggy_get_field(foggy_handle h, const double* x, int32_t mem, int32_t np
     if (npoints < 0) return fail(h, FOGGY_ERR_ARGUMENT, "npoints must be >= 0");
     if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
     if (npoints == 0) return FOGGY_OK;
+    Trace tr("foggy_get_field");
     CK(h, cudaSetDevice(h->device));
     const size_t len = (size_t)foggy_vector_length(h);
     const int C = (h->pg + 1) * (h->pg + 1) - 1;
