@@ -1,6 +1,7 @@
-"""The algorithmic flop count behind bench.py's roofline (CPU): the closed form over truncation
-orders equals an entry-by-entry enumeration of the same definition, the per-translation form
-sums to it, and the counts quoted for the two bench scenes hold."""
+"""bench.py's workload definitions on the CPU.  The algorithmic flop count behind the roofline: the
+closed form over truncation orders equals an entry-by-entry enumeration of the same definition,
+the per-translation form sums to it, and the counts quoted for the two bench scenes hold.  The
+128 right-hand sides of the several-right-hand-side workload: Fibonacci directions x TM/TE."""
 import os
 import sys
 
@@ -61,3 +62,19 @@ def test_bench_scene_counts():
     # 64-sphere cluster (p = 15) and the 2000-sphere lognormal cluster, per operator application
     assert bench.algorithmic_flops(S.small_cluster()) == 701184000.0
     assert bench.algorithmic_flops(S.medium_cluster()) == pytest.approx(1.0793e12, rel=1e-4)
+
+
+def test_fibonacci_right_hand_sides():
+    # 64 directions z_i = 1 - (2i+1)/64, phi_i = i pi (3 - sqrt 5) (mod 2 pi), each TM then TE
+    w = bench.fibonacci_waves(64)
+    i = np.arange(64)
+    assert len(w["wave_theta"]) == 128
+    assert np.allclose(np.cos(w["wave_theta"][::2]), 1.0 - (2.0 * i + 1.0) / 64.0, atol=1e-15)
+    assert np.allclose(w["wave_phi"][::2], np.mod(i * np.pi * (3.0 - np.sqrt(5.0)), 2.0 * np.pi), atol=1e-12)
+    assert np.array_equal(w["wave_theta"][::2], w["wave_theta"][1::2])
+    assert np.all(w["jones"][::2] == [1.0, 0.0, 0.0, 0.0]) and np.all(w["jones"][1::2] == [0.0, 0.0, 1.0, 0.0])
+    d = np.stack([np.sin(w["wave_theta"][::2]) * np.cos(w["wave_phi"][::2]),
+                  np.sin(w["wave_theta"][::2]) * np.sin(w["wave_phi"][::2]), np.cos(w["wave_theta"][::2])], 1)
+    # distinct directions, spread over the sphere (mean direction near zero)
+    assert np.min(np.linalg.norm(d[:, None] - d[None], axis=-1) + 10 * np.eye(64)) > 0.2
+    assert np.linalg.norm(d.mean(0)) < 0.05
