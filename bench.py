@@ -35,7 +35,11 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "MLFMM-GMRES solves/s, p50/p99 latency at 1e-6 rel err vs plain FP64 on 1 B200"
+# the reference's headline metric names the ML-FMM operator; lines that run the direct all-pairs
+# operator (exact, the default) say so in the metric text
+METRIC_MLFMM = "MLFMM-GMRES solves/s, p50/p99 latency at 1e-6 rel err vs plain FP64 on 1 B200"
+METRIC = ("GMRES solves/s with the direct all-pairs T-matrix operator (in place of the ML-FMM), p50/p99 latency "
+          "at 1e-6 rel err vs plain FP64 on 1 B200")
 
 # Operator applications one solve of the default workload takes (GMRES(50) to 1e-8 with the
 # initial residual and one explicit residual per restart), measured by the GPU arm; the CPU
@@ -460,7 +464,8 @@ def run_mixed(args):
         "iterations": its[-1], "matvecs": mvs[-1], "backward_error": st["backward_error"],
         "rel_coefficient_error": float(np.linalg.norm(x - x64) / np.linalg.norm(x64)),
         "c_ext_rel_error": float(abs(c[1] - c64[1]) / abs(c64[1])),
-        "roofline": {"bound": "simt", "compute": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        "roofline": {"bound": "fp32", "compute": "FP32 CUDA-core pipe (FFMA); no tensor-core instruction",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None, "kernel": "k_direct<cplxf> (+k_direct_finish)",
                      "flops_per_launch": flops, "ms_per_launch": t32,
                      "peak_source": "cuBLAS FP32 SGEMM 8192^3 (TF32 off) measured in this run (no FP32 figure "
@@ -621,14 +626,16 @@ def main():
             with open(tf) as f:
                 traffic = json.load(f).get(sc.name + ("_mlfmm" if fmm else ""))
         result = {
-            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC_MLFMM if fmm else METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_of(sc, args),
             "latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99)},
             "solve": {"iterations": iters, "matvecs_per_solve": mv_count // args.steps,
                       "backward_error": berr, "ms_operator_per_solve": mv_ms / args.steps},
-            "roofline": {"bound": "tensor", "compute": "fp64", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "fp64", "compute": "FP64 CUDA-core pipe (DFMA); no tensor-core instruction",
+                         "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
                          "kernel": ("k_translate (ML-FMM passes) + k_direct_finish" if fmm
                                     else "k_direct (+k_direct_finish)"), "flops_per_launch": flops,

@@ -345,8 +345,10 @@ DirectArgs direct_args(foggy_handle h, const cplx* x) {
     a.delta = h->d_delta;
     a.g = SGaunt{h->d_koffS, h->d_gs, h->gs_nm};
     a.dt = dtabs(h);
-    a.pt.stab = h->stab_ready ? h->d_stab : nullptr;
-    a.pt.stab32 = h->stab32_ready ? h->d_stab32 : nullptr;
+    // tables of another radial function are never read
+    const bool zok = h->stab_z == h->prm.z_coupling;
+    a.pt.stab = (zok && h->stab_ready) ? h->d_stab : nullptr;
+    a.pt.stab32 = (zok && h->stab32_ready) ? h->d_stab32 : nullptr;
     a.delta32 = h->d_delta32;
     a.fp32 = 0;
     a.pt.pair_off = h->d_pair_off;
@@ -421,7 +423,13 @@ int ensure_pair_tables(foggy_handle h) {
         h->stab32_ready = false;
         return FOGGY_OK;
     }
-    if (h->stab_z == h->prm.z_coupling && (mixed ? h->stab32_ready : h->stab_ready)) return FOGGY_OK;
+    // both precisions' tables were built for one radial function; a new one invalidates both,
+    // whichever of them this call rebuilds
+    if (h->stab_z != h->prm.z_coupling) {
+        h->stab_ready = false;
+        h->stab32_ready = false;
+    }
+    if (mixed ? h->stab32_ready : h->stab_ready) return FOGGY_OK;
     const int64_t npairs = (int64_t)h->N * (h->N - 1) / 2;
     // total size from the counts of each truncation order
     std::vector<int64_t> cnt(h->pmax + 1, 0);
@@ -1058,6 +1066,11 @@ int32_t foggy_set_params(foggy_handle h, const foggy_params* params) {
                         params->reference_row_rule != h->prm.reference_row_rule;
     foggy_params old = h->prm;
     h->prm = *params;
+    if (params->z_coupling != old.z_coupling) {
+        // the pair tables hold S for the old radial function
+        h->stab_ready = false;
+        h->stab32_ready = false;
+    }
     if (params->tree_l_max != old.tree_l_max || params->tree_s_opt != old.tree_s_opt) {
         h->tree_ready = false;
         free_fmm(h);

@@ -19,11 +19,14 @@ lp = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 
 
 def build():
-    """Compile liboracle.so (and, where the reference checkout exists, _ref/libwigxjpf.a)."""
-    ref = os.environ.get("FOGGY_REFERENCE", "/root/reference")
+    """Compile liboracle.so (and _ref/libwigxjpf.a from the reference checkout named by the
+    environment variable FOGGY_REFERENCE; without it the prebuilt _ref/ library is used)."""
+    ref = os.environ.get("FOGGY_REFERENCE", "")
     args = ["make", "-s", "-C", HERE]
-    if os.path.isdir(ref):
+    if ref and os.path.isdir(ref):
         args.append("REF=" + ref)
+    elif not os.path.exists(os.path.join(HERE, "_ref", "libwigxjpf.a")):
+        raise RuntimeError("oracle/_ref/libwigxjpf.a is missing: set FOGGY_REFERENCE to the reference checkout")
     subprocess.run(args, check=True)
 
 

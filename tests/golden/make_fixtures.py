@@ -135,4 +135,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FOGGY_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_fixtures.py REFERENCE_CHECKOUT (or set FOGGY_REFERENCE)")
+    main(ref)

@@ -10,6 +10,7 @@ after call: the array keeps the previous call's contents, which must not leak in
 This file is collected last so that it runs both alone and after every other test.
 """
 import ctypes as C
+import dataclasses
 import math
 
 import numpy as np
@@ -82,6 +83,61 @@ def test_static_matches_matvec_twice(native, case):
         ys4 = _static(s, torch, x1)
         assert _err(ys3, yp2, g) < TOL
         assert _err(ys4, yp1, g) < TOL
+
+
+def test_static_after_radial_function_change(native):
+    """The static entry reads pair tables it does not build: after foggy_matvec built them for
+    z = j_n, a switch to z = h_n through foggy_set_params must not let it read the old ones."""
+    torch = pytest.importorskip("torch")
+    sc = S.random_cluster(10, seed=23, p=None, z_coupling=1, reference_row_rule=False)
+    g = _g(sc)
+    x1, x2 = _vector(sc, 3), _vector(sc, 4)
+    with solver.MultiSphereSolver(sc) as s:
+        y1 = _plain(s, torch, x1)             # builds the z = 1 tables
+        assert _err(_static(s, torch, x1), y1, g) < TOL
+        s.params.z_coupling = 3
+        s._set()
+        ys = _static(s, torch, x2)            # before any z = 3 tables exist
+        yp = _plain(s, torch, x2)             # rebuilds the tables for z = 3
+        assert _err(ys, yp, g) < TOL
+        assert _err(_static(s, torch, x2), yp, g) < TOL   # now with the z = 3 tables
+        assert _err(yp, _plain_fresh(sc, torch, x2, 3), g) < TOL
+
+
+def _plain_fresh(sc, torch, x, z):
+    sc2 = dataclasses.replace(sc, z_coupling=z)
+    with solver.MultiSphereSolver(sc2) as s:
+        return _plain(s, torch, x)
+
+
+def test_static_on_mixed_precision_handle(native):
+    """A mixed-precision solve builds the single-precision tables (and the double ones when both
+    fit); the static entry is FP64 and must match foggy_matvec on that handle, also after a
+    precision switch and a radial-function change in between."""
+    torch = pytest.importorskip("torch")
+    sc = S.random_cluster(10, seed=24, p=None, z_coupling=3, reference_row_rule=False)
+    g = _g(sc)
+    x = _vector(sc, 5)
+    with solver.MultiSphereSolver(sc, precision=1) as s:
+        _, st = s.solve()
+        assert st["status"] == 0
+        yp = _plain(s, torch, x)
+        assert _err(_static(s, torch, x), yp, g) < TOL
+        # FP64 at z = 1, then mixed again at z = 1: the FP32 tables of z = 3 must be rebuilt
+        s.params.precision = 0
+        s.params.z_coupling = 1
+        s._set()
+        y1 = _plain(s, torch, x)
+        s.params.precision = 1
+        s._set()
+        _, st1 = s.solve()
+        assert st1["status"] == 0
+        assert _err(_static(s, torch, x), y1, g) < TOL
+    # the mixed solve at z = 1 on that handle takes the same Arnoldi steps as on a fresh handle
+    sc1 = dataclasses.replace(sc, z_coupling=1)
+    with solver.MultiSphereSolver(sc1, precision=1) as s:
+        _, st_fresh = s.solve()
+    assert st1["iterations"] == st_fresh["iterations"]
 
 
 def test_static_rejects_scene_above_limit(native):
