@@ -283,6 +283,16 @@ int32_t foggy_get_field(foggy_handle h, const double* x, int32_t mem, int32_t np
  * out == NULL to query the count. */
 int32_t foggy_tree_domain(foggy_handle h, int32_t l, int64_t n, int32_t kind, int64_t* out, int32_t* count);
 
+/* The ML-FMM's pass lists as the library builds them on the device from the sorted keys (the
+ * reference builds them in lib_ml_fmm_hf_create_hierarchy, libmlfmm/src/lib/lib_ml_fmm_helper_functions.f90:366-457,
+ * with lib_tree_get_domain_e1/e2/i4, libtree/src/lib/lib_tree.f90:492-1143), one CSR list per part:
+ * 0/1 aggregation (leaf box <- its coupled spheres), 2/3 children, 4/5 interaction list I4 (existing
+ * boxes), 6/7 parent, 8/9 box to sphere (sphere <- its leaf box), 10/11 near field (sphere <- E2 of
+ * its leaf without itself); even parts are pointers, odd parts indices.  Boxes are numbered level by
+ * level from l_min in ascending universal index, leaf pointers run over the leaf boxes in that order,
+ * spheres are 0-based input indices.  out = NULL queries the length. */
+int32_t foggy_fmm_lists(foggy_handle h, int32_t part, int32_t* out, int32_t* count);
+
 /* ---- operator without allocation ------------------------------------------------------- */
 
 /* y = A x for device buffers x, y (reference layout), the direct operator only, with no
@@ -326,6 +336,34 @@ int32_t foggy_solve_rhs(foggy_handle h, int32_t nrhs, const double* x0, double* 
  * each): lib_mie_ms_solver_calculate_vector_b (lib_mie_ms_solver_interface.f90:739-783) for several
  * vectors in one call; each y_v equals foggy_matvec of x_v. */
 int32_t foggy_matvec_rhs(foggy_handle h, int32_t nrhs, const double* x, double* y, int32_t mem);
+
+/* ---- several right-hand sides in one block -------------------------------------------- */
+
+/* The right-hand sides of one scene (one per plane wave set on the handle, nrhs = that count; no
+ * Gaussian beams) solved together.  The reference solves each illumination with its own GMRES run
+ * (lib_mie_ms_solver_run, lib_mie_ms_solver_interface.f90:143-154, around lib_solver_GMRES.f90:116-316);
+ * here every operator application serves the whole block: each CTA of the operator applies the
+ * translations of one target sphere to a tile of right-hand sides, whose width the library picks per
+ * launch shape by timing (foggy_block_tiles).  Each right-hand side keeps its own GMRES(m) recurrence
+ * (gmres_restart 1..63, gmres_tolerance, gmres_max_iterations apply to each) and leaves the block when
+ * its true residual meets the tolerance at a restart.  With params.precision = 1 the Arnoldi steps
+ * apply the operator with FP32 translation arithmetic and the restart residuals in FP64.  x (and x0, if
+ * not NULL) hold nrhs vectors of foggy_vector_length entries one after the other; cross_sections
+ * ({C_sca, C_ext, C_abs} per right-hand side), iterations and backward_errors (per right-hand side) may
+ * be NULL.  stats: iterations summed over right-hand sides, matvecs = vectors the operator was applied
+ * to, the largest backward error; the status is that of the first right-hand side that failed. */
+int32_t foggy_solve_block(foggy_handle h, int32_t nrhs, const double* x0, double* x, int32_t mem, foggy_stats* stats,
+                          double* cross_sections, int32_t* iterations, double* backward_errors);
+
+/* y_v = A x_v for nrhs vectors in one block operator application (the direct operator,
+ * lib_mie_ms_solver_calculate_vector_b, lib_mie_ms_solver_interface.f90:739-783, applied to several
+ * vectors at once); precision 0 = FP64 translations, 1 = FP32 translations (FP64 vectors). */
+int32_t foggy_matvec_block(foggy_handle h, int32_t nrhs, int32_t precision, const double* x, double* y, int32_t mem);
+
+/* The block operator's tile width per launch for a block of nrhs vectors, tuned on first use:
+ * out[4 i + 0..3] = (target spheres, source spheres, largest degree, right-hand sides per CTA) of
+ * launch i.  out = NULL queries the launch count.  No counterpart in the reference. */
+int32_t foggy_block_tiles(foggy_handle h, int32_t precision, int32_t nrhs, int32_t* out, int32_t* count);
 
 /* ---- serving ------------------------------------------------------------------------- */
 

@@ -38,7 +38,8 @@ EXPORTS = [
     "foggy_get_field", "foggy_set_gaussian_beams", "foggy_solve_rhs", "foggy_server_start",
     "foggy_server_submit", "foggy_server_poll", "foggy_server_cancel", "foggy_server_release",
     "foggy_server_stop", "foggy_matvec_rhs", "foggy_tree_parent", "foggy_tree_children",
-    "foggy_tree_centre_of_box", "foggy_tree_neighbours", "foggy_estimate_solve_bytes",
+    "foggy_tree_centre_of_box", "foggy_tree_neighbours", "foggy_estimate_solve_bytes", "foggy_solve_block",
+    "foggy_matvec_block", "foggy_block_tiles", "foggy_fmm_lists",
 ]
 
 
@@ -181,6 +182,10 @@ def load():
         "foggy_tree_centre_of_box": (i32, [i64, i32, pd]),
         "foggy_tree_neighbours": (i32, [i64, i32, pi64, pi32]),
         "foggy_estimate_solve_bytes": (i32, [C.POINTER(FoggyParams), i32, pi32, i32, pi32, pi64, pi64]),
+        "foggy_solve_block": (i32, [vp, i32, vp, vp, i32, C.POINTER(FoggyStats), vp, vp, vp]),
+        "foggy_matvec_block": (i32, [vp, i32, i32, vp, vp, i32]),
+        "foggy_block_tiles": (i32, [vp, i32, i32, pi32, pi32]),
+        "foggy_fmm_lists": (i32, [vp, i32, pi32, pi32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -11,6 +11,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -48,6 +49,7 @@ struct foggy_handle_s {
     cudaStream_t stream = nullptr;
     std::string err;
     std::vector<void*> allocs;   // every device allocation, freed in destroy
+    std::map<void*, size_t> alloc_bytes;   // their sizes, returned to the budget when freed
     size_t bytes_in_use = 0;
     size_t budget = 0;
 
@@ -151,7 +153,19 @@ struct foggy_handle_s {
     int* d_fmm_list = nullptr;       // CSR lists of the passes, concatenated
     int fmm_lofs[12] = {0};          // offsets of (ptr, idx) of: aggregation, children, I4, parent,
                                      // box-to-sphere, near field
+    int fmm_ltotal = 0;              // entries of the twelve lists
     cplx* d_fmm_slab = nullptr;      // box-to-sphere and near-field sums, 2 x n_unk
+    // several right-hand sides in one block (foggy_solve_block, foggy_matvec_block): vectors of
+    // nrhs slots, n_unk entries apart
+    int blk_nrhs = 0, blk_m = 0;
+    cplx* d_bV = nullptr;            // Krylov basis: vector i of slot b at (i nrhs + b) n_unk
+    cplx* d_bW = nullptr;            // operator output
+    cplx* d_bX = nullptr;            // iterates, slot order
+    cplx* d_bB = nullptr;            // right-hand sides, slot order
+    cplx* d_bR = nullptr;            // residuals
+    cplx* d_bsmall = nullptr;        // H, cs, g, h, c, y of every slot, dots partials
+    double* d_breal = nullptr;       // sn, norms, betas, tolerances, estimates, norm partials
+    int* d_bint = nullptr;           // live, kend, flags
 };
 
 namespace {
@@ -197,6 +211,7 @@ int dalloc(foggy_handle h, T** p, size_t count) {
     cudaError_t e = cudaMalloc((void**)p, bytes);
     if (e != cudaSuccess) return fail(h, FOGGY_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     h->allocs.push_back(*p);
+    h->alloc_bytes[*p] = bytes;
     h->bytes_in_use += bytes;
     return FOGGY_OK;
 }
@@ -206,6 +221,11 @@ void dfree(foggy_handle h, T*& p) {
     if (!p) return;
     auto it = std::find(h->allocs.begin(), h->allocs.end(), (void*)p);
     if (it != h->allocs.end()) h->allocs.erase(it);
+    auto sz = h->alloc_bytes.find((void*)p);
+    if (sz != h->alloc_bytes.end()) {
+        h->bytes_in_use -= std::min(h->bytes_in_use, sz->second);
+        h->alloc_bytes.erase(sz);
+    }
     cudaFree(p);
     p = nullptr;
 }
@@ -550,7 +570,8 @@ void free_fmm(foggy_handle h) {
     h->fmm_ready = false;
 }
 
-// Octree lists (host) and box storage (device) of the current scene and tree parameters.
+// Octree hierarchy and ML-FMM pass lists of the current scene and tree parameters, built on the
+// device from the sorted keys (k_tree.cu); the host keeps the level bounds only.
 int ensure_fmm(foggy_handle h) {
     if (h->fmm_ready) return FOGGY_OK;
     free_fmm(h);
@@ -558,77 +579,177 @@ int ensure_fmm(foggy_handle h) {
     TRY(ensure_tables(h, std::max(h->pg, 1)));
     TRY(build_tree_dev(h));
     const int n = h->N;
-    std::vector<unsigned long long> keys(n);
-    std::vector<int> order(n);
-    CK(h, cudaMemcpy(keys.data(), h->d_keys_sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-    CK(h, cudaMemcpy(order.data(), h->d_idx_sorted, n * sizeof(int), cudaMemcpyDeviceToHost));
-    FmmTree& t = h->fmm;
-    build_fmm_tree(n, reinterpret_cast<const uint64_t*>(keys.data()), order.data(), h->tree_lmin, h->tree_lmax, t);
-    // the reference's scaling (lib_tree_get_scaled_element_list, lib_tree.f90:320-374)
-    double D = 0.0;
-    for (int d = 0; d < 3; ++d) {
-        double lo = h->centres[d], hi = h->centres[d];
-        for (int i = 1; i < n; ++i) {
-            lo = std::min(lo, h->centres[3 * (size_t)i + d]);
-            hi = std::max(hi, h->centres[3 * (size_t)i + d]);
-        }
-        h->fmm_xmin[d] = lo;
-        D = std::max(D, (hi - lo) * (1.0 + std::ldexp(1.0, -52)));
+    int lmin = h->tree_lmin, lmax = h->tree_lmax;
+    if (lmax < lmin) lmin = lmax;
+    const int nlev = lmax - lmin + 1;
+    const size_t nl = (size_t)nlev * n;
+    std::vector<void*> scratch;
+    auto sc_alloc = [&](auto** p, size_t count) -> cudaError_t {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(**p));
+        if (e == cudaSuccess) scratch.push_back(q);
+        *p = static_cast<std::remove_reference_t<decltype(*p)>>(q);
+        return e;
+    };
+    auto cleanup = [&]() {
+        for (void* q : scratch) cudaFree(q);
+        scratch.clear();
+    };
+    auto bad = [&](cudaError_t e, const char* what) {
+        cleanup();
+        return fail(h, FOGGY_ERR_CUDA, std::string("ML-FMM tree (") + what + "): " + cudaGetErrorString(e));
+    };
+    int *flag, *incl, *run_start, *run_end, *parent, *box_level, *level_base, *cnt, *ptr;
+    long long* box_n;
+    double* mm;
+    cudaError_t e = cudaSuccess;
+    for (auto* pp : {&flag, &incl, &run_start, &run_end, &parent, &box_level})
+        if (e == cudaSuccess) e = sc_alloc(pp, nl + 1);
+    if (e == cudaSuccess) e = sc_alloc(&level_base, nlev + 1);
+    if (e == cudaSuccess) e = sc_alloc(&cnt, std::max(nl, (size_t)n) + 1);
+    if (e == cudaSuccess) e = sc_alloc(&ptr, 4 * (std::max(nl, (size_t)n) + 1));
+    if (e == cudaSuccess) e = sc_alloc(&box_n, nl + 1);
+    if (e == cudaSuccess) e = sc_alloc(&mm, 6);
+    if (e != cudaSuccess) return bad(e, "scratch");
+    // CUB scans: one temporary buffer of the largest size any of them needs
+    size_t tmp_bytes = 0, t2 = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, flag, incl, (int)nl, h->stream);
+    cub::DeviceScan::ExclusiveSum(nullptr, t2, cnt, ptr, (int)std::max(nl, (size_t)n) + 1, h->stream);
+    void* tmp = nullptr;
+    e = sc_alloc(reinterpret_cast<char**>(&tmp), std::max(tmp_bytes, t2));
+    if (e != cudaSuccess) return bad(e, "scan storage");
+    tmp_bytes = std::max(tmp_bytes, t2);
+    auto exscan = [&](const int* in, int* out, int items) {
+        size_t tb = tmp_bytes;
+        cub::DeviceScan::ExclusiveSum(tmp, tb, in, out, items, h->stream);
+    };
+    auto blocks = [](size_t items) { return (unsigned)((items + 255) / 256); };
+    const unsigned long long* keys = h->d_keys_sorted;
+    const int* order = h->d_idx_sorted;
+    k_minmax<<<1, 256, 0, h->stream>>>(n, h->d_centres, mm);
+    k_tree_flags<<<blocks(nl), 256, 0, h->stream>>>(n, nlev, lmin, keys, flag);
+    {
+        size_t tb = tmp_bytes;
+        cub::DeviceScan::InclusiveSum(tmp, tb, flag, incl, (int)nl, h->stream);
     }
-    const int nbox = (int)t.box_n.size();
-    const int nlev = t.lmax - t.lmin + 1;
-    const int leaf0 = t.level_base[nlev - 1], nleaf = nbox - leaf0;
-    const int Pg = h->pg * (h->pg + 2);
-    std::vector<double> bc(3 * (size_t)nbox);
-    std::vector<int> bp(nbox, h->pg);
-    std::vector<int64_t> bo(nbox);
-    for (int b = 0; b < nbox; ++b) {
-        box_centre(t.box_n[b], t.box_level[b], &bc[3 * (size_t)b]);
-        for (int d = 0; d < 3; ++d) bc[3 * (size_t)b + d] = bc[3 * (size_t)b + d] * D + h->fmm_xmin[d];
-        bo[b] = (int64_t)b * 2 * Pg;
-    }
-    // lists: aggregation (leaf <- its spheres; under the row rule only spheres of the global order
-    // contribute), children, I4, parent, box-to-sphere (sphere <- its leaf), near field
-    // (sphere <- E2 of its leaf without itself)
-    std::vector<int> agg_ptr(nleaf + 1, 0), agg_idx, par_ptr(nbox + 1, 0), par_idx, dor_ptr(n + 1), dor_idx(n),
-        near_ptr(n + 1, 0), near_idx;
-    for (int q = 0; q < nleaf; ++q) {
-        for (int e = t.e1_ptr[q]; e < t.e1_ptr[q + 1]; ++e)
-            if (h->couple[t.e1_idx[e]]) agg_idx.push_back(t.e1_idx[e]);
-        agg_ptr[q + 1] = (int)agg_idx.size();
-    }
-    for (int b = 0; b < nbox; ++b) {
-        if (t.parent[b] >= 0) par_idx.push_back(t.parent[b]);
-        par_ptr[b + 1] = (int)par_idx.size();
-    }
-    for (int j = 0; j < n; ++j) {
-        dor_ptr[j] = j;
-        dor_idx[j] = t.leaf_of[j];
-        const int q = t.leaf_of[j] - leaf0;
-        for (int e = t.e2_ptr[q]; e < t.e2_ptr[q + 1]; ++e)
-            if (t.e2_idx[e] != j) near_idx.push_back(t.e2_idx[e]);
-        near_ptr[j + 1] = (int)near_idx.size();
-    }
-    dor_ptr[n] = n;
-    const std::vector<int>* parts[12] = {&agg_ptr, &agg_idx, &t.child_ptr, &t.child_idx, &t.i4_ptr, &t.i4_idx,
-                                         &par_ptr, &par_idx, &dor_ptr, &dor_idx, &near_ptr, &near_idx};
-    std::vector<int> all;
+    k_tree_boxes<<<blocks(nl), 256, 0, h->stream>>>(n, nlev, lmin, keys, incl, box_n, box_level, run_start, level_base);
+    std::vector<int> lb(nlev + 1);
+    double mmh[6];
+    e = cudaMemcpyAsync(lb.data(), level_base, (nlev + 1) * sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(mmh, mm, sizeof(mmh), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return bad(e, "boxes");
+    const int nbox = lb[nlev];
+    const int lb1 = nlev > 1 ? lb[1] : nbox;
+    const int leaf0 = lb[nlev - 1], nleaf = nbox - leaf0;
+    h->launches += 4;
+    k_tree_links<<<blocks(nbox), 256, 0, h->stream>>>(nbox, n, nlev, incl, level_base, run_start, run_end, parent);
+    // per-item counts and their exclusive scans: I4 per box, E2 per leaf, near field per sphere,
+    // aggregation per leaf
+    int* i4ptr = ptr;
+    int* e2ptr = ptr + (nl + 1);
+    int* nearptr = ptr + 2 * (nl + 1);
+    int* aggptr = ptr + 3 * (nl + 1);
+    int* e2cnt = nullptr;
+    int* nearcnt = nullptr;
+    int* aggcnt = nullptr;
+    if ((e = sc_alloc(&e2cnt, nleaf + 1)) != cudaSuccess || (e = sc_alloc(&nearcnt, n + 1)) != cudaSuccess ||
+        (e = sc_alloc(&aggcnt, nleaf + 1)) != cudaSuccess)
+        return bad(e, "counts");
+    cudaMemsetAsync(cnt, 0, (nbox + 1) * sizeof(int), h->stream);
+    cudaMemsetAsync(e2cnt, 0, (nleaf + 1) * sizeof(int), h->stream);
+    cudaMemsetAsync(nearcnt, 0, (n + 1) * sizeof(int), h->stream);
+    cudaMemsetAsync(aggcnt, 0, (nleaf + 1) * sizeof(int), h->stream);
+    k_tree_i4<<<blocks(nbox), 256, 0, h->stream>>>(nbox, nlev, level_base, box_n, box_level, nullptr, cnt, nullptr);
+    exscan(cnt, i4ptr, nbox + 1);
+    k_tree_e2<<<blocks(nleaf), 256, 0, h->stream>>>(nleaf, leaf0, nbox, lmax, box_n, run_start, run_end, order, nullptr,
+                                                    e2cnt, nullptr);
+    exscan(e2cnt, e2ptr, nleaf + 1);
+    const int* incl_leaf = incl + (size_t)(nlev - 1) * n;
+    k_fmm_counts<<<blocks(std::max(n, nleaf)), 256, 0, h->stream>>>(n, nleaf, leaf0, order, h->d_couple, incl_leaf,
+                                                                     run_start, run_end, e2cnt, nearcnt, aggcnt);
+    exscan(nearcnt, nearptr, n + 1);
+    exscan(aggcnt, aggptr, nleaf + 1);
+    int tot[4] = {0, 0, 0, 0};   // I4, E2, near field, aggregation entries
+    e = cudaMemcpyAsync(&tot[0], i4ptr + nbox, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&tot[1], e2ptr + nleaf, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&tot[2], nearptr + n, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&tot[3], aggptr + nleaf, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return bad(e, "list sizes");
+    h->launches += 8;
+    int* e2idx = nullptr;
+    if ((e = sc_alloc(&e2idx, tot[1] + 1)) != cudaSuccess) return bad(e, "E2");
+    k_tree_e2<<<blocks(nleaf), 256, 0, h->stream>>>(nleaf, leaf0, nbox, lmax, box_n, run_start, run_end, order, e2ptr,
+                                                    nullptr, e2idx);
+    // the twelve lists of the passes, one buffer: aggregation, children, I4, parent, box to sphere,
+    // near field (pointers then indices each)
+    const int sizes[12] = {nleaf + 1, tot[3], nbox + 1, nbox - lb1, nbox + 1, tot[0],
+                           nbox + 1, nbox - lb1, n + 1, n, n + 1, tot[2]};
+    int total = 0;
     for (int i = 0; i < 12; ++i) {
-        h->fmm_lofs[i] = (int)all.size();
-        all.insert(all.end(), parts[i]->begin(), parts[i]->end());
+        h->fmm_lofs[i] = total;
+        total += sizes[i];
     }
-    all.push_back(0);
-    TRY(dalloc(h, &h->d_fmm_list, all.size()));
-    TRY(dalloc(h, &h->d_fmm_c, bc.size()));
-    TRY(dalloc(h, &h->d_fmm_p, bp.size()));
-    TRY(dalloc(h, &h->d_fmm_off, bo.size()));
-    TRY(dalloc(h, &h->d_fmm_C, (size_t)nbox * 2 * Pg));
-    TRY(dalloc(h, &h->d_fmm_D, (size_t)nbox * 2 * Pg));
-    TRY(dalloc(h, &h->d_fmm_slab, 2 * (size_t)h->n_unk));
-    CK(h, h2d(h, h->d_fmm_list, all.data(), all.size() * sizeof(int)));
-    CK(h, h2d(h, h->d_fmm_c, bc.data(), bc.size() * sizeof(double)));
-    CK(h, h2d(h, h->d_fmm_p, bp.data(), bp.size() * sizeof(int)));
-    CK(h, h2d(h, h->d_fmm_off, bo.data(), bo.size() * sizeof(int64_t)));
+    h->fmm_ltotal = total;
+    {
+        const int rc = dalloc(h, &h->d_fmm_list, (size_t)total + 1);
+        if (rc) {
+            cleanup();
+            return rc;
+        }
+    }
+    cudaMemsetAsync(h->d_fmm_list, 0, ((size_t)total + 1) * sizeof(int), h->stream);
+    k_fmm_child_ptr<<<blocks(nbox), 256, 0, h->stream>>>(nbox, lb1, parent, h->d_fmm_list + h->fmm_lofs[2]);
+    k_tree_i4<<<blocks(nbox), 256, 0, h->stream>>>(nbox, nlev, level_base, box_n, box_level, i4ptr, nullptr,
+                                                   h->d_fmm_list + h->fmm_lofs[5]);
+    FmmListArgs la{};
+    la.n = n;
+    la.nbox = nbox;
+    la.nleaf = nleaf;
+    la.leaf0 = leaf0;
+    la.lb1 = lb1;
+    la.order = order;
+    la.couple = h->d_couple;
+    la.incl_leaf = incl_leaf;
+    la.run_start = run_start;
+    la.run_end = run_end;
+    la.parent = parent;
+    la.e2_ptr = e2ptr;
+    la.e2_idx = e2idx;
+    la.agg_ptr = aggptr;
+    la.i4_ptr = i4ptr;
+    la.near_ptr = nearptr;
+    for (int i = 0; i < 12; ++i) la.lofs[i] = h->fmm_lofs[i];
+    la.list = h->d_fmm_list;
+    k_fmm_lists<<<blocks((size_t)std::max(n, nbox) + 1), 256, 0, h->stream>>>(la);
+    h->launches += 4;
+    // box centres, orders and coefficient offsets; the boxes' expansions
+    const int Pg = h->pg * (h->pg + 2);
+    int rc = FOGGY_OK;
+    if (!rc) rc = dalloc(h, &h->d_fmm_c, 3 * (size_t)nbox);
+    if (!rc) rc = dalloc(h, &h->d_fmm_p, (size_t)nbox);
+    if (!rc) rc = dalloc(h, &h->d_fmm_off, (size_t)nbox);
+    if (!rc) rc = dalloc(h, &h->d_fmm_C, (size_t)nbox * 2 * Pg);
+    if (!rc) rc = dalloc(h, &h->d_fmm_D, (size_t)nbox * 2 * Pg);
+    if (!rc) rc = dalloc(h, &h->d_fmm_slab, 2 * (size_t)h->n_unk);
+    if (rc) {
+        cleanup();
+        return rc;
+    }
+    k_fmm_boxes<<<blocks(nbox), 256, 0, h->stream>>>(nbox, box_n, box_level, mm, h->pg, h->d_fmm_c, h->d_fmm_p,
+                                                     h->d_fmm_off);
+    h->launches += 1;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cleanup();
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("ML-FMM lists: ") + cudaGetErrorString(e));
+    for (int d = 0; d < 3; ++d) h->fmm_xmin[d] = mmh[d];
+    FmmTree& t = h->fmm;
+    t = FmmTree();
+    t.lmin = lmin;
+    t.lmax = lmax;
+    t.level_base = lb;
     h->fmm_ready = true;
     return FOGGY_OK;
 }
@@ -644,7 +765,7 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
     const int z_dor = conv == 0 ? h->prm.z_translation_gt_r : 1;     // box to sphere
     const double sts = conv == 0 ? -1.0 : 1.0;                       // aggregation, M2L, box to sphere
     const int nlev = t.lmax - t.lmin + 1;
-    const int nbox = (int)t.box_n.size();
+    const int nbox = t.level_base[nlev];
     const int leaf0 = t.level_base[nlev - 1];
     const int* L = h->d_fmm_list;
     const int* lo = h->fmm_lofs;
@@ -772,6 +893,19 @@ int ensure_rhs(foggy_handle h) {
     return FOGGY_OK;
 }
 
+void free_block(foggy_handle h) {
+    dfree(h, h->d_bV);
+    dfree(h, h->d_bW);
+    dfree(h, h->d_bX);
+    dfree(h, h->d_bB);
+    dfree(h, h->d_bR);
+    dfree(h, h->d_bsmall);
+    dfree(h, h->d_breal);
+    dfree(h, h->d_bint);
+    h->blk_nrhs = 0;
+    h->blk_m = 0;
+}
+
 void free_scene(foggy_handle h) {
     dfree(h, h->d_centres);
     dfree(h, h->d_p);
@@ -805,6 +939,7 @@ void free_scene(foggy_handle h) {
     h->tree_ready = false;
     h->rhs_ready = false;
     free_fmm(h);
+    free_block(h);
 }
 
 int ensure_workspace(foggy_handle h, int restart) {
@@ -1859,6 +1994,31 @@ int32_t foggy_tree_domain(foggy_handle h, int32_t l, int64_t n, int32_t kind, in
     return FOGGY_OK;
 }
 
+// The ML-FMM's pass lists as built on the device (CSR, pointers then indices): part 0/1
+// aggregation (leaf <- spheres), 2/3 children, 4/5 I4, 6/7 parent, 8/9 box to sphere, 10/11 near
+// field (sphere <- E2 of its leaf without itself).  Boxes are numbered level by level from l_min
+// in ascending Morton order, leaves from the first leaf box.  No counterpart in the reference,
+// whose lists live in its hash tables (lib_tree.f90:492-1143).
+int32_t foggy_fmm_lists(foggy_handle h, int32_t part, int32_t* out, int32_t* count) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!count) return fail(h, FOGGY_ERR_ARGUMENT, "count is NULL");
+    if (part < 0 || part > 11) return fail(h, FOGGY_ERR_ARGUMENT, "part must be 0..11");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    CK(h, cudaSetDevice(h->device));
+    TRY(ensure_fmm(h));
+    const int beg = h->fmm_lofs[part];
+    const int end = part < 11 ? h->fmm_lofs[part + 1] : h->fmm_ltotal;
+    if (out) {
+        if (*count < end - beg) return fail(h, FOGGY_ERR_ARGUMENT, "out buffer too small");
+        if (end > beg) {
+            CK(h, cudaMemcpyAsync(out, h->d_fmm_list + beg, (end - beg) * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+        }
+    }
+    *count = end - beg;
+    return FOGGY_OK;
+}
+
 }  // extern "C"
 
 // ---- operator without allocation ------------------------------------------------------------
@@ -1925,3 +2085,531 @@ extern "C" int32_t foggy_matvec_static(foggy_handle h, const double* x, double* 
     CK(h, cudaStreamSynchronize(h->stream));
     return FOGGY_OK;
 }
+
+// ---- several right-hand sides in one block ------------------------------------------------------
+// The reference solves each illumination with its own GMRES run (lib_mie_ms_solver_run,
+// FoggySim/src/lib/mie_theory/lib_mie_ms_solver_interface.f90:143-154, around
+// lib_solver_GMRES.f90:116-316).  Here the right-hand sides of one scene share every operator
+// application: k_direct_block applies the operator to a block of vectors, each of its CTAs to a
+// tile of R of them, and the Krylov spaces of all right-hand sides advance in lock step (one
+// GMRES(m) recurrence per right-hand side, CGS2, Givens, explicit residual at each restart, as in
+// gmres()).  Right-hand sides that reach the tolerance at a restart leave the block.
+namespace {
+
+// Tile width R per launch shape, chosen by timing: (FP32, pair tables, largest degree, log2 of the
+// target count, block width up to 8) -> R.  Process-wide, as the choice depends on the shape only.
+std::mutex g_tile_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_tile_cache;
+
+int smem_optin(int device) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    return v;
+}
+
+std::vector<int> tile_candidates(bool fp32, int pp, bool tabs, int nrhs, int smem_max) {
+    std::vector<int> out;
+    const std::vector<int> all = fp32 ? std::vector<int>{1, 2, 4, 8} : std::vector<int>{1, 2, 4};
+    for (int R : all) {
+        if (R > 1 && R / 2 >= nrhs) break;   // a tile wider than the block would idle
+        if (block_smem_bytes(pp, tabs, fp32, R) <= (size_t)smem_max) out.push_back(R);
+    }
+    return out;
+}
+
+auto tile_key(const BlockArgs& ba, const DirectBucket& b, bool tabs) {
+    int lt = 0;
+    while ((1 << (lt + 1)) <= b.ntargets) ++lt;
+    return std::make_tuple(ba.d.fp32, (int)tabs, b.pp, lt, std::min(ba.nrhs, 8));
+}
+
+// The autotuner: every candidate width runs the launch's first 296 targets (two CTAs per SM)
+// against its first 48 sources for min(nrhs, 8) vectors into a scratch output, once to warm up
+// and once timed; the fastest wins.
+int choose_tile(foggy_handle h, const BlockArgs& ba, const DirectBucket& b, bool tabs, int* R_out) {
+    const auto key = tile_key(ba, b, tabs);
+    {
+        std::lock_guard<std::mutex> lk(g_tile_mu);
+        auto it = g_tile_cache.find(key);
+        if (it != g_tile_cache.end()) {
+            *R_out = it->second;
+            return FOGGY_OK;
+        }
+    }
+    const std::vector<int> cand = tile_candidates(ba.d.fp32, b.pp, tabs, ba.nrhs, smem_optin(h->device));
+    if (cand.empty()) return fail(h, FOGGY_ERR_UNSUPPORTED, "no tile width of the block operator fits this degree");
+    int best = cand[0];
+    if (cand.size() > 1) {
+        const int nrt = std::min(ba.nrhs, 8);
+        cplx* scratch = nullptr;
+        CK(h, cudaMalloc(&scratch, (size_t)nrt * h->n_unk * sizeof(cplx)));
+        BlockArgs bt = ba;
+        bt.y = scratch;
+        bt.nrhs = nrt;
+        DirectBucket db = b;
+        db.ntargets = std::min(b.ntargets, 296);
+        db.nsources = std::min(b.nsources, 48);
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        float best_ms = 1e30f;
+        cudaError_t err = cudaSuccess;
+        for (int R : cand) {
+            launch_direct_block(bt, db, R, h->stream);
+            cudaEventRecord(e0, h->stream);
+            launch_direct_block(bt, db, R, h->stream);
+            cudaEventRecord(e1, h->stream);
+            err = cudaEventSynchronize(e1);
+            if (err == cudaSuccess) err = cudaGetLastError();
+            if (err != cudaSuccess) break;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = R;
+            }
+            h->launches += 2;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaFree(scratch);
+        if (err != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("block tile tuning: ") + cudaGetErrorString(err));
+    }
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    g_tile_cache[key] = best;
+    *R_out = best;
+    return FOGGY_OK;
+}
+
+BlockArgs block_args(foggy_handle h, const cplx* X, cplx* Y, int nrhs, bool fp32) {
+    BlockArgs ba{};
+    ba.d = direct_args(h, nullptr);
+    ba.d.fp32 = fp32 ? 1 : 0;
+    ba.x = X;
+    ba.y = Y;
+    ba.nrhs = nrhs;
+    ba.ld = h->n_unk;
+    return ba;
+}
+
+// Y_r = A X_r for r < nrhs (device layout, n_unk apart), FP64 or FP32 translation arithmetic
+int apply_operator_block(foggy_handle h, const cplx* X, cplx* Y, int nrhs, bool fp32) {
+    if (h->prm.matvec_mode != FOGGY_MATVEC_DIRECT)
+        return fail(h, FOGGY_ERR_UNSUPPORTED, "several right-hand sides in one block: direct operator only");
+    TRY(ensure_pair_tables(h));
+    const BlockArgs ba = block_args(h, X, Y, nrhs, fp32);
+    const bool tabs = fp32 ? ba.d.pt.stab32 != nullptr : ba.d.pt.stab != nullptr;
+    Trace tr(fp32 ? "block operator (FP32)" : "block operator (FP64)");
+    CK(h, cudaMemcpyAsync(Y, X, (size_t)nrhs * h->n_unk * sizeof(cplx), cudaMemcpyDeviceToDevice, h->stream));
+    for (const DirectBucket& b : h->launches_direct) {
+        int R = 1;
+        TRY(choose_tile(h, ba, b, tabs, &R));
+        launch_direct_block(ba, b, R, h->stream);
+        h->launches += 1;
+    }
+    CKL(h);
+    return FOGGY_OK;
+}
+
+// Workspace of a block of nrhs right-hand sides with restart m; allocated before the pair tables
+// so that those are only kept when they fit beside it.
+int ensure_block_ws(foggy_handle h, int nrhs, int m) {
+    if (h->blk_nrhs >= nrhs && h->blk_m >= m && h->d_bV) return FOGGY_OK;
+    free_block(h);
+    const size_t n = (size_t)h->n_unk, nb = (size_t)nrhs;
+    TRY(dalloc(h, &h->d_bV, (size_t)(m + 1) * nb * n));
+    TRY(dalloc(h, &h->d_bW, nb * n));
+    TRY(dalloc(h, &h->d_bX, nb * n));
+    TRY(dalloc(h, &h->d_bB, nb * n));
+    TRY(dalloc(h, &h->d_bR, nb * n));
+    // H (m+1) m, cs m, g, h, c, y (m+1) each per slot; dots partials (m+1) kRedBlocks per slot
+    TRY(dalloc(h, &h->d_bsmall, nb * ((size_t)(m + 1) * m + m + 4 * (size_t)(m + 1) + (size_t)(m + 1) * kRedBlocks)));
+    // sn m, bnorm, beta, hn, tol, res per slot; norm partials kRedBlocks per slot
+    TRY(dalloc(h, &h->d_breal, nb * ((size_t)m + 5 + kRedBlocks)));
+    TRY(dalloc(h, &h->d_bint, 3 * nb));
+    h->blk_nrhs = nrhs;
+    h->blk_m = m;
+    return FOGGY_OK;
+}
+
+struct BlockPtrs {
+    cplx *H, *cs, *g, *hh, *c, *y, *part;
+    double *sn, *bnorm, *beta, *hn, *tol, *res, *npart;
+    int *live, *kend, *flags;
+};
+
+BlockPtrs block_ptrs(foggy_handle h) {
+    const size_t nb = (size_t)h->blk_nrhs, m = (size_t)h->blk_m;
+    BlockPtrs p;
+    cplx* c = h->d_bsmall;
+    p.H = c;     c += nb * (m + 1) * m;
+    p.cs = c;    c += nb * m;
+    p.g = c;     c += nb * (m + 1);
+    p.hh = c;    c += nb * (m + 1);
+    p.c = c;     c += nb * (m + 1);
+    p.y = c;     c += nb * (m + 1);
+    p.part = c;
+    double* d = h->d_breal;
+    p.sn = d;    d += nb * m;
+    p.bnorm = d; d += nb;
+    p.beta = d;  d += nb;
+    p.hn = d;    d += nb;
+    p.tol = d;   d += nb;
+    p.res = d;   d += nb;
+    p.npart = d;
+    p.live = h->d_bint;
+    p.kend = h->d_bint + nb;
+    p.flags = h->d_bint + 2 * nb;
+    return p;
+}
+
+// ||W_b|| for the first ns slots into out[b]
+int block_norms(foggy_handle h, const cplx* W, int ns, const int* live, double* out, const BlockPtrs& p) {
+    k_norm_partial_b<<<dim3(kRedBlocks, ns), 256, 0, h->stream>>>(W, h->n_unk, h->n_unk, live, p.npart);
+    k_norm_reduce_b<<<dim3(1, ns), 256, 0, h->stream>>>(p.npart, live, out, 1);
+    h->launches += 2;
+    CKL(h);
+    return FOGGY_OK;
+}
+
+// Batched GMRES over nrhs right-hand sides.  On entry h->d_bB and h->d_bX hold the right-hand sides
+// and initial guesses in right-hand-side order (slot r = right-hand side r); slots are reordered as
+// right-hand sides leave the block, and emit(a, r) stores slot a's iterate as the solution of
+// right-hand side r when it does.  iters / berr / rstatus: per right-hand side.
+template <class Emit>
+int block_gmres(foggy_handle h, int nrhs, foggy_stats* st, std::vector<int>& iters, std::vector<double>& berr,
+                std::vector<int>& rstatus, Emit emit) {
+    const int m = h->prm.gmres_restart;
+    const int maxit = h->prm.gmres_max_iterations;
+    const double tol = h->prm.gmres_tolerance;
+    const int64_t n = h->n_unk;
+    const size_t vb = (size_t)n * sizeof(cplx);
+    const bool mixed = h->prm.precision == 1;
+    const int G = grid_for(n);
+    const BlockPtrs p = block_ptrs(h);
+    const size_t ldi = (size_t)h->blk_nrhs * n;   // basis vector i -> i + 1 of one slot
+    iters.assign(nrhs, 0);
+    berr.assign(nrhs, 0.0);
+    rstatus.assign(nrhs, FOGGY_OK);
+    std::vector<int> rhs_of(nrhs);
+    for (int r = 0; r < nrhs; ++r) rhs_of[r] = r;
+    cudaEvent_t ea, eb;
+    cudaEventCreate(&ea);
+    cudaEventCreate(&eb);
+    auto matvec = [&](const cplx* Xin, cplx* Yout, int ns, bool arnoldi) -> int {
+        cudaEventRecord(ea, h->stream);
+        const int r = apply_operator_block(h, Xin, Yout, ns, arnoldi && mixed);
+        cudaEventRecord(eb, h->stream);
+        cudaEventSynchronize(eb);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ea, eb);
+        st->ms_matvec += ms;
+        st->matvecs += ns;
+        return r;
+    };
+    auto done = [&]() {
+        cudaEventDestroy(ea);
+        cudaEventDestroy(eb);
+    };
+    int nact = nrhs;
+    TRY(block_norms(h, h->d_bB, nact, nullptr, p.bnorm, p));
+    std::vector<double> hb(nrhs), hbeta(nrhs);
+    std::vector<int> hlive(nrhs), hflags(nrhs);
+    CK(h, cudaMemcpyAsync(hb.data(), p.bnorm, nrhs * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    // residuals of the current iterates; slots that meet the tolerance (or failed) leave the block
+    auto residuals = [&]() -> int {
+        int r_ = matvec(h->d_bX, h->d_bW, nact, false);
+        if (r_) return r_;
+        k_sub_b<<<dim3(G, nact), 256, 0, h->stream>>>(h->d_bB, h->d_bW, h->d_bR, n, n);
+        h->launches += 1;
+        TRY(block_norms(h, h->d_bR, nact, nullptr, p.beta, p));
+        CK(h, cudaMemcpyAsync(hbeta.data(), p.beta, nact * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        for (int a = nact - 1; a >= 0; --a) {
+            const int r = rhs_of[a];
+            const double e = hb[a] == 0.0 ? 0.0 : hbeta[a] / hb[a];
+            berr[r] = e;
+            int out = -1;
+            if (!std::isfinite(e)) out = FOGGY_ERR_NAN;
+            else if (e <= tol) out = FOGGY_OK;
+            else if (iters[r] >= maxit) out = FOGGY_ERR_NOT_CONVERGED;
+            else if (rstatus[r] == FOGGY_ERR_BREAKDOWN) out = FOGGY_ERR_BREAKDOWN;
+            if (out == -1) continue;
+            rstatus[r] = out;
+            if (hb[a] == 0.0) CK(h, cudaMemsetAsync(h->d_bX + (size_t)a * n, 0, vb, h->stream));
+            TRY(emit(a, r));
+            const int last = nact - 1;
+            if (a != last) {
+                CK(h, cudaMemcpyAsync(h->d_bX + (size_t)a * n, h->d_bX + (size_t)last * n, vb, cudaMemcpyDeviceToDevice, h->stream));
+                CK(h, cudaMemcpyAsync(h->d_bB + (size_t)a * n, h->d_bB + (size_t)last * n, vb, cudaMemcpyDeviceToDevice, h->stream));
+                CK(h, cudaMemcpyAsync(h->d_bR + (size_t)a * n, h->d_bR + (size_t)last * n, vb, cudaMemcpyDeviceToDevice, h->stream));
+                rhs_of[a] = rhs_of[last];
+                hb[a] = hb[last];
+                hbeta[a] = hbeta[last];
+            }
+            --nact;
+        }
+        CK(h, cudaMemcpyAsync(p.bnorm, hb.data(), nact * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(h, cudaMemcpyAsync(p.beta, hbeta.data(), nact * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        return FOGGY_OK;
+    };
+    int rc = residuals();
+    if (rc) { done(); return rc; }
+    std::vector<double> htol(nrhs);
+    while (nact > 0) {
+        for (int a = 0; a < nact; ++a) htol[a] = tol * hb[a];
+        CK(h, cudaMemcpyAsync(p.tol, htol.data(), nact * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        k_scale_copy_b<<<dim3(G, nact), 256, 0, h->stream>>>(h->d_bR, n, p.beta, 1, h->d_bV, n, n, nullptr);
+        k_init_cycle_b<<<(nact + 63) / 64, 64, 0, h->stream>>>(p.g, m + 1, p.beta, nact, p.live, p.kend);
+        CK(h, cudaMemsetAsync(p.flags, 0, nact * sizeof(int), h->stream));
+        h->launches += 2;
+        // the cycle's steps; a slot may stop early (converged estimate, breakdown, iteration limit)
+        int steps = m;
+        for (int a = 0; a < nact; ++a) steps = std::min(steps, std::max(1, maxit - iters[rhs_of[a]]));
+        for (int k = 0; k < m; ++k) {
+            cplx* Vk = h->d_bV + (size_t)k * ldi;
+            cplx* Vk1 = h->d_bV + (size_t)(k + 1) * ldi;
+            rc = matvec(Vk, h->d_bW, nact, true);
+            if (rc) { done(); return rc; }
+            for (int pass = 0; pass < 2; ++pass) {
+                cplx* coef = pass ? p.c : p.hh;
+                k_dots_partial_b<<<dim3(kRedBlocks, nact), 256, 0, h->stream>>>(h->d_bV, ldi, n, k + 1, h->d_bW, n,
+                                                                                p.live, p.part);
+                k_dots_reduce_b<<<dim3(k + 1, nact), 256, 0, h->stream>>>(p.part, k + 1, p.live, coef, m + 1);
+                k_axpy_multi_b<<<dim3(G, nact), 256, 0, h->stream>>>(h->d_bV, ldi, n, k + 1, coef, m + 1, h->d_bW, n,
+                                                                     p.live);
+            }
+            TRY(block_norms(h, h->d_bW, nact, p.live, p.hn, p));
+            k_scale_copy_b<<<dim3(G, nact), 256, 0, h->stream>>>(h->d_bW, n, p.hn, 1, Vk1, n, n, p.live);
+            k_givens_b<<<(nact + 63) / 64, 64, 0, h->stream>>>(p.H, m, p.cs, p.sn, p.g, p.hh, p.c, p.hn, k, p.tol,
+                                                                p.res, p.flags, p.live, p.kend, nact);
+            h->launches += 8;
+            CKL(h);
+            // slots live at this step did an Arnoldi step
+            std::vector<int> was(hlive.begin(), hlive.begin() + nact);
+            if (k == 0) std::fill(was.begin(), was.end(), 1);
+            CK(h, cudaMemcpyAsync(hlive.data(), p.live, nact * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaMemcpyAsync(hflags.data(), p.flags, nact * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+            int any = 0;
+            for (int a = 0; a < nact; ++a) {
+                if (was[a]) iters[rhs_of[a]]++, st->iterations++;
+                if (hflags[a] == 2) rstatus[rhs_of[a]] = FOGGY_ERR_NAN;
+                // a breakdown before any column leaves nothing to update with; later ones solve with
+                // the columns built so far, as gmres() does
+                if (hflags[a] == 1 && k == 0) rstatus[rhs_of[a]] = FOGGY_ERR_BREAKDOWN;
+                any |= hlive[a];
+            }
+            if (!any || k + 1 >= steps) break;
+        }
+        k_trisolve_b<<<(nact + 63) / 64, 64, 0, h->stream>>>(p.H, m, p.g, p.kend, p.y, nact);
+        k_update_x_b<<<dim3(G, nact), 256, 0, h->stream>>>(h->d_bX, n, h->d_bV, ldi, p.y, m + 1, p.kend, n);
+        h->launches += 2;
+        CKL(h);
+        st->restarts++;
+        rc = residuals();
+        if (rc) { done(); return rc; }
+    }
+    done();
+    int status = FOGGY_OK;
+    double worst = 0.0;
+    for (int r = 0; r < nrhs; ++r) {
+        worst = std::max(worst, berr[r]);
+        if (rstatus[r] != FOGGY_OK && status == FOGGY_OK) status = rstatus[r];
+    }
+    st->backward_error = worst;
+    return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t foggy_matvec_block(foggy_handle h, int32_t nrhs, int32_t precision, const double* x, double* y, int32_t mem) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!x || !y || nrhs < 1) return fail(h, FOGGY_ERR_ARGUMENT, "x or y is NULL, or nrhs < 1");
+    if (precision != 0 && precision != 1) return fail(h, FOGGY_ERR_ARGUMENT, "precision must be 0 (FP64) or 1 (FP32)");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    CK(h, cudaSetDevice(h->device));
+    TRY(stage_ref_buffers(h));
+    const size_t len = (size_t)foggy_vector_length(h);
+    const size_t n = (size_t)h->n_unk;
+    cplx* X = nullptr;
+    TRY(dalloc(h, &X, 2 * (size_t)nrhs * n));
+    cplx* Y = X + (size_t)nrhs * n;
+    SceneView sv = scene_view(h);
+    auto fin = [&](int rc) {
+        dfree(h, X);
+        return rc;
+    };
+    for (int r = 0; r < nrhs; ++r) {
+        const cplx* src = reinterpret_cast<const cplx*>(x) + r * len;
+        if (mem == FOGGY_MEM_HOST) {
+            if (cudaMemcpyAsync(h->d_ref_a, src, len * sizeof(cplx), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+                return fin(fail(h, FOGGY_ERR_CUDA, "foggy_matvec_block: host to device copy"));
+            src = h->d_ref_a;
+        }
+        k_unpack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, src, X + (size_t)r * n);
+    }
+    int rc = apply_operator_block(h, X, Y, nrhs, precision == 1);
+    if (rc) return fin(rc);
+    for (int r = 0; r < nrhs; ++r) {
+        const cplx* xr = reinterpret_cast<const cplx*>(x) + r * len;
+        cplx* dst = reinterpret_cast<cplx*>(y) + r * len;
+        if (mem == FOGGY_MEM_HOST) {
+            // the identity rows above a sphere's degree come from x, staged again
+            cudaMemcpyAsync(h->d_ref_a, xr, len * sizeof(cplx), cudaMemcpyHostToDevice, h->stream);
+            xr = h->d_ref_a;
+            k_pack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, Y + (size_t)r * n, xr, h->d_ref_b);
+            cudaMemcpyAsync(dst, h->d_ref_b, len * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
+        } else {
+            k_pack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, Y + (size_t)r * n, xr, dst);
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fin(fail(h, FOGGY_ERR_CUDA, std::string("foggy_matvec_block: ") + cudaGetErrorString(e)));
+    return fin(FOGGY_OK);
+}
+
+int32_t foggy_solve_block(foggy_handle h, int32_t nrhs, const double* x0, double* x, int32_t mem, foggy_stats* stats,
+                          double* cross_sections, int32_t* iterations, double* backward_errors) {
+    if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
+    if (!x) return fail(h, FOGGY_ERR_ARGUMENT, "x is NULL");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    if (nrhs < 1 || nrhs != (int)h->waves.size())
+        return fail(h, FOGGY_ERR_ARGUMENT, "nrhs must equal the number of plane waves set (one right-hand side each)");
+    if (!h->beams.empty()) return fail(h, FOGGY_ERR_ARGUMENT, "one right-hand side per plane wave excludes Gaussian beams");
+    if (h->prm.matvec_mode != FOGGY_MATVEC_DIRECT)
+        return fail(h, FOGGY_ERR_UNSUPPORTED, "several right-hand sides in one block: direct operator only");
+    if (h->prm.gmres_restart < 1 || h->prm.gmres_restart > 63)
+        return fail(h, FOGGY_ERR_ARGUMENT, "gmres_restart must be 1..63 for the block solve");
+    Trace tr("foggy_solve_block");
+    CK(h, cudaSetDevice(h->device));
+    foggy_stats st{};
+    h->launches = 0;
+    if (!h->ev0) {
+        cudaEventCreate(&h->ev0);
+        cudaEventCreate(&h->ev1);
+    }
+    CK(h, cudaEventRecord(h->ev0, h->stream));
+    TRY(ensure_block_ws(h, nrhs, h->prm.gmres_restart));
+    TRY(stage_ref_buffers(h));
+    const size_t len = (size_t)foggy_vector_length(h);
+    const size_t n = (size_t)h->n_unk;
+    SceneView sv = scene_view(h);
+    // right-hand sides, one per plane wave, and initial guesses, in right-hand-side order
+    const std::vector<WaveDev> all = h->waves;
+    int rc = FOGGY_OK;
+    for (int r = 0; r < nrhs && rc == FOGGY_OK; ++r) {
+        h->waves.assign(1, all[r]);
+        h->rhs_ready = false;
+        rc = ensure_rhs(h);
+        if (rc) break;
+        cudaError_t e = cudaMemcpyAsync(h->d_bB + r * n, h->d_b, n * sizeof(cplx), cudaMemcpyDeviceToDevice, h->stream);
+        if (e == cudaSuccess) {
+            if (x0) {
+                const cplx* src = reinterpret_cast<const cplx*>(x0) + r * len;
+                if (mem == FOGGY_MEM_HOST) {
+                    e = cudaMemcpyAsync(h->d_ref_a, src, len * sizeof(cplx), cudaMemcpyHostToDevice, h->stream);
+                    src = h->d_ref_a;
+                }
+                k_unpack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, src, h->d_bX + r * n);
+                h->launches += 1;
+            } else if (h->prm.use_initial_guess) {
+                e = cudaMemcpyAsync(h->d_bX + r * n, h->d_b, n * sizeof(cplx), cudaMemcpyDeviceToDevice, h->stream);
+            } else {
+                e = cudaMemsetAsync(h->d_bX + r * n, 0, n * sizeof(cplx), h->stream);
+            }
+        }
+        if (e != cudaSuccess) rc = fail(h, FOGGY_ERR_CUDA, std::string("foggy_solve_block: ") + cudaGetErrorString(e));
+    }
+    h->waves = all;
+    h->rhs_ready = false;
+    if (rc) return rc;
+    // a right-hand side that leaves the block is written to x at once (reference layout)
+    auto emit = [&](int a, int r) -> int {
+        cplx* dst = reinterpret_cast<cplx*>(x) + (size_t)r * len;
+        if (mem == FOGGY_MEM_HOST) {
+            k_pack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, h->d_bX + (size_t)a * n, nullptr, h->d_ref_b);
+            CK(h, cudaMemcpyAsync(dst, h->d_ref_b, len * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+        } else {
+            k_pack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, h->d_bX + (size_t)a * n, nullptr, dst);
+        }
+        h->launches += 1;
+        CKL(h);
+        return FOGGY_OK;
+    };
+    std::vector<int> its, rst;
+    std::vector<double> be;
+    const int status = block_gmres(h, nrhs, &st, its, be, rst, emit);
+    if (status == FOGGY_ERR_CUDA || status == FOGGY_ERR_UNSUPPORTED || status == FOGGY_ERR_NOMEM) return status;
+    CK(h, cudaEventRecord(h->ev1, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    st.ms_total = ms;
+    st.kernel_launches = h->launches;
+    st.status = status;
+    h->last_berr = st.backward_error;
+    for (int r = 0; r < nrhs; ++r) {
+        if (iterations) iterations[r] = its[r];
+        if (backward_errors) backward_errors[r] = be[r];
+    }
+    if (cross_sections) {
+        for (int r = 0; r < nrhs; ++r) {
+            h->waves.assign(1, all[r]);
+            h->rhs_ready = false;
+            const int rc2 = foggy_cross_sections(h, x + 2 * len * r, mem, cross_sections + 3 * r);
+            if (rc2 != FOGGY_OK) {
+                h->waves = all;
+                h->rhs_ready = false;
+                return rc2;
+            }
+        }
+        h->waves = all;
+        h->rhs_ready = false;
+    }
+    if (stats) *stats = st;
+    if (status != FOGGY_OK) {
+        const char* what = status == FOGGY_ERR_NOT_CONVERGED ? "GMRES did not reach the tolerance for every right-hand side"
+                           : status == FOGGY_ERR_BREAKDOWN   ? "GMRES breakdown"
+                                                             : "NaN or Inf in a residual";
+        fail(h, status, what);
+    }
+    return status;
+}
+
+// Tile width of each operator launch (tuned on first use) for a block of nrhs vectors:
+// out[4 i .. 4 i + 3] = (targets, sources, largest degree, tile width) of launch i.
+int32_t foggy_block_tiles(foggy_handle h, int32_t precision, int32_t nrhs, int32_t* out, int32_t* count) {
+    if (!h || !count) return fail(h, FOGGY_ERR_ARGUMENT, "handle or count is NULL");
+    if (h->N == 0) return fail(h, FOGGY_ERR_STATE, "no spheres set");
+    if (nrhs < 1) return fail(h, FOGGY_ERR_ARGUMENT, "nrhs < 1");
+    CK(h, cudaSetDevice(h->device));
+    *count = (int)h->launches_direct.size();
+    if (!out) return FOGGY_OK;
+    TRY(ensure_pair_tables(h));
+    // the tuner reads the first min(nrhs, 8) vectors of the block: zeros serve
+    cplx* X = nullptr;
+    const int nrt = std::min(nrhs, 8);
+    TRY(dalloc(h, &X, (size_t)nrt * h->n_unk));
+    CK(h, cudaMemsetAsync(X, 0, (size_t)nrt * h->n_unk * sizeof(cplx), h->stream));
+    BlockArgs ba = block_args(h, X, nullptr, nrhs, precision == 1);
+    const bool tabs = ba.d.fp32 ? ba.d.pt.stab32 != nullptr : ba.d.pt.stab != nullptr;
+    int rc = FOGGY_OK;
+    for (size_t i = 0; i < h->launches_direct.size() && rc == FOGGY_OK; ++i) {
+        const DirectBucket& b = h->launches_direct[i];
+        int R = 0;
+        rc = choose_tile(h, ba, b, tabs, &R);
+        out[4 * i] = b.ntargets;
+        out[4 * i + 1] = b.nsources;
+        out[4 * i + 2] = b.pp;
+        out[4 * i + 3] = R;
+    }
+    dfree(h, X);
+    return rc;
+}
+
+}  // extern "C"

@@ -37,19 +37,12 @@ void raise_smem_ceiling(const void* func, size_t bytes);
 int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_index, int NP, const int* n_range,
                              int pair_tables, int64_t* table_bytes);
 
-// ---- host: octree lists of the ML-FMM (fmm_tree.cpp) ----------------------------------------
-// Boxes of all levels l_min..l_max with a global id (level by level, ascending Morton code).
+// ---- host: octree box arithmetic (fmm_tree.cpp) ----------------------------------------------
+// Level bounds of the ML-FMM's boxes (built on the device): levels l_min..l_max, boxes with a
+// global id level by level in ascending Morton code.
 struct FmmTree {
     int lmin = 0, lmax = 0;
     std::vector<int> level_base;           // first id of level lmin + i; level_base[nlev] = boxes
-    std::vector<int64_t> box_n;            // Morton code of each box at its level
-    std::vector<int> box_level;
-    std::vector<int> parent;               // id of the parent box (-1 on level lmin)
-    std::vector<int> child_ptr, child_idx; // existing children, CSR by box id
-    std::vector<int> i4_ptr, i4_idx;       // existing interaction-list boxes, CSR by box id
-    std::vector<int> e1_ptr, e1_idx;       // spheres of each leaf box, CSR by leaf (id - first leaf id)
-    std::vector<int> e2_ptr, e2_idx;       // spheres of each leaf box and its neighbours, same index
-    std::vector<int> leaf_of;              // leaf box id of each sphere
 };
 void morton_deinterleave(int64_t n, int l, int64_t c[3]);
 int64_t morton_interleave(const int64_t c[3], int l);
@@ -58,8 +51,6 @@ void box_centre(int64_t n, int l, double out[3]);
 // interaction list of box n at level l (ascending, every candidate inside the domain)
 void tree_i2(int64_t n, int l, std::vector<int64_t>& out);
 void tree_i4(int64_t n, int l, std::vector<int64_t>& out);
-// key21_sorted: level-21 universal indices in ascending order, order: the sphere of each
-void build_fmm_tree(int n, const uint64_t* key21_sorted, const int* order, int lmin, int lmax, FmmTree& t);
 
 // Maximum truncation order of a sphere (the reference caps single spheres at 45,
 // lib_mie_ss_helper_functions.f90:32).

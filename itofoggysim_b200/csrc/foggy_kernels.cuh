@@ -114,6 +114,20 @@ struct DirectBucket {
     int pp;                    // largest degree of the launch (sizes shared memory)
 };
 size_t direct_smem_bytes(int pp, bool tabs, bool fp32 = false);
+// Several right-hand sides: nrhs vectors of n_unk entries at x + r ld (ragged scaled layout); each
+// launch adds T times its (target bucket <- source bucket) sum onto y + r ld.  d carries the scene
+// and tables (d.fp32 selects the FP32 operator); d.x, d.partial and d.cmax are not used.
+struct BlockArgs {
+    DirectArgs d;
+    const cplx* x;
+    cplx* y;
+    int nrhs;
+    int64_t ld;
+};
+// shared memory of one CTA of the several-right-hand-side operator with R vectors per CTA
+size_t block_smem_bytes(int pp, bool tabs, bool fp32, int R);
+// false when R is not one of the built tile widths (FP32: 1, 2, 4, 8; FP64: 1, 2, 4)
+bool launch_direct_block(const BlockArgs& a, const DirectBucket& b, int R, cudaStream_t s);
 size_t translation_pair_smem_bytes(int pmax);
 void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s);
 // scalar coaxial tables of every pair, in FP64 (stab: cplx*) or FP32 (cplxf*)
@@ -164,11 +178,62 @@ __global__ void k_givens(cplx* H, int ldh, cplx* cs, double* sn, cplx* g, const 
 __global__ void k_trisolve(const cplx* H, int ldh, const cplx* g, int k, cplx* y);
 __global__ void k_update_x(cplx* x, const cplx* V, int64_t ld, const cplx* y, int k, int64_t n);
 __global__ void k_init_cycle(cplx* g, int m1, const double* beta, int* flags);
+// several right-hand sides: one Krylov space per slot (blockIdx.y), basis vector i of slot b at
+// V + i ldi + b ld; live[b] = 0 skips a slot that has left the restart cycle
+__global__ void k_dots_partial_b(const cplx* V, int64_t ldi, int64_t ld, int nv, const cplx* W, int64_t n,
+                                 const int* live, cplx* part);
+__global__ void k_dots_reduce_b(const cplx* part, int nv, const int* live, cplx* out, int ostride);
+__global__ void k_axpy_multi_b(const cplx* V, int64_t ldi, int64_t ld, int nv, const cplx* h, int hstride, cplx* W,
+                               int64_t n, const int* live);
+__global__ void k_norm_partial_b(const cplx* W, int64_t ld, int64_t n, const int* live, double* part);
+__global__ void k_norm_reduce_b(const double* part, const int* live, double* out, int ostride);
+__global__ void k_scale_copy_b(const cplx* W, int64_t ldw, const double* nrm, int nstride, cplx* Vout, int64_t ldv,
+                               int64_t n, const int* live);
+__global__ void k_sub_b(const cplx* Bv, const cplx* AX, cplx* Rv, int64_t ld, int64_t n);
+__global__ void k_init_cycle_b(cplx* g, int m1, const double* beta, int nslots, int* live, int* kend);
+__global__ void k_givens_b(cplx* H, int m, cplx* cs, double* sn, cplx* g, const cplx* h, const cplx* c,
+                           const double* hn, int k, const double* tol_abs, double* res_est, int* flags, int* live,
+                           int* kend, int nslots);
+__global__ void k_trisolve_b(const cplx* H, int m, const cplx* g, const int* kend, cplx* y, int nslots);
+__global__ void k_update_x_b(cplx* X, int64_t ld, const cplx* V, int64_t ldi, const cplx* y, int ystride,
+                             const int* kend, int64_t n);
 
 // k_tree.cu -- octree keys (libtree)
 __global__ void k_minmax(int n, const double* c, double* out);
 __global__ void k_morton(int n, const double* c, const double* mm, unsigned long long* key, int* idx);
 __global__ void k_level_max(int n, int s, const unsigned long long* key, int* lmax);
 __global__ void k_uindex_points(int n, const double* pts, int l, long long* out);
+// ML-FMM hierarchy and pass lists from the sorted keys (all on the device)
+__global__ void k_tree_flags(int n, int nlev, int lmin, const unsigned long long* key, int* flag);
+__global__ void k_tree_boxes(int n, int nlev, int lmin, const unsigned long long* key, const int* incl,
+                             long long* box_n, int* box_level, int* run_start, int* level_base);
+__global__ void k_tree_links(int nbox, int n, int nlev, const int* incl, const int* level_base, const int* run_start,
+                             int* run_end, int* parent);
+__global__ void k_tree_i4(int nbox, int nlev, const int* level_base, const long long* box_n, const int* box_level,
+                          const int* ptr, int* cnt_out, int* out);
+__global__ void k_tree_e2(int nleaf, int leaf0, int nbox, int lmax, const long long* box_n, const int* run_start,
+                          const int* run_end, const int* order, const int* ptr, int* cnt_out, int* out);
+struct FmmListArgs {
+    int n, nbox, nleaf, leaf0, lb1;
+    const int* order;
+    const int* couple;
+    const int* incl_leaf;
+    const int* run_start;
+    const int* run_end;
+    const int* parent;
+    const int* e2_ptr;
+    const int* e2_idx;
+    const int* agg_ptr;
+    const int* i4_ptr;
+    const int* near_ptr;
+    int lofs[12];
+    int* list;
+};
+__global__ void k_fmm_lists(FmmListArgs a);
+__global__ void k_fmm_child_ptr(int nbox, int lb1, const int* parent, int* out);
+__global__ void k_fmm_counts(int n, int nleaf, int leaf0, const int* order, const int* couple, const int* incl_leaf,
+                             const int* run_start, const int* run_end, const int* e2_cnt, int* near_cnt, int* agg_cnt);
+__global__ void k_fmm_boxes(int nbox, const long long* box_n, const int* box_level, const double* mm, int pg,
+                            double* bc, int* bp, int64_t* bo);
 
 }  // namespace foggy

@@ -605,6 +605,12 @@ __global__ void __launch_bounds__(256) k_pair_s(SceneView sc, SGaunt g, int z, c
 // ---------------------------------------------------------------------------------------------
 // the pair tables and the d(pi/2) table of an operator precision
 __device__ __forceinline__ const cplx* stab_of(const DirectArgs& a, cplx*) { return a.pt.stab; }
+template <class C>
+__host__ inline const C* stab_of_host(const DirectArgs& a);
+template <>
+__host__ inline const cplx* stab_of_host<cplx>(const DirectArgs& a) { return a.pt.stab; }
+template <>
+__host__ inline const cplxf* stab_of_host<cplxf>(const DirectArgs& a) { return a.pt.stab32; }
 __device__ __forceinline__ const cplxf* stab_of(const DirectArgs& a, cplxf*) { return a.pt.stab32; }
 __device__ __forceinline__ const double* delta_of(const DirectArgs& a, cplx*) { return a.delta; }
 __device__ __forceinline__ const float* delta_of(const DirectArgs& a, cplxf*) { return a.delta32; }
@@ -757,6 +763,536 @@ void launch_translate(const TransArgs& a, int ntargets, cudaStream_t s) {
     size_t smem = smem_bytes<cplx>(a.pp, false);
     raise_smem_ceiling(reinterpret_cast<const void*>(k_translate), smem);
     k_translate<<<ntargets, kThreads, smem, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Several right-hand sides per CTA (the incidence directions and polarisations of one scene).
+//
+// The same seven stages as k_direct, but each item of a stage is computed for R right-hand
+// sides at once: every d(pi/2) entry, phase and coaxial coefficient S(k; n, mu) a thread reads is
+// applied to R vectors held in registers, and one set of barriers serves R translations.  The
+// shared buffers hold R values per entry, contiguous, so a thread's operands are vector loads.
+// One CTA owns one target sphere and one tile of R right-hand sides and walks all sources of a
+// bucket in order; at the end it adds T (a_n, b_n) times its sum onto y.  Launches of one
+// operator application run in order on one stream and each (target, tile) belongs to one CTA, so
+// the result is deterministic.
+namespace {
+
+template <class C, int R>
+__host__ __device__ inline size_t smem_bytes_block(int pp, bool tabs) {
+    size_t c = ((size_t)szA(pp) + szB(pp) + szAcc(pp)) * R + 4 * (size_t)(pp + 1) + (tabs ? 0 : szZ(pp));
+    size_t d = (tabs ? 0 : 4 * (size_t)szZ(pp)) + 2;
+    return c * sizeof(C) + d * sizeof(double) + (size_t)szNK(pp) * sizeof(short2);
+}
+
+template <class C, int R>
+__device__ inline Bufs<C> carve_block(double* base, int pp, bool tabs) {
+    Bufs<C> s;
+    C* c = reinterpret_cast<C*>(base);
+    s.A = c;           c += (size_t)szA(pp) * R;
+    s.B = c;           c += (size_t)szB(pp) * R;
+    s.acc = c;         c += (size_t)szAcc(pp) * R;
+    s.eps = c;         c += 2 * (pp + 1);
+    s.eth = c;         c += 2 * (pp + 1);
+    s.zeta = c;        c += tabs ? 0 : szZ(pp);
+    double* d = reinterpret_cast<double*>(c);
+    s.jb = d;          d += tabs ? 0 : 2 * szZ(pp);
+    s.yb = d;          d += tabs ? 0 : 2 * szZ(pp);
+    s.rho = d;         d += 2;
+    s.nk = reinterpret_cast<short2*>(d);
+    return s;
+}
+
+// R consecutive values from shared memory, with 16-byte loads where the size allows
+template <class C, int R>
+__device__ __forceinline__ void ldR(const C* p, C (&v)[R]) {
+    if constexpr (sizeof(C) == 16) {
+        const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double2 d = q[r];
+            v[r] = C{d.x, d.y};
+        }
+    } else if constexpr (R % 2 == 0) {
+        const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+        for (int i = 0; i < R / 2; ++i) {
+            const float4 f = q[i];
+            v[2 * i] = C{f.x, f.y};
+            v[2 * i + 1] = C{f.z, f.w};
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = p[r];
+    }
+}
+
+// E = sum over even a, O = sum over odd a of Q[a (j+1) + o] u[a][r], for both parts and R vectors
+template <class C, int R>
+__device__ __forceinline__ void delta_sum_block(const real_of<C>* __restrict__ Q, int j, int o, int amax,
+                                                const C* ua, const C* ub, C (&Ea)[R], C (&Oa)[R], C (&Eb)[R],
+                                                C (&Ob)[R]) {
+    using Rl = real_of<C>;
+#pragma unroll
+    for (int r = 0; r < R; ++r) Ea[r] = Oa[r] = Eb[r] = Ob[r] = C{0, 0};
+    const int st = j + 1;
+    int a = 0;
+    for (; a + 1 <= amax; a += 2) {
+        const Rl q0 = __ldg(Q + a * st + o);
+        const Rl q1 = __ldg(Q + (a + 1) * st + o);
+        C u0[R], u1[R];
+        ldR<C, R>(ua + a * R, u0);
+        ldR<C, R>(ua + (a + 1) * R, u1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            Ea[r].x = fma(q0, u0[r].x, Ea[r].x);
+            Ea[r].y = fma(q0, u0[r].y, Ea[r].y);
+            Oa[r].x = fma(q1, u1[r].x, Oa[r].x);
+            Oa[r].y = fma(q1, u1[r].y, Oa[r].y);
+        }
+        ldR<C, R>(ub + a * R, u0);
+        ldR<C, R>(ub + (a + 1) * R, u1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            Eb[r].x = fma(q0, u0[r].x, Eb[r].x);
+            Eb[r].y = fma(q0, u0[r].y, Eb[r].y);
+            Ob[r].x = fma(q1, u1[r].x, Ob[r].x);
+            Ob[r].y = fma(q1, u1[r].y, Ob[r].y);
+        }
+    }
+    if (a <= amax) {
+        const Rl q0 = __ldg(Q + a * st + o);
+        C u0[R], v0[R];
+        ldR<C, R>(ua + a * R, u0);
+        ldR<C, R>(ub + a * R, v0);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            Ea[r].x = fma(q0, u0[r].x, Ea[r].x);
+            Ea[r].y = fma(q0, u0[r].y, Ea[r].y);
+            Eb[r].x = fma(q0, v0[r].x, Eb[r].x);
+            Eb[r].y = fma(q0, v0[r].y, Eb[r].y);
+        }
+    }
+}
+
+// stages 2 and 6 for R vectors (fwd_item with R values per entry)
+template <class C, int R>
+__device__ __forceinline__ void fwd_item_block(const real_of<C>* delta, const C* src, C* dst, int SP, int j, int s_,
+                                               int amax, C eth) {
+    const int fold = ((j + s_) & 1) ? j + 1 : 0;
+    const C* ua = src + (size_t)(off2(j) + fold) * R;
+    C Ea[R], Oa[R], Eb[R], Ob[R];
+    delta_sum_block<C, R>(delta + qoff(j), j, s_, amax, ua, ua + (size_t)SP * R, Ea, Oa, Eb, Ob);
+    const real_of<C> pj_ = sgn(j), ps = sgn(s_);
+    C* d = dst + (size_t)off2(j) * R;
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+        C* dp = d + (size_t)part * SP * R;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const C E = part ? Eb[r] : Ea[r], O = part ? Ob[r] : Oa[r];
+            const C wp = eth * (E + O);
+            if (s_ == 0) {
+                dp[r] = wp;
+                dp[(j + 1) * R + r] = wp;
+            } else {
+                const C wm = conjg(eth) * (pj_ * (E - O));
+                dp[s_ * R + r] = ps * (wp + wm);
+                dp[(j + 1 + s_) * R + r] = ps * (wp - wm);
+            }
+        }
+    }
+}
+
+// One translation (target degree pj <- source degree pl) for the R vectors xl + r ld (r < rc),
+// added into c.s.acc; stages as in run_pair.
+template <class C, int R, class Next>
+__device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int pl, const cplx* __restrict__ xl,
+                                      int64_t ld, int rc, const C* pair_s, int cur, Next next) {
+    using Rl = real_of<C>;
+    using V2 = typename Vec2T<C>::type;
+    const Bufs<C>& s = c.s;
+    const Rl* delta = c.delta;
+    const int pp = c.pp, SP = c.SP, XP = c.XP;
+    const bool tabs = c.tabs;
+    const int Pj = pj * (pj + 2);
+    const int Pl = pl * (pl + 2);
+    if (s.rho[cur] == 0.0) {
+        const int pm = min(pj, pl), Pm = pm * (pm + 2);
+        for (int t = tid; t < 2 * Pm; t += kThreads) {
+            const int part = t >= Pm, e = t - part * Pm;
+            C* a = s.acc + (size_t)(part * Pj + e) * R;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (r < rc) {
+                    const cplx v = xl[(size_t)r * ld + part * Pl + e];
+                    a[r] = a[r] + cm<C>(v.x, v.y);
+                }
+        }
+        next(tid);
+        __syncthreads();
+        return;
+    }
+    const int kmax = min(pj, pl);
+    const C* eps = s.eps + cur * (pp + 1);
+    const C* eth = s.eth + cur * (pp + 1);
+    // ---- 1. u = e^{i mu (phi + pi/2)} x, folded ------------------------------------------
+    {
+        const int items = pl * (pl + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            const int nu = d_.x, mu = d_.y;
+            const int base = nu * nu - 1 + nu;
+            const C e = eps[mu];
+            C* U = s.A + (size_t)(off2(nu) + mu) * R;
+            C* UB = U + (size_t)SP * R;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                double2 ap{0, 0}, am{0, 0}, bp{0, 0}, bm{0, 0};
+                if (r < rc) {
+                    const double2* xv = reinterpret_cast<const double2*>(xl + (size_t)r * ld + base);
+                    ap = __ldcg(xv + mu);
+                    am = __ldcg(xv - mu);
+                    bp = __ldcg(xv + Pl + mu);
+                    bm = __ldcg(xv + Pl - mu);
+                }
+                const C ua = e * cm<C>(ap.x, ap.y), ub = e * cm<C>(bp.x, bp.y);
+                if (mu == 0) {
+                    U[r] = ua;
+                    U[(nu + 1) * R + r] = ua;
+                    UB[r] = ub;
+                    UB[(nu + 1) * R + r] = ub;
+                } else {
+                    const C va = conjg(e) * cm<C>(am.x, am.y), vb = conjg(e) * cm<C>(bm.x, bm.y);
+                    U[r] = ua + va;
+                    U[(nu + 1) * R + r] = ua - va;
+                    UB[r] = ub + vb;
+                    UB[(nu + 1) * R + r] = ub - vb;
+                }
+            }
+        }
+        if (!tabs) {
+            const int P = pj + pl + 1;
+            const double* jb = s.jb + cur * szZ(pp);
+            const double* yb = s.yb + cur * szZ(pp);
+            for (int p = tid; p <= P; p += kThreads) {
+                const cplx z = zeta_of(c.z, p, jb, yb);
+                s.zeta[p] = cm<C>(z.x, z.y);
+            }
+        }
+    }
+    __syncthreads();
+    // ---- 2. Delta u, e^{-i s theta} ----------------------------------------------------------
+    {
+        const int items = pl * (pl + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            fwd_item_block<C, R>(delta, s.A, s.B, SP, d_.x, d_.y, d_.x, eth[d_.y]);
+        }
+    }
+    __syncthreads();
+    // ---- 3. Delta^T: x'(nu, +-k) = i^{+-k} T_{+-k}, stored times (2nu+1) ------------------
+    {
+        const int items = pl * (pl + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            const int nu = d_.x, k = d_.y;
+            const int fold = ((nu + k) & 1) ? nu + 1 : 0;
+            const C* va = s.B + (size_t)(off2(nu) + fold) * R;
+            C Ea[R], Oa[R], Eb[R], Ob[R];
+            delta_sum_block<C, R>(delta + qoff(nu), nu, k, nu, va, va + (size_t)SP * R, Ea, Oa, Eb, Ob);
+            const Rl f = 2.0 * nu + 1.0;
+            const Rl pn = sgn(nu);
+            C* X = s.A + (size_t)(nu * nu - 1 + nu) * R;
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                C* Xp = X + (size_t)part * XP * R;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const C E = part ? Eb[r] : Ea[r], O = part ? Ob[r] : Oa[r];
+                    Xp[k * R + r] = ipow_mul(k, f * (E + O));
+                    if (k > 0) Xp[-k * R + r] = ipow_mul(-k, (f * pn) * (E - O));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // ---- 4. w(k, mu) for a', b' at +k and -k ---------------------------------------------
+    const int NW = (kmax + 1) * (pl + 2) - kmax * (kmax + 1) / 2;   // w plane stride (entries)
+    {
+        const double x = s.rho[cur];
+        const int W = c.dt.K + 1;
+        for (int t = tid; t < NW; t += kThreads) {
+            int k = 0, rem = t;
+            while (rem >= pl + 2 - k) {
+                rem -= pl + 2 - k;
+                ++k;
+            }
+            const int mu = k + rem;
+            const int lo = max(1, k);
+            const Rl c0 = 2.0 * mu * (mu + 1.0);
+            const Rl c1m = (mu - 1 >= lo) ? x * 2.0 * (mu - 1) * c.dt.rs[mu * W + k] / (2.0 * mu - 1.0) : 0.0;
+            const Rl c2p = (mu + 1 <= pl) ? x * 2.0 * (mu + 2) * c.dt.rs[(mu + 1) * W + k] / (2.0 * mu + 3.0) : 0.0;
+            const Rl bk2 = 2.0 * k * x;
+#pragma unroll
+            for (int sg = 0; sg < 2; ++sg) {
+                const int kk = sg ? -k : k;
+                const Rl bs = sg ? -bk2 : bk2;
+                C* wa = s.B + ((size_t)(2 * sg) * NW + t) * R;
+                C* wb = s.B + ((size_t)(2 * sg + 1) * NW + t) * R;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    C av[3], bv[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const int nu = mu - 1 + d;
+                        const bool ok = nu >= lo && nu <= pl;
+                        const int o = nu * nu - 1 + nu + kk;
+                        av[d] = ok ? s.A[(size_t)o * R + r] : C{0, 0};
+                        bv[d] = ok ? s.A[(size_t)(XP + o) * R + r] : C{0, 0};
+                    }
+                    const C ia = bs * bv[1] + c1m * av[0] - c2p * av[2];
+                    const C ib = bs * av[1] + c1m * bv[0] - c2p * bv[2];
+                    wa[r] = C{c0 * av[1].x - ia.y, c0 * av[1].y + ia.x};
+                    wb[r] = C{c0 * bv[1].x - ib.y, c0 * bv[1].y + ib.x};
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // ---- 5. out(k, n) = sum_mu S(k; n, mu) w(k, mu), folded for the back rotation ----------
+    {
+        const int rows_tot = pj + (kmax >= 1 ? kmax * pj - (kmax - 1) * kmax / 2 : 0);
+        const int M2 = max(pj, pl) + 2;
+        for (int t = tid; t < rows_tot; t += kThreads) {
+            int k = 0, rem = t;
+            for (;;) {
+                const int rk = pj - max(1, k) + 1;
+                if (rem < rk) break;
+                rem -= rk;
+                ++k;
+            }
+            const int n = max(1, k) + rem;
+            const C* w = s.B + (size_t)(k * (pl + 2) - k * (k - 1) / 2) * R;
+            const int cnt = pl + 2 - k;
+            C acc0[R], acc1[R], acc2[R], acc3[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc0[r] = acc1[r] = acc2[r] = acc3[r] = C{0, 0};
+            const int Wk = M2 - k;
+            const V2* sp = tabs ? reinterpret_cast<const V2*>(pair_s + pair_block_offset(k, M2, M2) + (n - k)) : nullptr;
+            const int Wg = c.g.NM - k + 1;
+            const size_t plane = (size_t)Wg * Wg;
+            const double* G = c.g.gs + c.g.koff[k] + (n - k);
+            for (int q = 0; q < cnt; ++q) {
+                C S;
+                if (tabs) {
+                    const V2 sv = __ldcg(sp + (size_t)q * Wk);
+                    S = C{sv.x, sv.y};
+                } else {
+                    const int mu = k + q;
+                    const double* gp = G + (size_t)(mu - k) * Wg;
+                    const int qm = min(n, mu);
+                    int p = n + mu;
+                    double sx = 0.0, sy = 0.0;
+                    for (int qq = 0; qq <= qm; ++qq, p -= 2) {
+                        const double gq = __ldg(gp + qq * plane);
+                        sx += gq * s.zeta[p].x;
+                        sy += gq * s.zeta[p].y;
+                    }
+                    S = cm<C>(sx, sy);
+                }
+                C wv[R];
+                ldR<C, R>(w + (size_t)q * R, wv);
+#pragma unroll
+                for (int r = 0; r < R; ++r) cmac(acc0[r].x, acc0[r].y, S, wv[r]);
+                ldR<C, R>(w + ((size_t)NW + q) * R, wv);
+#pragma unroll
+                for (int r = 0; r < R; ++r) cmac(acc1[r].x, acc1[r].y, S, wv[r]);
+                ldR<C, R>(w + ((size_t)2 * NW + q) * R, wv);
+#pragma unroll
+                for (int r = 0; r < R; ++r) cmac(acc2[r].x, acc2[r].y, S, wv[r]);
+                ldR<C, R>(w + ((size_t)3 * NW + q) * R, wv);
+#pragma unroll
+                for (int r = 0; r < R; ++r) cmac(acc3[r].x, acc3[r].y, S, wv[r]);
+            }
+            const Rl f = sgn(k) / (2.0 * n * (n + 1.0));
+            C* U = s.A + (size_t)(off2(n) + k) * R;
+            C* UB = U + (size_t)SP * R;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (k == 0) {
+                    const C a0 = f * acc0[r], b0 = f * acc1[r];
+                    U[r] = a0;
+                    U[(n + 1) * R + r] = a0;
+                    UB[r] = b0;
+                    UB[(n + 1) * R + r] = b0;
+                } else {
+                    const C ap = ipow_mul(-k, f * acc0[r]), am = ipow_mul(k, f * acc2[r]);
+                    const C bp = ipow_mul(-k, f * acc1[r]), bm = ipow_mul(k, f * acc3[r]);
+                    U[r] = ap + am;
+                    U[(n + 1) * R + r] = ap - am;
+                    UB[r] = bp + bm;
+                    UB[(n + 1) * R + r] = bp - bm;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // ---- 6. Delta on the translated field, e^{-i s theta} (orders |k| <= kmax only) ----------
+    {
+        const int items = pj * (pj + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            fwd_item_block<C, R>(delta, s.A, s.B, SP, d_.x, d_.y, min((int)d_.x, kmax), eth[d_.y]);
+        }
+    }
+    __syncthreads();
+    // ---- 7. Delta^T, phase, accumulate; then the next pair's tables ---------------------------
+    {
+        const int items = pj * (pj + 3) / 2;
+        for (int t = tid; t < items; t += kThreads) {
+            const short2 d_ = s.nk[t];
+            const int n = d_.x, m = d_.y;
+            const int fold = ((n + m) & 1) ? n + 1 : 0;
+            const C* va = s.B + (size_t)(off2(n) + fold) * R;
+            C Ea[R], Oa[R], Eb[R], Ob[R];
+            delta_sum_block<C, R>(delta + qoff(n), n, m, n, va, va + (size_t)SP * R, Ea, Oa, Eb, Ob);
+            const Rl pn = sgn(n);
+            const C e = eps[m];
+            const int base = n * n - 1 + n;
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                C* ap = s.acc + (size_t)(part * Pj + base + m) * R;
+                C* am = s.acc + (size_t)(part * Pj + base - m) * R;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const C E = part ? Eb[r] : Ea[r], O = part ? Ob[r] : Oa[r];
+                    ap[r] = ap[r] + conjg(e) * (E + O);
+                    if (m > 0) am[r] = am[r] + e * (pn * (E - O));
+                }
+            }
+        }
+        next(tid);
+    }
+    __syncthreads();
+}
+
+}  // namespace
+
+template <class C, int R>
+__global__ void __launch_bounds__(kThreads, 1) k_direct_block(BlockArgs ba, DirectBucket bk) {
+    extern __shared__ __align__(16) double smem_d[];
+    const DirectArgs& a = ba.d;
+    const SceneView& sc = a.sc;
+    const int pp = bk.pp;
+    const C* stab = stab_of(a, (C*)nullptr);
+    const bool tabs = stab != nullptr;
+    const Bufs<C> s = carve_block<C, R>(smem_d, pp, tabs);
+    const int tile = blockIdx.x;
+    const int j = bk.targets[blockIdx.y];
+    if (!sc.couple[j]) return;
+    const int r0 = tile * R;
+    const int rc = min(R, ba.nrhs - r0);
+    const int tid = threadIdx.x;
+    const int pj = sc.p[j];
+    const int Pj = pj * (pj + 2);
+    const int SP = pp * (pp + 3);
+    const int XP = pp * (pp + 2);
+    const PairCtx<C> ctx{s, delta_of(a, (C*)nullptr), a.dt, a.g, a.z, pp, SP, XP, tabs};
+    for (int t = tid; t < 2 * Pj * R; t += kThreads) s.acc[t] = C{0, 0};
+    for (int t = tid; t < pp * (pp + 3) / 2; t += kThreads) {
+        int n, k;
+        decode_nk(t, n, k);
+        s.nk[t] = make_short2((short)n, (short)k);
+    }
+    auto block = [&](int l) -> const C* {
+        return tabs ? stab + a.pt.pair_off[pair_index(min(j, l), max(j, l), sc.n)] : nullptr;
+    };
+    auto disp = [&](int l) {
+        return Disp{sc.centres + 3 * (size_t)j, sc.centres + 3 * (size_t)l, sc.k, 1.0, {0.0, 0.0, 0.0}};
+    };
+    const cplx* X = ba.x + (size_t)r0 * ba.ld;
+    int i = 0;
+    if (i < bk.nsources && bk.sources[i] == j) ++i;
+    if (i < bk.nsources) {
+        const int l = bk.sources[i];
+        prep_pair(s, disp(l), a.z, block(l), pj, sc.p[l], pp, 0, tid, !tabs);
+    }
+    __syncthreads();
+    int cur = 0;
+    while (i < bk.nsources) {
+        const int l = bk.sources[i];
+        int inext = i + 1;
+        if (inext < bk.nsources && bk.sources[inext] == j) ++inext;
+        run_pair_block<C, R>(ctx, tid, pj, sc.p[l], X + sc.off[l], ba.ld, rc, block(l), cur, [&](int t) {
+            if (inext < bk.nsources) {
+                const int ln = bk.sources[inext];
+                prep_pair(s, disp(ln), a.z, block(ln), pj, sc.p[ln], pp, cur ^ 1, t, !tabs);
+            }
+        });
+        cur ^= 1;
+        i = inext;
+    }
+    // y += T sum, T = diag(a_n, b_n) of the target
+    cplx* Y = ba.y + (size_t)r0 * ba.ld + sc.off[j];
+    for (int t = tid; t < 2 * Pj; t += kThreads) {
+        const int tt = t < Pj ? t : t - Pj;
+        int n, m;
+        decode_nm(tt, n, m);
+        const cplx tm = (t < Pj) ? sc.an[(size_t)j * sc.pmax + n - 1] : sc.bn[(size_t)j * sc.pmax + n - 1];
+        const C* av = s.acc + (size_t)t * R;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (r < rc) {
+                cplx* yp = Y + (size_t)r * ba.ld + t;
+                *yp = *yp + tm * mk(av[r].x, av[r].y);
+            }
+    }
+}
+
+size_t block_smem_bytes(int pp, bool tabs, bool fp32, int R) {
+    if (fp32) {
+        switch (R) {
+            case 1: return smem_bytes_block<cplxf, 1>(pp, tabs);
+            case 2: return smem_bytes_block<cplxf, 2>(pp, tabs);
+            case 4: return smem_bytes_block<cplxf, 4>(pp, tabs);
+            case 8: return smem_bytes_block<cplxf, 8>(pp, tabs);
+        }
+    } else {
+        switch (R) {
+            case 1: return smem_bytes_block<cplx, 1>(pp, tabs);
+            case 2: return smem_bytes_block<cplx, 2>(pp, tabs);
+            case 4: return smem_bytes_block<cplx, 4>(pp, tabs);
+        }
+    }
+    return 0;
+}
+
+template <class C, int R>
+static void launch_block_t(const BlockArgs& a, const DirectBucket& b, cudaStream_t s) {
+    const bool tabs = stab_of_host<C>(a.d) != nullptr;
+    const size_t smem = smem_bytes_block<C, R>(b.pp, tabs);
+    raise_smem_ceiling(reinterpret_cast<const void*>(k_direct_block<C, R>), smem);
+    dim3 grid((a.nrhs + R - 1) / R, b.ntargets);
+    k_direct_block<C, R><<<grid, kThreads, smem, s>>>(a, b);
+}
+
+bool launch_direct_block(const BlockArgs& a, const DirectBucket& b, int R, cudaStream_t s) {
+    if (a.d.fp32) {
+        switch (R) {
+            case 1: launch_block_t<cplxf, 1>(a, b, s); return true;
+            case 2: launch_block_t<cplxf, 2>(a, b, s); return true;
+            case 4: launch_block_t<cplxf, 4>(a, b, s); return true;
+            case 8: launch_block_t<cplxf, 8>(a, b, s); return true;
+        }
+    } else {
+        switch (R) {
+            case 1: launch_block_t<cplx, 1>(a, b, s); return true;
+            case 2: launch_block_t<cplx, 2>(a, b, s); return true;
+            case 4: launch_block_t<cplx, 4>(a, b, s); return true;
+        }
+    }
+    return false;
 }
 
 // y = x + T (sum of the slabs) for coupled spheres, y = x otherwise

@@ -329,6 +329,34 @@ module foggy_gpu_f
             type(c_ptr), value :: h, x, y       ! device pointers
             integer(c_int32_t) :: rc
         end function
+        function foggy_solve_block(h, nrhs, x0, x, mem, stats, cross_sections, iterations, backward_errors) &
+                result(rc) bind(c, name="foggy_solve_block")
+            import :: c_ptr, c_int32_t, foggy_stats
+            type(c_ptr), value :: h, x0, x, cross_sections, iterations, backward_errors
+            integer(c_int32_t), value :: nrhs, mem
+            type(foggy_stats), intent(out) :: stats
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_matvec_block(h, nrhs, precision, x, y, mem) result(rc) bind(c, name="foggy_matvec_block")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: h, x, y
+            integer(c_int32_t), value :: nrhs, precision, mem
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_fmm_lists(h, part, out, count) result(rc) bind(c, name="foggy_fmm_lists")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: h, out
+            integer(c_int32_t), value :: part
+            integer(c_int32_t), intent(out) :: count
+            integer(c_int32_t) :: rc
+        end function
+        function foggy_block_tiles(h, precision, nrhs, out, count) result(rc) bind(c, name="foggy_block_tiles")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: h, out
+            integer(c_int32_t), value :: precision, nrhs
+            integer(c_int32_t), intent(out) :: count
+            integer(c_int32_t) :: rc
+        end function
     end interface
 
     public :: foggy_default_params, foggy_create, foggy_destroy, foggy_set_spheres
@@ -340,7 +368,8 @@ module foggy_gpu_f
     public :: foggy_solve_rhs, foggy_server_start, foggy_server_submit, foggy_server_poll
     public :: foggy_server_cancel, foggy_server_release, foggy_server_stop, foggy_matvec_rhs
     public :: foggy_tree_parent, foggy_tree_children, foggy_tree_centre_of_box, foggy_tree_neighbours
-    public :: foggy_estimate_solve_bytes
+    public :: foggy_estimate_solve_bytes, foggy_solve_block, foggy_matvec_block, foggy_block_tiles
+    public :: foggy_fmm_lists
     public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
     public :: foggy_ms_get_backward_error, foggy_ms_destructor, foggy_ms_vector_length
 

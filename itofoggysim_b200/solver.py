@@ -181,6 +181,45 @@ class MultiSphereSolver:
             N.check(rc, self.h)
         return x.reshape(nrhs, self.n), cs.reshape(nrhs, 3), self.last_stats
 
+    def solve_block(self, x0=None, raise_on_error=True):
+        """All plane waves' right-hand sides in one block (foggy_solve_block): x of shape (nrhs, n),
+        cross-sections (nrhs, 3), per-right-hand-side iterations and backward errors, summed stats."""
+        nrhs = self.scene.n_waves
+        x = np.zeros(nrhs * self.n, np.complex128)
+        cs = np.zeros(3 * nrhs)
+        its = np.zeros(nrhs, np.int32)
+        be = np.zeros(nrhs)
+        st = N.FoggyStats()
+        x0p = None
+        if x0 is not None:
+            x0 = N.as_c128(np.asarray(x0).reshape(-1))
+            x0p = x0.ctypes.data
+        rc = self.L.foggy_solve_block(self.h, nrhs, x0p, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), cs.ctypes.data,
+                                      its.ctypes.data, be.ctypes.data)
+        self.last_stats = st.as_dict()
+        if raise_on_error:
+            N.check(rc, self.h)
+        return x.reshape(nrhs, self.n), cs.reshape(nrhs, 3), its, be, self.last_stats
+
+    def calculate_vector_b_block(self, X, precision=0):
+        """y_v = A x_v for the rows of X in one block application (foggy_matvec_block); precision 1
+        uses FP32 translation arithmetic."""
+        X = N.as_c128(np.asarray(X).reshape(-1))
+        nr = X.size // self.n
+        Y = np.zeros(nr * self.n, np.complex128)
+        N.check(self.L.foggy_matvec_block(self.h, nr, int(precision), X.ctypes.data, Y.ctypes.data,
+                                          N.FOGGY_MEM_HOST), self.h)
+        return Y.reshape(nr, self.n)
+
+    def block_tiles(self, nrhs, precision=0):
+        """(targets, sources, largest degree, right-hand sides per CTA) of each operator launch."""
+        cnt = C.c_int32(0)
+        N.check(self.L.foggy_block_tiles(self.h, int(precision), int(nrhs), None, C.byref(cnt)), self.h)
+        out = np.zeros(4 * cnt.value, np.int32)
+        N.check(self.L.foggy_block_tiles(self.h, int(precision), int(nrhs), N.ptr(out, C.c_int32), C.byref(cnt)),
+                self.h)
+        return out.reshape(-1, 4)
+
     def solve_device(self, x_ptr, x0_ptr=None):
         st = N.FoggyStats()
         rc = self.L.foggy_solve(self.h, C.c_void_p(x0_ptr) if x0_ptr else None, C.c_void_p(x_ptr),

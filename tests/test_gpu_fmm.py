@@ -54,6 +54,69 @@ def test_tree_lists_match_oracle(native, oracle):
                     assert np.array_equal(got, ref), (l, n, kind)
 
 
+def _fmm_lists(s):
+    import ctypes as C
+    from itofoggysim_b200 import _native
+    parts = []
+    for part in range(12):
+        cnt = C.c_int32(0)
+        _native.check(s.L.foggy_fmm_lists(s.h, part, None, C.byref(cnt)), s.h)
+        out = np.zeros(max(cnt.value, 1), np.int32)
+        _native.check(s.L.foggy_fmm_lists(s.h, part, _native.ptr(out, C.c_int32), C.byref(cnt)), s.h)
+        parts.append(out[:cnt.value])
+    return parts
+
+
+def _csr(lists):
+    ptr = np.concatenate([[0], np.cumsum([len(v) for v in lists])]).astype(np.int32)
+    idx = np.array([i for v in lists for i in v], np.int32)
+    return ptr, idx
+
+
+@pytest.mark.parametrize("n,lmax,rule", [(40, 3, False), (300, 4, False), (24, 2, True), (1, 3, False)])
+def test_device_fmm_lists_match_oracle(native, oracle, n, lmax, rule):
+    """The ML-FMM's pass lists, built on the device from the sorted keys, against the lists that
+    follow from the oracle's hierarchy and domains (E1, E2, I4 of the reference's libtree)."""
+    sc = S.random_cluster(n, seed=50 + n, p=None if rule else 3, reference_row_rule=rule)
+    sc.tree_l_max = lmax
+    with solver.MultiSphereSolver(sc, use_ml_fmm=True) as s:
+        u, order, lmin, lmax_ = s.build_tree()
+        got = _fmm_lists(s)
+    assert lmax_ == lmax
+    uo, oo, lmino, lmaxo = oracle.build_tree(sc.centres, s=10, l_max=lmax)
+    lmin = min(lmino, lmax)
+    boxes = {l: np.unique(uo >> (3 * (lmax - l))) for l in range(lmin, lmax + 1)}
+    gid, base = {}, 0
+    for l in range(lmin, lmax + 1):
+        for k, b in enumerate(boxes[l]):
+            gid[(l, int(b))] = base + k
+        base += len(boxes[l])
+    leaves = [int(b) for b in boxes[lmax]]
+    p = sc.p_of_sphere()
+    couple = np.ones(n, bool) if not rule else (p >= sc.n_range[1])
+    e1 = {b: oracle.tree_domain(sc.centres, lmax, lmax, b, 1) for b in leaves}
+    e2 = {b: oracle.tree_domain(sc.centres, lmax, lmax, b, 2) for b in leaves}
+    leaf_of = {int(j): gid[(lmax, b)] for b in leaves for j in e1[b]}
+    ref = []
+    ref += _csr([[int(j) for j in e1[b] if couple[j]] for b in leaves])
+    kids, i4, par = [], [], []
+    for l in range(lmin, lmax + 1):
+        for b in boxes[l]:
+            b = int(b)
+            kids.append([gid[(l + 1, int(c))] for c in boxes.get(l + 1, []) if int(c) >> 3 == b])
+            cand = oracle.tree_domain(sc.centres, lmax, l, b, 4)
+            i4.append([gid[(l, int(c))] for c in cand if (l, int(c)) in gid])
+            par.append([gid[(l - 1, b >> 3)]] if l > lmin else [])
+    ref += _csr(kids) + _csr(i4) + _csr(par)
+    ref += _csr([[leaf_of[j]] for j in range(n)])
+    leaf_box = {gid[(lmax, b)]: b for b in leaves}
+    ref += _csr([[int(i) for i in e2[leaf_box[leaf_of[j]]] if i != j] for j in range(n)])
+    names = ["aggregation ptr", "aggregation idx", "children ptr", "children idx", "I4 ptr", "I4 idx",
+             "parent ptr", "parent idx", "box-to-sphere ptr", "box-to-sphere idx", "near ptr", "near idx"]
+    for k in range(12):
+        assert np.array_equal(got[k], ref[k]), names[k]
+
+
 CASES = [
     # n, p, z, convention, row rule, l_max
     (16, 3, 1, 0, True, 2),
