@@ -270,6 +270,43 @@ def cpu_sample(sc, budget_s=15.0, seed=0):
     return per_pair * N * (N - 1), done, elapsed
 
 
+def cpu_cached_sample():
+    """BASELINE.md's oracle-direct-cached mode: the oracle's operator with the translation blocks of
+    every ordered pair built once and kept (bit-identical to recomputing them), timed on all host cores
+    for the 64-sphere cluster, where the cache fits (4032 pairs x 2 blocks of 255^2 complex, 8.4 GB).  Returns seconds per cached application and the seconds the cache took to build."""
+    from oracle import oracle as O
+    from itofoggysim_b200 import scene as S
+    sc = S.small_cluster()
+    P = O.Problem(sc)
+    x = P.vector_b()
+    t0 = time.perf_counter()
+    P.matvec_rows(x, 0, sc.n_spheres, cache=True)
+    build = time.perf_counter() - t0
+    reps = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        P.matvec_rows(x, 0, sc.n_spheres, cache=True)
+        reps.append(time.perf_counter() - t0)
+    return float(np.median(reps)), build, sc
+
+
+def cached_scale(sc_from, sc_to):
+    """Ratio of the cached operator's work between two scenes: a cached application is one dense
+    (2 P_j x 2 P_l) block product per ordered pair, so its cost goes with sum_{j != l} P_j P_l."""
+    def w(sc):
+        p = sc.p_of_sphere().astype(np.float64)
+        P = p * (p + 2)
+        return float(P.sum() ** 2 - (P * P).sum())
+    return w(sc_to) / w(sc_from)
+
+
+def cached_bytes(sc):
+    """Bytes of every ordered pair's two translation blocks A, B: 2 x P_j P_l x 16."""
+    p = sc.p_of_sphere().astype(np.float64)
+    P = p * (p + 2)
+    return 32.0 * float(P.sum() ** 2 - (P * P).sum())
+
+
 def job_rate(local_ms, units, world, torch, dev, dist):
     """Whole-job rate of replicas: every rank processed `units` in local_ms of its own device
     time; the job's time is the slowest rank's, so rate = world * units / max over ranks.
@@ -405,6 +442,169 @@ def run_multi_rhs(args):
     print(json.dumps(line), flush=True)
 
 
+def block_scene(n_spheres):
+    """SURVEY config 4's scene shape at n_spheres: lognormal water spheres (median 0.6 um, sigma_ln 0.3,
+    clipped to 0.2-1.5 um) at config 4's number density (20,000 spheres in a 90 um cube), 64 Fibonacci
+    directions x TM/TE = 128 right-hand sides, GMRES(30) to 1e-6."""
+    from itofoggysim_b200 import scene as S
+    box = 90.0 * (n_spheres / 20000.0) ** (1.0 / 3.0)
+    sc = S.medium_cluster(seed=4, n=n_spheres, box=box)
+    return S.Scene(**{**sc.__dict__, **fibonacci_waves(64), "gmres_tolerance": 1e-6, "gmres_restart": 30,
+                      "tree_l_max": 0, "name": "lognormal_%d_rhs128" % n_spheres})
+
+
+def run_block(args):
+    """The 128 right-hand sides of one scene solved as one block in mixed precision
+    (foggy_solve_block: FP32 translation arithmetic in the Arnoldi steps, FP64 restart residuals,
+    every operator application shared by the block), against the plain FP64 path (one FP64 GMRES per
+    right-hand side, foggy_solve_rhs) on the same scene.  value = right-hand sides solved per second
+    (device time of the block solve); errors of every right-hand side against the FP64 solutions."""
+    import ctypes as C
+    import torch
+    from itofoggysim_b200 import _native as N, solver
+    dev = torch.device("cuda", 0)
+    sc = block_scene(args.spheres)
+    nrhs = sc.n_waves
+    # the plain FP64 path, one GMRES per right-hand side (the reference's one run per illumination)
+    with solver.MultiSphereSolver(sc) as s:
+        x64, cs64, st64 = s.solve_rhs()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    with solver.MultiSphereSolver(sc, precision=1) as s:
+        for _ in range(args.warmup):
+            s.solve_block()
+        torch.cuda.synchronize()
+        ms, launches, its = [], 0, []
+        with ClockSampler(0) as clk:
+            for _ in range(args.steps):
+                flush.zero_()
+                x, cs, it, be, st = s.solve_block()
+                ms.append(st["ms_total"])
+                launches += st["kernel_launches"]
+                its.append(int(it.sum()))
+            torch.cuda.synchronize()
+        tiles = s.block_tiles(nrhs, precision=1)
+        # the FP32 block operator alone on the 128 solutions (device buffers, CUDA events)
+        xd = torch.from_numpy(np.ascontiguousarray(x).reshape(-1).view(np.float64).copy()).to(dev)
+        yd = torch.empty_like(xd)
+        s.L.foggy_matvec_block(s.h, nrhs, 1, C.c_void_p(xd.data_ptr()), C.c_void_p(yd.data_ptr()), N.FOGGY_MEM_DEVICE)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        N.check(s.L.foggy_matvec_block(s.h, nrhs, 1, C.c_void_p(xd.data_ptr()), C.c_void_p(yd.data_ptr()),
+                                       N.FOGGY_MEM_DEVICE), s.h)
+        e1.record()
+        torch.cuda.synchronize()
+        t_op = e0.elapsed_time(e1)
+        del xd, yd
+    # end to end through the public API: scene from host memory, the block solve, solutions to host
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with solver.MultiSphereSolver(sc, precision=1) as s2:
+        xh, _, _, _, _ = s2.solve_block()
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    h2d = (sc.centres.nbytes + sc.param_index.nbytes + sc.refractive_index.nbytes + sc.radius.nbytes
+           + sc.n_range_param.nbytes + 6 * 8 * nrhs)
+    del flush
+    torch.cuda.empty_cache()
+    g = g_layout(sc)
+    rel = [float(np.linalg.norm((x[r] - x64[r]) / g) / np.linalg.norm(x64[r] / g)) for r in range(nrhs)]
+    cext = [float(abs(cs[r, 1] - cs64[r, 1]) / abs(cs64[r, 1])) for r in range(nrhs)]
+    peak = measure_fp32_peak(torch, dev)
+    flops = algorithmic_flops(sc) * nrhs
+    achieved = flops / (t_op * 1e-3) / 1e12
+    value = nrhs * len(ms) / (float(np.sum(ms)) * 1e-3)
+    plain = nrhs / (st64["ms_total"] * 1e-3)
+    p = sc.p_of_sphere()
+    line = {
+        "metric": METRIC, "value": value, "unit": "rhs solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": float(np.mean(ms)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 translations, f64 Krylov and residuals", "data": "synthetic",
+        "config": {"workload": sc.name, "spheres": sc.n_spheres, "p_max": int(p.max()), "p_median": float(np.median(p)),
+                   "rhs": nrhs, "gmres_restart": sc.gmres_restart, "gmres_tolerance": sc.gmres_tolerance,
+                   "solver": "batched GMRES, one Krylov space per right-hand side, block operator",
+                   "matvec": "direct (all pairs, rotation-axial-rotation), right-hand-side tiles per CTA",
+                   "l2": "Krylov block exceeds L2; 256 MB L2 flush between steps"},
+        "plain_fp64": {"rhs_per_s": plain, "ms_total": st64["ms_total"], "iterations": st64["iterations"],
+                       "solver": "foggy_solve_rhs: one FP64 GMRES per right-hand side"},
+        "speedup_vs_plain_fp64": value / plain,
+        "iterations_total": its[-1], "max_rel_coefficient_error": max(rel), "max_c_ext_rel_error": max(cext),
+        "tiles": {"fp32_per_launch": tiles[:, 3].tolist()},
+        "roofline": {"bound": "fp32", "compute": "FP32 CUDA-core pipe (packed fma.rn.f32x2); no tensor-core instruction",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "kernel": "k_direct_block<cplxf> (one block application of 128 vectors)",
+                     "flops_per_launch": flops, "ms_per_launch": t_op,
+                     "peak_source": "cuBLAS FP32 SGEMM 8192^3 (TF32 off) measured in this run"},
+        "e2e": {"value": nrhs / (e2e_ms * 1e-3), "unit": "rhs solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(xh.nbytes)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_operator(args):
+    """Operator applications alone, for timing and ncu captures: the lognormal scene of --spheres
+    (the 2000-sphere cube's volume fraction), --rhs vectors (the right-hand sides of its plane
+    wave), FP64 or FP32 translations (--precision), through foggy_matvec (one vector) or
+    foggy_matvec_block.  One untimed application builds the pair tables and tunes the tiles; the
+    CUDA profiler is started after it, so `ncu --profile-from-start off` captures the timed ones."""
+    import ctypes as C
+    import torch
+    from itofoggysim_b200 import _native as N, scene as S, solver
+    dev = torch.device("cuda", 0)
+    n = args.spheres
+    sc = S.medium_cluster(n=n, box=40.0 * (n / 2000.0) ** (1.0 / 3.0))
+    prec = 1 if args.precision == "mixed" else 0
+    with solver.MultiSphereSolver(sc, precision=prec) as s:
+        b = np.tile(s.get_vector_b(), (args.rhs, 1))
+        xd = torch.from_numpy(b.reshape(-1).view(np.float64).copy()).to(dev)
+        yd = torch.empty_like(xd)
+
+        def apply():
+            if args.rhs == 1 and prec == 0:
+                s.matvec_device(xd.data_ptr(), yd.data_ptr())
+            else:
+                N.check(s.L.foggy_matvec_block(s.h, args.rhs, prec, C.c_void_p(xd.data_ptr()),
+                                               C.c_void_p(yd.data_ptr()), N.FOGGY_MEM_DEVICE), s.h)
+
+        apply()
+        torch.cuda.synchronize()
+        if args.solve:
+            # one GMRES(50) solve to 1e-8 instead (mixed precision: FP32 operator in the Arnoldi steps)
+            s.set_restart(50)
+            s.set_tolerance(1e-8)
+            torch.cuda.profiler.start()
+            _, st = s.solve()
+            torch.cuda.profiler.stop()
+            print(json.dumps({"workload": "operator", "spheres": n, "solve": args.precision,
+                              "ms_total": st["ms_total"], "iterations": st["iterations"],
+                              "backward_error": st["backward_error"]}), flush=True)
+            return
+        torch.cuda.profiler.start()
+        out = []
+        for _ in range(args.applications):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            apply()
+            e1.record()
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1))
+        torch.cuda.profiler.stop()
+    flops = algorithmic_flops(sc) * args.rhs
+    print(json.dumps({"workload": "operator", "spheres": n, "rhs": args.rhs, "precision": args.precision,
+                      "ms_per_application": out, "ms_per_rhs": float(np.mean(out)) / args.rhs,
+                      "tflops": flops / (float(np.mean(out)) * 1e-3) / 1e12}), flush=True)
+
+
+def g_layout(sc):
+    g = np.array([math.sqrt(math.factorial(n + m) / math.factorial(n - m))
+                  for n in range(1, sc.n_range[1] + 1) for m in range(-n, n + 1)])
+    return np.tile(np.concatenate([g, g]), sc.n_spheres)
+
+
 def run_mixed(args):
     """The workload solved with the FP32 operator in the Arnoldi steps and FP64 true residuals
     (the 2000-sphere lognormal scene); value = solves/s (device time), with the relative error
@@ -496,8 +696,14 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="medium", choices=["medium", "small", "serving", "multi_rhs"],
-                    help="serving: a request stream through the solve server (its own JSON line)")
+    ap.add_argument("--workload", default="medium", choices=["medium", "small", "serving", "multi_rhs", "block",
+                                                             "operator"],
+                    help="serving: a request stream through the solve server; block: 128 right-hand sides of "
+                         "one lognormal scene as one mixed-precision block (their own JSON lines)")
+    ap.add_argument("--spheres", type=int, default=500, help="spheres of the block and operator workloads' scenes")
+    ap.add_argument("--rhs", type=int, default=1, help="vectors per application of the operator workload")
+    ap.add_argument("--applications", type=int, default=2, help="timed applications of the operator workload")
+    ap.add_argument("--solve", action="store_true", help="operator workload: one GMRES solve instead")
     ap.add_argument("--concurrent", type=int, default=3, help="co-resident requests of the serving workload")
     ap.add_argument("--operator", default="direct", choices=["direct", "mlfmm"],
                     help="mlfmm: the ML-FMM passes (fmm_convention below) instead of all pairs")
@@ -505,6 +711,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU sampling")
     ap.add_argument("--matvecs-per-solve", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-cached", action="store_true",
+                    help="also time the oracle with cached translation blocks (about a minute of CPU)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 Arnoldi operator, FP64 true residuals (its own JSON line, with errors "
                          "against an FP64 solve)")
@@ -514,7 +722,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
-    if args.precision == "mixed":
+    if args.precision == "mixed" and args.workload not in ("operator", "block"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no mixed-precision solve"}),
                   flush=True)
@@ -528,6 +736,21 @@ def main():
                   flush=True)
         elif rank == 0:
             run_multi_rhs(args)
+        return
+
+    if args.workload == "operator":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "operator timing mode of the GPU arm"}), flush=True)
+        elif rank == 0:
+            run_operator(args)
+        return
+
+    if args.workload == "block":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "CPU reference arm times the single-RHS workloads"}),
+                  flush=True)
+        elif rank == 0:
+            run_block(args)
         return
 
     if args.workload == "serving":
@@ -655,6 +878,16 @@ def main():
                 "sample": "%d random sphere pairs (%.1f s), exact Xu translations recomputed per pair as the "
                           "reference does, extrapolated x N(N-1) pairs x %d matvecs/solve"
                           % (pairs, el, mv_count // args.steps)}
+        if args.cpu_cached:
+            t_c, t_build, sc_small = cpu_cached_sample()
+            per_solve_c = t_c * cached_scale(sc_small, sc) * (mv_count / args.steps)
+            result["cpu_baseline_cached"] = {
+                "value": 1.0 / per_solve_c, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                "sample": "oracle operator with every pair's translation blocks cached (BASELINE.md "
+                          "oracle-direct-cached), %.3f s per application of the 64-sphere cluster (cache built in "
+                          "%.1f s), scaled by sum_{j!=l} P_j P_l to this scene and x %d matvecs/solve; this "
+                          "scene's cache (two P_j x P_l complex blocks per ordered pair) would need "
+                          "%.0f TB" % (t_c, t_build, mv_count // args.steps, cached_bytes(sc) / 1e12)}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

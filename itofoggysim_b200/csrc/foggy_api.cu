@@ -1714,6 +1714,18 @@ int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_in
     if (table_bytes_out) *table_bytes_out = tb;
     return bytes + (pair_tables == 1 ? tb : 0);
 }
+
+int64_t estimate_block_bytes(const foggy_params& prm, int N, const int* param_index, int NP, const int* n_range,
+                             int nrhs) {
+    const int pg = prm.n_range[1];
+    int64_t n_unk = 0;
+    for (int j = 0; j < N; ++j) {
+        const int p = std::max(1, std::min(n_range[2 * param_index[j] + 1], pg));
+        n_unk += 2 * (int64_t)p * (p + 2);
+    }
+    const int64_t m = prm.gmres_restart, v = (int64_t)sizeof(cplx);
+    return (m + 5) * nrhs * n_unk * v + nrhs * ((m + 1) * (m + 5 + kRedBlocks) * v + (m + 5 + kRedBlocks) * 8 + 12);
+}
 }  // namespace foggy
 
 extern "C" {
@@ -2109,7 +2121,7 @@ int smem_optin(int device) {
 
 std::vector<int> tile_candidates(bool fp32, int pp, bool tabs, int nrhs, int smem_max) {
     std::vector<int> out;
-    const std::vector<int> all = fp32 ? std::vector<int>{1, 2, 4, 8} : std::vector<int>{1, 2, 4};
+    const std::vector<int> all = fp32 ? std::vector<int>{1, 2, 4, 8, 16} : std::vector<int>{1, 2, 4, 8};
     for (int R : all) {
         if (R > 1 && R / 2 >= nrhs) break;   // a tile wider than the block would idle
         if (block_smem_bytes(pp, tabs, fp32, R) <= (size_t)smem_max) out.push_back(R);
@@ -2120,11 +2132,11 @@ std::vector<int> tile_candidates(bool fp32, int pp, bool tabs, int nrhs, int sme
 auto tile_key(const BlockArgs& ba, const DirectBucket& b, bool tabs) {
     int lt = 0;
     while ((1 << (lt + 1)) <= b.ntargets) ++lt;
-    return std::make_tuple(ba.d.fp32, (int)tabs, b.pp, lt, std::min(ba.nrhs, 8));
+    return std::make_tuple(ba.d.fp32, (int)tabs, b.pp, lt, std::min(ba.nrhs, 16));
 }
 
 // The autotuner: every candidate width runs the launch's first 296 targets (two CTAs per SM)
-// against its first 48 sources for min(nrhs, 8) vectors into a scratch output, once to warm up
+// against its first 48 sources for min(nrhs, 16) vectors into a scratch output, once to warm up
 // and once timed; the fastest wins.
 int choose_tile(foggy_handle h, const BlockArgs& ba, const DirectBucket& b, bool tabs, int* R_out) {
     const auto key = tile_key(ba, b, tabs);
@@ -2140,7 +2152,7 @@ int choose_tile(foggy_handle h, const BlockArgs& ba, const DirectBucket& b, bool
     if (cand.empty()) return fail(h, FOGGY_ERR_UNSUPPORTED, "no tile width of the block operator fits this degree");
     int best = cand[0];
     if (cand.size() > 1) {
-        const int nrt = std::min(ba.nrhs, 8);
+        const int nrt = std::min(ba.nrhs, 16);
         cplx* scratch = nullptr;
         CK(h, cudaMalloc(&scratch, (size_t)nrt * h->n_unk * sizeof(cplx)));
         BlockArgs bt = ba;
@@ -2591,9 +2603,9 @@ int32_t foggy_block_tiles(foggy_handle h, int32_t precision, int32_t nrhs, int32
     *count = (int)h->launches_direct.size();
     if (!out) return FOGGY_OK;
     TRY(ensure_pair_tables(h));
-    // the tuner reads the first min(nrhs, 8) vectors of the block: zeros serve
+    // the tuner reads the first min(nrhs, 16) vectors of the block: zeros serve
     cplx* X = nullptr;
-    const int nrt = std::min(nrhs, 8);
+    const int nrt = std::min(nrhs, 16);
     TRY(dalloc(h, &X, (size_t)nrt * h->n_unk));
     CK(h, cudaMemsetAsync(X, 0, (size_t)nrt * h->n_unk * sizeof(cplx), h->stream));
     BlockArgs ba = block_args(h, X, nullptr, nrhs, precision == 1);

@@ -36,6 +36,10 @@ void raise_smem_ceiling(const void* func, size_t bytes);
 // *table_bytes either way)
 int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_index, int NP, const int* n_range,
                              int pair_tables, int64_t* table_bytes);
+// device bytes foggy_solve_block adds for a block of nrhs right-hand sides (its Krylov block,
+// iterates, residuals and small arrays)
+int64_t estimate_block_bytes(const foggy_params& prm, int N, const int* param_index, int NP, const int* n_range,
+                             int nrhs);
 
 // ---- host: octree box arithmetic (fmm_tree.cpp) ----------------------------------------------
 // Level bounds of the ML-FMM's boxes (built on the device): levels l_min..l_max, boxes with a

@@ -126,7 +126,7 @@ struct BlockArgs {
 };
 // shared memory of one CTA of the several-right-hand-side operator with R vectors per CTA
 size_t block_smem_bytes(int pp, bool tabs, bool fp32, int R);
-// false when R is not one of the built tile widths (FP32: 1, 2, 4, 8; FP64: 1, 2, 4)
+// false when R is not one of the built tile widths (FP32: 1, 2, 4, 8, 16; FP64: 1, 2, 4, 8)
 bool launch_direct_block(const BlockArgs& a, const DirectBucket& b, int R, cudaStream_t s);
 size_t translation_pair_smem_bytes(int pmax);
 void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s);

@@ -125,6 +125,11 @@ __device__ inline Bufs<C> carve(double* base, int pp, bool tabs) {
     return s;
 }
 
+// Packed FP32 (Blackwell fma.rn.f32x2): both components of a complex accumulator in one FMA.
+__device__ __forceinline__ float2 f2(cplxf c) { return make_float2(c.x, c.y); }
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 bcast(float q) { return make_float2(q, q); }
+
 // r += s w in two fused multiply-adds per component
 template <class C>
 __device__ __forceinline__ void cmac(real_of<C>& rx, real_of<C>& ry, C s, C w) {
@@ -133,6 +138,45 @@ __device__ __forceinline__ void cmac(real_of<C>& rx, real_of<C>& ry, C s, C w) {
     ry = fma(s.x, w.y, ry);
     ry = fma(s.y, w.x, ry);
 }
+
+// sum over mu of S(k; n, mu) w_i(mu) for the four planes i of the coaxial stage (a', b' at +k and
+// -k).  FP64: four complex MACs per S entry.  FP32: with P_i = sum Re(S) w_i and Q_i = sum Im(S) w_i
+// in packed registers, two fma.rn.f32x2 per plane, and S w_i = (P_i.x - Q_i.y, P_i.y + Q_i.x).
+template <class C>
+struct Mac4;
+template <>
+struct Mac4<cplx> {
+    double r0x = 0, r0y = 0, r1x = 0, r1y = 0, r2x = 0, r2y = 0, r3x = 0, r3y = 0;
+    __device__ __forceinline__ void add(cplx S, cplx w0, cplx w1, cplx w2, cplx w3) {
+        cmac(r0x, r0y, S, w0);
+        cmac(r1x, r1y, S, w1);
+        cmac(r2x, r2y, S, w2);
+        cmac(r3x, r3y, S, w3);
+    }
+    __device__ __forceinline__ cplx get(int i) const {
+        return i == 0 ? cplx{r0x, r0y} : i == 1 ? cplx{r1x, r1y} : i == 2 ? cplx{r2x, r2y} : cplx{r3x, r3y};
+    }
+};
+template <>
+struct Mac4<cplxf> {
+    float2 P[4], Q[4];
+    __device__ __forceinline__ Mac4() {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) P[i] = Q[i] = make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ void add(cplxf S, cplxf w0, cplxf w1, cplxf w2, cplxf w3) {
+        const float2 sx = bcast(S.x), sy = bcast(S.y);
+        P[0] = ffma2(sx, f2(w0), P[0]);
+        Q[0] = ffma2(sy, f2(w0), Q[0]);
+        P[1] = ffma2(sx, f2(w1), P[1]);
+        Q[1] = ffma2(sy, f2(w1), Q[1]);
+        P[2] = ffma2(sx, f2(w2), P[2]);
+        Q[2] = ffma2(sy, f2(w2), Q[2]);
+        P[3] = ffma2(sx, f2(w3), P[3]);
+        Q[3] = ffma2(sy, f2(w3), Q[3]);
+    }
+    __device__ __forceinline__ cplxf get(int i) const { return cplxf{P[i].x - Q[i].y, P[i].y + Q[i].x}; }
+};
 
 // Where a translation points: t = k (sign (c_src - c_tgt) + shift).  The direct operator uses
 // sign = 1, shift = 0 (t = k (d_l - d_j), the reference's d_j_l); the ML-FMM passes follow the
@@ -203,10 +247,41 @@ __device__ inline void prep_pair(const Bufs<C>& s, const Disp& g, int z, const C
     if (e4) s.rho[b] = r;
 }
 
+// The FP32 Delta sums with packed FMAs: each real table entry scales a complex value, so one
+// fma.rn.f32x2 does the two real multiply-adds of the scalar form (same roundings, half the
+// instructions).  u[a STRIDE] for a = 0..amax.
+template <int STRIDE>
+__device__ __forceinline__ void delta_sum_f2(const float* __restrict__ Q, int j, int o, int amax, const cplxf* ua,
+                                             const cplxf* ub, cplxf& Ea, cplxf& Oa, cplxf& Eb, cplxf& Ob) {
+    float2 ea = make_float2(0.f, 0.f), oa = ea, eb = ea, ob = ea;
+    const int st = j + 1;
+    int a = 0;
+    for (; a + 1 <= amax; a += 2) {
+        const float2 q0 = bcast(__ldg(Q + a * st + o));
+        const float2 q1 = bcast(__ldg(Q + (a + 1) * st + o));
+        ea = ffma2(q0, f2(ua[a * STRIDE]), ea);
+        oa = ffma2(q1, f2(ua[(a + 1) * STRIDE]), oa);
+        eb = ffma2(q0, f2(ub[a * STRIDE]), eb);
+        ob = ffma2(q1, f2(ub[(a + 1) * STRIDE]), ob);
+    }
+    if (a <= amax) {
+        const float2 q0 = bcast(__ldg(Q + a * st + o));
+        ea = ffma2(q0, f2(ua[a * STRIDE]), ea);
+        eb = ffma2(q0, f2(ub[a * STRIDE]), eb);
+    }
+    Ea = cplxf{ea.x, ea.y};
+    Oa = cplxf{oa.x, oa.y};
+    Eb = cplxf{eb.x, eb.y};
+    Ob = cplxf{ob.x, ob.y};
+}
+
 // E = sum over even a, O = sum over odd a of Q[a (j+1) + o] u[a], a = 0..amax, for the two parts
 template <class C>
 __device__ __forceinline__ void delta_sum(const real_of<C>* __restrict__ Q, int j, int o, int amax, const C* ua,
                                           const C* ub, C& Ea, C& Oa, C& Eb, C& Ob) {
+    if constexpr (sizeof(C) == 8) {
+        delta_sum_f2<1>(Q, j, o, amax, ua, ub, Ea, Oa, Eb, Ob);
+    } else {
     using R = real_of<C>;
     R eax = 0, eay = 0, oax = 0, oay = 0, ebx = 0, eby = 0, obx = 0, oby = 0;
     const int st = j + 1;
@@ -236,6 +311,7 @@ __device__ __forceinline__ void delta_sum(const real_of<C>* __restrict__ Q, int 
     Oa = C{oax, oay};
     Eb = C{ebx, eby};
     Ob = C{obx, oby};
+    }
 }
 
 // stages 2 and 6: W = Delta u at +-s, times e^{-+i s theta}; stored folded for the transposed
@@ -431,67 +507,117 @@ __device__ inline void run_pair(const PairCtx<C>& c, int tid, int pj, int pl, co
             const int n = max(1, k) + rem;
             const C* w = s.B + (k * (pl + 2) - k * (k - 1) / 2);
             const int cnt = pl + 2 - k;
-            R r0x = 0, r0y = 0, r1x = 0, r1y = 0, r2x = 0, r2y = 0, r3x = 0, r3y = 0;
-            if (tabs) {
-                const int Wk = M2 - k;
-                const V2* sp = reinterpret_cast<const V2*>(pair_s + pair_block_offset(k, M2, M2) + (n - k));
-                // kPrefetch5 coaxial entries in flight per thread: the rows come from L2, so the loop
-                // is bounded by how many loads overlap, not by the multiply-adds
-                int q = 0;
-                for (; q + kPrefetch5 <= cnt; q += kPrefetch5) {
-                    V2 sv[kPrefetch5];
-#pragma unroll
-                    for (int u = 0; u < kPrefetch5; ++u) sv[u] = __ldcg(sp + (q + u) * Wk);
-#pragma unroll
-                    for (int u = 0; u < kPrefetch5; ++u) {
-                        const C S = C{sv[u].x, sv[u].y};
-                        cmac(r0x, r0y, S, w[q + u]);
-                        cmac(r1x, r1y, S, w[NW + q + u]);
-                        cmac(r2x, r2y, S, w[2 * NW + q + u]);
-                        cmac(r3x, r3y, S, w[3 * NW + q + u]);
+            // FP32: packed FMAs (Mac4); FP64: four scalar complex MACs per S entry
+            C a0, a1, a2, a3;
+            if constexpr (sizeof(C) == 8) {
+                Mac4<C> acc;
+                if (tabs) {
+                    const int Wk = M2 - k;
+                    const V2* sp = reinterpret_cast<const V2*>(pair_s + pair_block_offset(k, M2, M2) + (n - k));
+                    // kPrefetch5 coaxial entries in flight per thread: the rows come from L2, so the loop
+                    // is bounded by how many loads overlap, not by the multiply-adds
+                    int q = 0;
+                    for (; q + kPrefetch5 <= cnt; q += kPrefetch5) {
+                        V2 sv[kPrefetch5];
+    #pragma unroll
+                        for (int u = 0; u < kPrefetch5; ++u) sv[u] = __ldcg(sp + (q + u) * Wk);
+    #pragma unroll
+                        for (int u = 0; u < kPrefetch5; ++u)
+                            acc.add(C{sv[u].x, sv[u].y}, w[q + u], w[NW + q + u], w[2 * NW + q + u], w[3 * NW + q + u]);
+                    }
+                    for (; q < cnt; ++q) {
+                        const V2 sv = __ldcg(sp + q * Wk);
+                        acc.add(C{sv.x, sv.y}, w[q], w[NW + q], w[2 * NW + q], w[3 * NW + q]);
+                    }
+                } else {
+                    const int W = c.g.NM - k + 1;
+                    const size_t plane = (size_t)W * W;
+                    const double* G = c.g.gs + c.g.koff[k] + (n - k);
+                    for (int q = 0; q < cnt; ++q) {
+                        const int mu = k + q;
+                        const double* gp = G + (size_t)(mu - k) * W;
+                        const int qm = min(n, mu);
+                        int p = n + mu;
+                        double sx = 0.0, sy = 0.0;
+                        for (int qq = 0; qq <= qm; ++qq, p -= 2) {
+                            const double gq = __ldg(gp + qq * plane);
+                            sx += gq * s.zeta[p].x;
+                            sy += gq * s.zeta[p].y;
+                        }
+                        acc.add(cm<C>(sx, sy), w[q], w[NW + q], w[2 * NW + q], w[3 * NW + q]);
                     }
                 }
-                for (; q < cnt; ++q) {
-                    const V2 sv = __ldcg(sp + q * Wk);
-                    const C S = C{sv.x, sv.y};
-                    cmac(r0x, r0y, S, w[q]);
-                    cmac(r1x, r1y, S, w[NW + q]);
-                    cmac(r2x, r2y, S, w[2 * NW + q]);
-                    cmac(r3x, r3y, S, w[3 * NW + q]);
-                }
+                a0 = acc.get(0);
+                a1 = acc.get(1);
+                a2 = acc.get(2);
+                a3 = acc.get(3);
             } else {
-                const int W = c.g.NM - k + 1;
-                const size_t plane = (size_t)W * W;
-                const double* G = c.g.gs + c.g.koff[k] + (n - k);
-                for (int q = 0; q < cnt; ++q) {
-                    const int mu = k + q;
-                    const double* gp = G + (size_t)(mu - k) * W;
-                    const int qm = min(n, mu);
-                    int p = n + mu;
-                    double sx = 0.0, sy = 0.0;
-                    for (int qq = 0; qq <= qm; ++qq, p -= 2) {
-                        const double gq = __ldg(gp + qq * plane);
-                        sx += gq * s.zeta[p].x;
-                        sy += gq * s.zeta[p].y;
+                R r0x = 0, r0y = 0, r1x = 0, r1y = 0, r2x = 0, r2y = 0, r3x = 0, r3y = 0;
+                if (tabs) {
+                    const int Wk = M2 - k;
+                    const V2* sp = reinterpret_cast<const V2*>(pair_s + pair_block_offset(k, M2, M2) + (n - k));
+                    // kPrefetch5 coaxial entries in flight per thread: the rows come from L2, so the loop
+                    // is bounded by how many loads overlap, not by the multiply-adds
+                    int q = 0;
+                    for (; q + kPrefetch5 <= cnt; q += kPrefetch5) {
+                        V2 sv[kPrefetch5];
+    #pragma unroll
+                        for (int u = 0; u < kPrefetch5; ++u) sv[u] = __ldcg(sp + (q + u) * Wk);
+    #pragma unroll
+                        for (int u = 0; u < kPrefetch5; ++u) {
+                            const C S = C{sv[u].x, sv[u].y};
+                            cmac(r0x, r0y, S, w[q + u]);
+                            cmac(r1x, r1y, S, w[NW + q + u]);
+                            cmac(r2x, r2y, S, w[2 * NW + q + u]);
+                            cmac(r3x, r3y, S, w[3 * NW + q + u]);
+                        }
                     }
-                    const C S = cm<C>(sx, sy);
-                    cmac(r0x, r0y, S, w[q]);
-                    cmac(r1x, r1y, S, w[NW + q]);
-                    cmac(r2x, r2y, S, w[2 * NW + q]);
-                    cmac(r3x, r3y, S, w[3 * NW + q]);
+                    for (; q < cnt; ++q) {
+                        const V2 sv = __ldcg(sp + q * Wk);
+                        const C S = C{sv.x, sv.y};
+                        cmac(r0x, r0y, S, w[q]);
+                        cmac(r1x, r1y, S, w[NW + q]);
+                        cmac(r2x, r2y, S, w[2 * NW + q]);
+                        cmac(r3x, r3y, S, w[3 * NW + q]);
+                    }
+                } else {
+                    const int W = c.g.NM - k + 1;
+                    const size_t plane = (size_t)W * W;
+                    const double* G = c.g.gs + c.g.koff[k] + (n - k);
+                    for (int q = 0; q < cnt; ++q) {
+                        const int mu = k + q;
+                        const double* gp = G + (size_t)(mu - k) * W;
+                        const int qm = min(n, mu);
+                        int p = n + mu;
+                        double sx = 0.0, sy = 0.0;
+                        for (int qq = 0; qq <= qm; ++qq, p -= 2) {
+                            const double gq = __ldg(gp + qq * plane);
+                            sx += gq * s.zeta[p].x;
+                            sy += gq * s.zeta[p].y;
+                        }
+                        const C S = cm<C>(sx, sy);
+                        cmac(r0x, r0y, S, w[q]);
+                        cmac(r1x, r1y, S, w[NW + q]);
+                        cmac(r2x, r2y, S, w[2 * NW + q]);
+                        cmac(r3x, r3y, S, w[3 * NW + q]);
+                    }
                 }
+                a0 = C{r0x, r0y};
+                a1 = C{r1x, r1y};
+                a2 = C{r2x, r2y};
+                a3 = C{r3x, r3y};
             }
             const R f = sgn(k) / (2.0 * n * (n + 1.0));
             C* U = s.A + off2(n) + k;
             if (k == 0) {
-                U[0] = C{f * r0x, f * r0y};
+                U[0] = f * a0;
                 U[n + 1] = U[0];
-                U[SP] = C{f * r1x, f * r1y};
+                U[SP] = f * a1;
                 U[SP + n + 1] = U[SP];
             } else {
                 // u'_{+k} = i^{-k} y'(+k), u'_{-k} = i^{k} y'(-k)
-                const C ap = ipow_mul(-k, C{f * r0x, f * r0y}), am = ipow_mul(k, C{f * r2x, f * r2y});
-                const C bp = ipow_mul(-k, C{f * r1x, f * r1y}), bm = ipow_mul(k, C{f * r3x, f * r3y});
+                const C ap = ipow_mul(-k, f * a0), am = ipow_mul(k, f * a2);
+                const C bp = ipow_mul(-k, f * a1), bm = ipow_mul(k, f * a3);
                 U[0] = ap + am;
                 U[n + 1] = ap - am;
                 U[SP] = bp + bm;
@@ -768,10 +894,11 @@ void launch_translate(const TransArgs& a, int ntargets, cudaStream_t s) {
 // ---------------------------------------------------------------------------------------------
 // Several right-hand sides per CTA (the incidence directions and polarisations of one scene).
 //
-// The same seven stages as k_direct, but each item of a stage is computed for R right-hand
-// sides at once: every d(pi/2) entry, phase and coaxial coefficient S(k; n, mu) a thread reads is
-// applied to R vectors held in registers, and one set of barriers serves R translations.  The
-// shared buffers hold R values per entry, contiguous, so a thread's operands are vector loads.
+// The same seven stages as k_direct, each over (item, right-hand side) units with the right-hand
+// side fastest: the R lanes that share an item read its d(pi/2) entries, phases and coaxial
+// coefficients S(k; n, mu) once per warp instruction (one broadcast) and R consecutive values of
+// the shared buffers, which hold R values per entry; one set of barriers serves R translations,
+// and a thread's registers are those of the single-vector kernel.
 // One CTA owns one target sphere and one tile of R right-hand sides and walks all sources of a
 // bucket in order; at the end it adds T (a_n, b_n) times its sum onto y.  Launches of one
 // operator application run in order on one stream and each (target, tile) belongs to one CTA, so
@@ -803,109 +930,76 @@ __device__ inline Bufs<C> carve_block(double* base, int pp, bool tabs) {
     return s;
 }
 
-// R consecutive values from shared memory, with 16-byte loads where the size allows
+// E = sum over even a, O = sum over odd a of Q[a (j+1) + o] u[a R], for both parts: delta_sum
+// over one right-hand side of a buffer that holds R values per entry
 template <class C, int R>
-__device__ __forceinline__ void ldR(const C* p, C (&v)[R]) {
-    if constexpr (sizeof(C) == 16) {
-        const double2* q = reinterpret_cast<const double2*>(p);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const double2 d = q[r];
-            v[r] = C{d.x, d.y};
-        }
-    } else if constexpr (R % 2 == 0) {
-        const float4* q = reinterpret_cast<const float4*>(p);
-#pragma unroll
-        for (int i = 0; i < R / 2; ++i) {
-            const float4 f = q[i];
-            v[2 * i] = C{f.x, f.y};
-            v[2 * i + 1] = C{f.z, f.w};
-        }
-    } else {
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = p[r];
+__device__ __forceinline__ void delta_sum_r(const real_of<C>* __restrict__ Q, int j, int o, int amax, const C* ua,
+                                            const C* ub, C& Ea, C& Oa, C& Eb, C& Ob) {
+    if constexpr (sizeof(C) == 8) {
+        delta_sum_f2<R>(Q, j, o, amax, ua, ub, Ea, Oa, Eb, Ob);
+        return;
     }
-}
-
-// E = sum over even a, O = sum over odd a of Q[a (j+1) + o] u[a][r], for both parts and R vectors
-template <class C, int R>
-__device__ __forceinline__ void delta_sum_block(const real_of<C>* __restrict__ Q, int j, int o, int amax,
-                                                const C* ua, const C* ub, C (&Ea)[R], C (&Oa)[R], C (&Eb)[R],
-                                                C (&Ob)[R]) {
     using Rl = real_of<C>;
-#pragma unroll
-    for (int r = 0; r < R; ++r) Ea[r] = Oa[r] = Eb[r] = Ob[r] = C{0, 0};
+    Rl eax = 0, eay = 0, oax = 0, oay = 0, ebx = 0, eby = 0, obx = 0, oby = 0;
     const int st = j + 1;
     int a = 0;
     for (; a + 1 <= amax; a += 2) {
         const Rl q0 = __ldg(Q + a * st + o);
         const Rl q1 = __ldg(Q + (a + 1) * st + o);
-        C u0[R], u1[R];
-        ldR<C, R>(ua + a * R, u0);
-        ldR<C, R>(ua + (a + 1) * R, u1);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            Ea[r].x = fma(q0, u0[r].x, Ea[r].x);
-            Ea[r].y = fma(q0, u0[r].y, Ea[r].y);
-            Oa[r].x = fma(q1, u1[r].x, Oa[r].x);
-            Oa[r].y = fma(q1, u1[r].y, Oa[r].y);
-        }
-        ldR<C, R>(ub + a * R, u0);
-        ldR<C, R>(ub + (a + 1) * R, u1);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            Eb[r].x = fma(q0, u0[r].x, Eb[r].x);
-            Eb[r].y = fma(q0, u0[r].y, Eb[r].y);
-            Ob[r].x = fma(q1, u1[r].x, Ob[r].x);
-            Ob[r].y = fma(q1, u1[r].y, Ob[r].y);
-        }
+        const C u0 = ua[a * R], u1 = ua[(a + 1) * R], v0 = ub[a * R], v1 = ub[(a + 1) * R];
+        eax = fma(q0, u0.x, eax);
+        eay = fma(q0, u0.y, eay);
+        oax = fma(q1, u1.x, oax);
+        oay = fma(q1, u1.y, oay);
+        ebx = fma(q0, v0.x, ebx);
+        eby = fma(q0, v0.y, eby);
+        obx = fma(q1, v1.x, obx);
+        oby = fma(q1, v1.y, oby);
     }
     if (a <= amax) {
         const Rl q0 = __ldg(Q + a * st + o);
-        C u0[R], v0[R];
-        ldR<C, R>(ua + a * R, u0);
-        ldR<C, R>(ub + a * R, v0);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            Ea[r].x = fma(q0, u0[r].x, Ea[r].x);
-            Ea[r].y = fma(q0, u0[r].y, Ea[r].y);
-            Eb[r].x = fma(q0, v0[r].x, Eb[r].x);
-            Eb[r].y = fma(q0, v0[r].y, Eb[r].y);
-        }
+        const C u0 = ua[a * R], v0 = ub[a * R];
+        eax = fma(q0, u0.x, eax);
+        eay = fma(q0, u0.y, eay);
+        ebx = fma(q0, v0.x, ebx);
+        eby = fma(q0, v0.y, eby);
     }
+    Ea = C{eax, eay};
+    Oa = C{oax, oay};
+    Eb = C{ebx, eby};
+    Ob = C{obx, oby};
 }
 
-// stages 2 and 6 for R vectors (fwd_item with R values per entry)
+// stages 2 and 6 for right-hand side r of the block layout (fwd_item with stride R)
 template <class C, int R>
-__device__ __forceinline__ void fwd_item_block(const real_of<C>* delta, const C* src, C* dst, int SP, int j, int s_,
-                                               int amax, C eth) {
+__device__ __forceinline__ void fwd_item_r(const real_of<C>* delta, const C* src, C* dst, int SP, int j, int s_,
+                                           int amax, C eth, int r) {
     const int fold = ((j + s_) & 1) ? j + 1 : 0;
-    const C* ua = src + (size_t)(off2(j) + fold) * R;
-    C Ea[R], Oa[R], Eb[R], Ob[R];
-    delta_sum_block<C, R>(delta + qoff(j), j, s_, amax, ua, ua + (size_t)SP * R, Ea, Oa, Eb, Ob);
+    const C* ua = src + (size_t)(off2(j) + fold) * R + r;
+    C Ea, Oa, Eb, Ob;
+    delta_sum_r<C, R>(delta + qoff(j), j, s_, amax, ua, ua + (size_t)SP * R, Ea, Oa, Eb, Ob);
     const real_of<C> pj_ = sgn(j), ps = sgn(s_);
-    C* d = dst + (size_t)off2(j) * R;
+    C* d = dst + (size_t)off2(j) * R + r;
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
         C* dp = d + (size_t)part * SP * R;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const C E = part ? Eb[r] : Ea[r], O = part ? Ob[r] : Oa[r];
-            const C wp = eth * (E + O);
-            if (s_ == 0) {
-                dp[r] = wp;
-                dp[(j + 1) * R + r] = wp;
-            } else {
-                const C wm = conjg(eth) * (pj_ * (E - O));
-                dp[s_ * R + r] = ps * (wp + wm);
-                dp[(j + 1 + s_) * R + r] = ps * (wp - wm);
-            }
+        const C E = part ? Eb : Ea, O = part ? Ob : Oa;
+        const C wp = eth * (E + O);
+        if (s_ == 0) {
+            dp[0] = wp;
+            dp[(j + 1) * R] = wp;
+        } else {
+            const C wm = conjg(eth) * (pj_ * (E - O));
+            dp[s_ * R] = ps * (wp + wm);
+            dp[(j + 1 + s_) * R] = ps * (wp - wm);
         }
     }
 }
 
 // One translation (target degree pj <- source degree pl) for the R vectors xl + r ld (r < rc),
-// added into c.s.acc; stages as in run_pair.
+// added into c.s.acc.  The stages of run_pair, each over (item, right-hand side) units with the
+// right-hand side fastest: the R lanes of one item share its d(pi/2) entries, phases and coaxial
+// coefficients and read R consecutive values of each buffer.
 template <class C, int R, class Next>
 __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int pl, const cplx* __restrict__ xl,
                                       int64_t ld, int rc, const C* pair_s, int cur, Next next) {
@@ -919,15 +1013,14 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     const int Pl = pl * (pl + 2);
     if (s.rho[cur] == 0.0) {
         const int pm = min(pj, pl), Pm = pm * (pm + 2);
-        for (int t = tid; t < 2 * Pm; t += kThreads) {
+        for (int u = tid; u < 2 * Pm * R; u += kThreads) {
+            const int t = u / R, r = u % R;
             const int part = t >= Pm, e = t - part * Pm;
-            C* a = s.acc + (size_t)(part * Pj + e) * R;
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                if (r < rc) {
-                    const cplx v = xl[(size_t)r * ld + part * Pl + e];
-                    a[r] = a[r] + cm<C>(v.x, v.y);
-                }
+            if (r < rc) {
+                const cplx v = xl[(size_t)r * ld + part * Pl + e];
+                C& a = s.acc[(size_t)(part * Pj + e) * R + r];
+                a = a + cm<C>(v.x, v.y);
+            }
         }
         next(tid);
         __syncthreads();
@@ -939,36 +1032,34 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     // ---- 1. u = e^{i mu (phi + pi/2)} x, folded ------------------------------------------
     {
         const int items = pl * (pl + 3) / 2;
-        for (int t = tid; t < items; t += kThreads) {
+        for (int u = tid; u < items * R; u += kThreads) {
+            const int t = u / R, r = u % R;
             const short2 d_ = s.nk[t];
             const int nu = d_.x, mu = d_.y;
             const int base = nu * nu - 1 + nu;
             const C e = eps[mu];
-            C* U = s.A + (size_t)(off2(nu) + mu) * R;
+            C* U = s.A + (size_t)(off2(nu) + mu) * R + r;
             C* UB = U + (size_t)SP * R;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                double2 ap{0, 0}, am{0, 0}, bp{0, 0}, bm{0, 0};
-                if (r < rc) {
-                    const double2* xv = reinterpret_cast<const double2*>(xl + (size_t)r * ld + base);
-                    ap = __ldcg(xv + mu);
-                    am = __ldcg(xv - mu);
-                    bp = __ldcg(xv + Pl + mu);
-                    bm = __ldcg(xv + Pl - mu);
-                }
-                const C ua = e * cm<C>(ap.x, ap.y), ub = e * cm<C>(bp.x, bp.y);
-                if (mu == 0) {
-                    U[r] = ua;
-                    U[(nu + 1) * R + r] = ua;
-                    UB[r] = ub;
-                    UB[(nu + 1) * R + r] = ub;
-                } else {
-                    const C va = conjg(e) * cm<C>(am.x, am.y), vb = conjg(e) * cm<C>(bm.x, bm.y);
-                    U[r] = ua + va;
-                    U[(nu + 1) * R + r] = ua - va;
-                    UB[r] = ub + vb;
-                    UB[(nu + 1) * R + r] = ub - vb;
-                }
+            double2 ap{0, 0}, am{0, 0}, bp{0, 0}, bm{0, 0};
+            if (r < rc) {
+                const double2* xv = reinterpret_cast<const double2*>(xl + (size_t)r * ld + base);
+                ap = __ldcg(xv + mu);
+                am = __ldcg(xv - mu);
+                bp = __ldcg(xv + Pl + mu);
+                bm = __ldcg(xv + Pl - mu);
+            }
+            const C ua = e * cm<C>(ap.x, ap.y), ub = e * cm<C>(bp.x, bp.y);
+            if (mu == 0) {
+                U[0] = ua;
+                U[(nu + 1) * R] = ua;
+                UB[0] = ub;
+                UB[(nu + 1) * R] = ub;
+            } else {
+                const C va = conjg(e) * cm<C>(am.x, am.y), vb = conjg(e) * cm<C>(bm.x, bm.y);
+                U[0] = ua + va;
+                U[(nu + 1) * R] = ua - va;
+                UB[0] = ub + vb;
+                UB[(nu + 1) * R] = ub - vb;
             }
         }
         if (!tabs) {
@@ -985,34 +1076,33 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     // ---- 2. Delta u, e^{-i s theta} ----------------------------------------------------------
     {
         const int items = pl * (pl + 3) / 2;
-        for (int t = tid; t < items; t += kThreads) {
+        for (int u = tid; u < items * R; u += kThreads) {
+            const int t = u / R, r = u % R;
             const short2 d_ = s.nk[t];
-            fwd_item_block<C, R>(delta, s.A, s.B, SP, d_.x, d_.y, d_.x, eth[d_.y]);
+            fwd_item_r<C, R>(delta, s.A, s.B, SP, d_.x, d_.y, d_.x, eth[d_.y], r);
         }
     }
     __syncthreads();
     // ---- 3. Delta^T: x'(nu, +-k) = i^{+-k} T_{+-k}, stored times (2nu+1) ------------------
     {
         const int items = pl * (pl + 3) / 2;
-        for (int t = tid; t < items; t += kThreads) {
+        for (int u = tid; u < items * R; u += kThreads) {
+            const int t = u / R, r = u % R;
             const short2 d_ = s.nk[t];
             const int nu = d_.x, k = d_.y;
             const int fold = ((nu + k) & 1) ? nu + 1 : 0;
-            const C* va = s.B + (size_t)(off2(nu) + fold) * R;
-            C Ea[R], Oa[R], Eb[R], Ob[R];
-            delta_sum_block<C, R>(delta + qoff(nu), nu, k, nu, va, va + (size_t)SP * R, Ea, Oa, Eb, Ob);
+            const C* va = s.B + (size_t)(off2(nu) + fold) * R + r;
+            C Ea, Oa, Eb, Ob;
+            delta_sum_r<C, R>(delta + qoff(nu), nu, k, nu, va, va + (size_t)SP * R, Ea, Oa, Eb, Ob);
             const Rl f = 2.0 * nu + 1.0;
             const Rl pn = sgn(nu);
-            C* X = s.A + (size_t)(nu * nu - 1 + nu) * R;
+            C* X = s.A + (size_t)(nu * nu - 1 + nu) * R + r;
 #pragma unroll
             for (int part = 0; part < 2; ++part) {
                 C* Xp = X + (size_t)part * XP * R;
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const C E = part ? Eb[r] : Ea[r], O = part ? Ob[r] : Oa[r];
-                    Xp[k * R + r] = ipow_mul(k, f * (E + O));
-                    if (k > 0) Xp[-k * R + r] = ipow_mul(-k, (f * pn) * (E - O));
-                }
+                const C E = part ? Eb : Ea, O = part ? Ob : Oa;
+                Xp[k * R] = ipow_mul(k, f * (E + O));
+                if (k > 0) Xp[-k * R] = ipow_mul(-k, (f * pn) * (E - O));
             }
         }
     }
@@ -1022,7 +1112,8 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     {
         const double x = s.rho[cur];
         const int W = c.dt.K + 1;
-        for (int t = tid; t < NW; t += kThreads) {
+        for (int u = tid; u < NW * R; u += kThreads) {
+            const int t = u / R, r = u % R;
             int k = 0, rem = t;
             while (rem >= pl + 2 - k) {
                 rem -= pl + 2 - k;
@@ -1038,24 +1129,19 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
             for (int sg = 0; sg < 2; ++sg) {
                 const int kk = sg ? -k : k;
                 const Rl bs = sg ? -bk2 : bk2;
-                C* wa = s.B + ((size_t)(2 * sg) * NW + t) * R;
-                C* wb = s.B + ((size_t)(2 * sg + 1) * NW + t) * R;
+                C av[3], bv[3];
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    C av[3], bv[3];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        const int nu = mu - 1 + d;
-                        const bool ok = nu >= lo && nu <= pl;
-                        const int o = nu * nu - 1 + nu + kk;
-                        av[d] = ok ? s.A[(size_t)o * R + r] : C{0, 0};
-                        bv[d] = ok ? s.A[(size_t)(XP + o) * R + r] : C{0, 0};
-                    }
-                    const C ia = bs * bv[1] + c1m * av[0] - c2p * av[2];
-                    const C ib = bs * av[1] + c1m * bv[0] - c2p * bv[2];
-                    wa[r] = C{c0 * av[1].x - ia.y, c0 * av[1].y + ia.x};
-                    wb[r] = C{c0 * bv[1].x - ib.y, c0 * bv[1].y + ib.x};
+                for (int d = 0; d < 3; ++d) {
+                    const int nu = mu - 1 + d;
+                    const bool ok = nu >= lo && nu <= pl;
+                    const int o = nu * nu - 1 + nu + kk;
+                    av[d] = ok ? s.A[(size_t)o * R + r] : C{0, 0};
+                    bv[d] = ok ? s.A[(size_t)(XP + o) * R + r] : C{0, 0};
                 }
+                const C ia = bs * bv[1] + c1m * av[0] - c2p * av[2];
+                const C ib = bs * av[1] + c1m * bv[0] - c2p * bv[2];
+                s.B[((size_t)(2 * sg) * NW + t) * R + r] = C{c0 * av[1].x - ia.y, c0 * av[1].y + ia.x};
+                s.B[((size_t)(2 * sg + 1) * NW + t) * R + r] = C{c0 * bv[1].x - ib.y, c0 * bv[1].y + ib.x};
             }
         }
     }
@@ -1064,7 +1150,8 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     {
         const int rows_tot = pj + (kmax >= 1 ? kmax * pj - (kmax - 1) * kmax / 2 : 0);
         const int M2 = max(pj, pl) + 2;
-        for (int t = tid; t < rows_tot; t += kThreads) {
+        for (int u = tid; u < rows_tot * R; u += kThreads) {
+            const int t = u / R, r = u % R;
             int k = 0, rem = t;
             for (;;) {
                 const int rk = pj - max(1, k) + 1;
@@ -1073,22 +1160,34 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
                 ++k;
             }
             const int n = max(1, k) + rem;
-            const C* w = s.B + (size_t)(k * (pl + 2) - k * (k - 1) / 2) * R;
+            const C* w = s.B + (size_t)(k * (pl + 2) - k * (k - 1) / 2) * R + r;
+            const size_t NWR = (size_t)NW * R;
             const int cnt = pl + 2 - k;
-            C acc0[R], acc1[R], acc2[R], acc3[R];
+            Mac4<C> acc;
+            if (tabs) {
+                const int Wk = M2 - k;
+                const V2* sp = reinterpret_cast<const V2*>(pair_s + pair_block_offset(k, M2, M2) + (n - k));
+                int q = 0;
+                for (; q + kPrefetch5 <= cnt; q += kPrefetch5) {
+                    V2 sv[kPrefetch5];
 #pragma unroll
-            for (int r = 0; r < R; ++r) acc0[r] = acc1[r] = acc2[r] = acc3[r] = C{0, 0};
-            const int Wk = M2 - k;
-            const V2* sp = tabs ? reinterpret_cast<const V2*>(pair_s + pair_block_offset(k, M2, M2) + (n - k)) : nullptr;
-            const int Wg = c.g.NM - k + 1;
-            const size_t plane = (size_t)Wg * Wg;
-            const double* G = c.g.gs + c.g.koff[k] + (n - k);
-            for (int q = 0; q < cnt; ++q) {
-                C S;
-                if (tabs) {
-                    const V2 sv = __ldcg(sp + (size_t)q * Wk);
-                    S = C{sv.x, sv.y};
-                } else {
+                    for (int v = 0; v < kPrefetch5; ++v) sv[v] = __ldcg(sp + (q + v) * Wk);
+#pragma unroll
+                    for (int v = 0; v < kPrefetch5; ++v) {
+                        const size_t o = (size_t)(q + v) * R;
+                        acc.add(C{sv[v].x, sv[v].y}, w[o], w[NWR + o], w[2 * NWR + o], w[3 * NWR + o]);
+                    }
+                }
+                for (; q < cnt; ++q) {
+                    const V2 sv = __ldcg(sp + q * Wk);
+                    const size_t o = (size_t)q * R;
+                    acc.add(C{sv.x, sv.y}, w[o], w[NWR + o], w[2 * NWR + o], w[3 * NWR + o]);
+                }
+            } else {
+                const int Wg = c.g.NM - k + 1;
+                const size_t plane = (size_t)Wg * Wg;
+                const double* G = c.g.gs + c.g.koff[k] + (n - k);
+                for (int q = 0; q < cnt; ++q) {
                     const int mu = k + q;
                     const double* gp = G + (size_t)(mu - k) * Wg;
                     const int qm = min(n, mu);
@@ -1099,41 +1198,26 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
                         sx += gq * s.zeta[p].x;
                         sy += gq * s.zeta[p].y;
                     }
-                    S = cm<C>(sx, sy);
+                    const size_t o = (size_t)q * R;
+                    acc.add(cm<C>(sx, sy), w[o], w[NWR + o], w[2 * NWR + o], w[3 * NWR + o]);
                 }
-                C wv[R];
-                ldR<C, R>(w + (size_t)q * R, wv);
-#pragma unroll
-                for (int r = 0; r < R; ++r) cmac(acc0[r].x, acc0[r].y, S, wv[r]);
-                ldR<C, R>(w + ((size_t)NW + q) * R, wv);
-#pragma unroll
-                for (int r = 0; r < R; ++r) cmac(acc1[r].x, acc1[r].y, S, wv[r]);
-                ldR<C, R>(w + ((size_t)2 * NW + q) * R, wv);
-#pragma unroll
-                for (int r = 0; r < R; ++r) cmac(acc2[r].x, acc2[r].y, S, wv[r]);
-                ldR<C, R>(w + ((size_t)3 * NW + q) * R, wv);
-#pragma unroll
-                for (int r = 0; r < R; ++r) cmac(acc3[r].x, acc3[r].y, S, wv[r]);
             }
             const Rl f = sgn(k) / (2.0 * n * (n + 1.0));
-            C* U = s.A + (size_t)(off2(n) + k) * R;
+            C* U = s.A + (size_t)(off2(n) + k) * R + r;
             C* UB = U + (size_t)SP * R;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (k == 0) {
-                    const C a0 = f * acc0[r], b0 = f * acc1[r];
-                    U[r] = a0;
-                    U[(n + 1) * R + r] = a0;
-                    UB[r] = b0;
-                    UB[(n + 1) * R + r] = b0;
-                } else {
-                    const C ap = ipow_mul(-k, f * acc0[r]), am = ipow_mul(k, f * acc2[r]);
-                    const C bp = ipow_mul(-k, f * acc1[r]), bm = ipow_mul(k, f * acc3[r]);
-                    U[r] = ap + am;
-                    U[(n + 1) * R + r] = ap - am;
-                    UB[r] = bp + bm;
-                    UB[(n + 1) * R + r] = bp - bm;
-                }
+            if (k == 0) {
+                const C a0 = f * acc.get(0), b0 = f * acc.get(1);
+                U[0] = a0;
+                U[(n + 1) * R] = a0;
+                UB[0] = b0;
+                UB[(n + 1) * R] = b0;
+            } else {
+                const C ap = ipow_mul(-k, f * acc.get(0)), am = ipow_mul(k, f * acc.get(2));
+                const C bp = ipow_mul(-k, f * acc.get(1)), bm = ipow_mul(k, f * acc.get(3));
+                U[0] = ap + am;
+                U[(n + 1) * R] = ap - am;
+                UB[0] = bp + bm;
+                UB[(n + 1) * R] = bp - bm;
             }
         }
     }
@@ -1141,34 +1225,35 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     // ---- 6. Delta on the translated field, e^{-i s theta} (orders |k| <= kmax only) ----------
     {
         const int items = pj * (pj + 3) / 2;
-        for (int t = tid; t < items; t += kThreads) {
+        for (int u = tid; u < items * R; u += kThreads) {
+            const int t = u / R, r = u % R;
             const short2 d_ = s.nk[t];
-            fwd_item_block<C, R>(delta, s.A, s.B, SP, d_.x, d_.y, min((int)d_.x, kmax), eth[d_.y]);
+            fwd_item_r<C, R>(delta, s.A, s.B, SP, d_.x, d_.y, min((int)d_.x, kmax), eth[d_.y], r);
         }
     }
     __syncthreads();
     // ---- 7. Delta^T, phase, accumulate; then the next pair's tables ---------------------------
     {
         const int items = pj * (pj + 3) / 2;
-        for (int t = tid; t < items; t += kThreads) {
+        for (int u = tid; u < items * R; u += kThreads) {
+            const int t = u / R, r = u % R;
             const short2 d_ = s.nk[t];
             const int n = d_.x, m = d_.y;
             const int fold = ((n + m) & 1) ? n + 1 : 0;
-            const C* va = s.B + (size_t)(off2(n) + fold) * R;
-            C Ea[R], Oa[R], Eb[R], Ob[R];
-            delta_sum_block<C, R>(delta + qoff(n), n, m, n, va, va + (size_t)SP * R, Ea, Oa, Eb, Ob);
+            const C* va = s.B + (size_t)(off2(n) + fold) * R + r;
+            C Ea, Oa, Eb, Ob;
+            delta_sum_r<C, R>(delta + qoff(n), n, m, n, va, va + (size_t)SP * R, Ea, Oa, Eb, Ob);
             const Rl pn = sgn(n);
             const C e = eps[m];
             const int base = n * n - 1 + n;
 #pragma unroll
             for (int part = 0; part < 2; ++part) {
-                C* ap = s.acc + (size_t)(part * Pj + base + m) * R;
-                C* am = s.acc + (size_t)(part * Pj + base - m) * R;
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const C E = part ? Eb[r] : Ea[r], O = part ? Ob[r] : Oa[r];
-                    ap[r] = ap[r] + conjg(e) * (E + O);
-                    if (m > 0) am[r] = am[r] + e * (pn * (E - O));
+                const C E = part ? Eb : Ea, O = part ? Ob : Oa;
+                C& ap = s.acc[(size_t)(part * Pj + base + m) * R + r];
+                ap = ap + conjg(e) * (E + O);
+                if (m > 0) {
+                    C& am = s.acc[(size_t)(part * Pj + base - m) * R + r];
+                    am = am + e * (pn * (E - O));
                 }
             }
         }
@@ -1179,8 +1264,10 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
 
 }  // namespace
 
+// CTAs per SM the block kernel's registers are set for (the single-vector operator's bounds:
+// its per-thread work is the same)
 template <class C, int R>
-__global__ void __launch_bounds__(kThreads, 1) k_direct_block(BlockArgs ba, DirectBucket bk) {
+__global__ void __launch_bounds__(kThreads, DirectOcc<C>::ctas) k_direct_block(BlockArgs ba, DirectBucket bk) {
     extern __shared__ __align__(16) double smem_d[];
     const DirectArgs& a = ba.d;
     const SceneView& sc = a.sc;
@@ -1235,18 +1322,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_direct_block(BlockArgs ba, Dire
     }
     // y += T sum, T = diag(a_n, b_n) of the target
     cplx* Y = ba.y + (size_t)r0 * ba.ld + sc.off[j];
-    for (int t = tid; t < 2 * Pj; t += kThreads) {
+    for (int u = tid; u < 2 * Pj * R; u += kThreads) {
+        const int r = u / (2 * Pj), t = u - r * 2 * Pj;   // right-hand side slowest: coalesced rows of y
+        if (r >= rc) continue;
         const int tt = t < Pj ? t : t - Pj;
         int n, m;
         decode_nm(tt, n, m);
         const cplx tm = (t < Pj) ? sc.an[(size_t)j * sc.pmax + n - 1] : sc.bn[(size_t)j * sc.pmax + n - 1];
-        const C* av = s.acc + (size_t)t * R;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (r < rc) {
-                cplx* yp = Y + (size_t)r * ba.ld + t;
-                *yp = *yp + tm * mk(av[r].x, av[r].y);
-            }
+        const C av = s.acc[(size_t)t * R + r];
+        cplx* yp = Y + (size_t)r * ba.ld + t;
+        *yp = *yp + tm * mk(av.x, av.y);
     }
 }
 
@@ -1257,12 +1342,14 @@ size_t block_smem_bytes(int pp, bool tabs, bool fp32, int R) {
             case 2: return smem_bytes_block<cplxf, 2>(pp, tabs);
             case 4: return smem_bytes_block<cplxf, 4>(pp, tabs);
             case 8: return smem_bytes_block<cplxf, 8>(pp, tabs);
+            case 16: return smem_bytes_block<cplxf, 16>(pp, tabs);
         }
     } else {
         switch (R) {
             case 1: return smem_bytes_block<cplx, 1>(pp, tabs);
             case 2: return smem_bytes_block<cplx, 2>(pp, tabs);
             case 4: return smem_bytes_block<cplx, 4>(pp, tabs);
+            case 8: return smem_bytes_block<cplx, 8>(pp, tabs);
         }
     }
     return 0;
@@ -1284,12 +1371,14 @@ bool launch_direct_block(const BlockArgs& a, const DirectBucket& b, int R, cudaS
             case 2: launch_block_t<cplxf, 2>(a, b, s); return true;
             case 4: launch_block_t<cplxf, 4>(a, b, s); return true;
             case 8: launch_block_t<cplxf, 8>(a, b, s); return true;
+            case 16: launch_block_t<cplxf, 16>(a, b, s); return true;
         }
     } else {
         switch (R) {
             case 1: launch_block_t<cplx, 1>(a, b, s); return true;
             case 2: launch_block_t<cplx, 2>(a, b, s); return true;
             case 4: launch_block_t<cplx, 4>(a, b, s); return true;
+            case 8: launch_block_t<cplx, 8>(a, b, s); return true;
         }
     }
     return false;

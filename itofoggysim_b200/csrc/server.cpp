@@ -6,8 +6,9 @@
 // requests already running (admission by HBM footprint); a request larger than the whole budget is
 // refused.  A running request owns its own handle, CUDA stream, operator tables and Krylov state,
 // so co-resident solves overlap on the GPU and each result is the one the request would get alone
-// (no state or reduction is shared between requests).  Results stay with the server until
-// released.  The reference has no serving layer; the solve each request runs is
+// (no state or reduction is shared between requests).  A request with several right-hand sides
+// solves them as one block (foggy_solve_block), so they share every operator application.
+// Results stay with the server until released.  The reference has no serving layer; the solve each request runs is
 // lib_mie_ms_solver_run (FoggySim/src/lib/mie_theory/lib_mie_ms_solver_interface.f90:143-154).
 #include <algorithm>
 #include <chrono>
@@ -96,7 +97,10 @@ void run_request(foggy_server_s* S, Request& r) {
     r.nrhs = r.per_wave ? r.nw : 1;
     r.x.assign((size_t)(2 * len * r.nrhs), 0.0);
     r.cs.assign((size_t)(3 * r.nrhs), 0.0);
-    if (r.per_wave) {
+    if (r.per_wave && r.nw > 1) {
+        // the request's right-hand sides share every operator application
+        rc = foggy_solve_block(h, r.nw, nullptr, r.x.data(), FOGGY_MEM_HOST, &r.stats, r.cs.data(), nullptr, nullptr);
+    } else if (r.per_wave) {
         rc = foggy_solve_rhs(h, r.nw, nullptr, r.x.data(), FOGGY_MEM_HOST, &r.stats, r.cs.data());
     } else {
         rc = foggy_solve(h, nullptr, r.x.data(), FOGGY_MEM_HOST, &r.stats);
@@ -207,7 +211,10 @@ int32_t foggy_server_submit(foggy_server S, const foggy_request* q, int64_t* id)
     const int share = (int)std::max<size_t>(1, S->workers.size());
     bool tables = r->prm.pair_tables == 1 || (r->prm.pair_tables == 0 && base + tb <= S->budget / share);
     r->prm.pair_tables = tables ? 1 : -1;
-    r->footprint = base + (tables ? tb : 0);
+    r->footprint = base + (tables ? tb : 0) +
+                   (r->per_wave && r->nw > 1
+                        ? foggy::estimate_block_bytes(r->prm, r->N, r->pidx.data(), r->NP, r->nr.data(), r->nw)
+                        : 0);
     r->prm.matvec_mode = FOGGY_MATVEC_DIRECT;
     {
         std::lock_guard<std::mutex> lk(S->mu);

@@ -1,6 +1,7 @@
 """The solve server on the GPU: a mixed stream of requests (different sphere counts, orders and
 right-hand-side counts) run up to three at a time, and every result is bit-identical to the same
-request solved alone on a handle of its own; one solve per plane wave matches single-wave solves
+request solved alone on a handle of its own (a request's several right-hand sides as one block,
+foggy_solve_block, within the tolerance of one-by-one solves); one solve per plane wave matches single-wave solves
 and the oracle; a request larger than the budget is refused; a queued request can be cancelled."""
 import numpy as np
 import pytest
@@ -37,7 +38,13 @@ def test_stream_results_equal_solo_solves(native):
         assert info["state"] == N.REQ_DONE, info["error"]
         assert info["ms_latency"] >= info["ms_solve"] > 0 and info["footprint"] > 0
         with solver.MultiSphereSolver(sc) as s:
-            if pw:
+            if pw and sc.n_waves > 1:
+                # several right-hand sides run as one block in the server, as alone
+                xs, css, _, _, _ = s.solve_block()
+                xr, _, _ = s.solve_rhs()
+                for r in range(sc.n_waves):
+                    assert np.linalg.norm(xs[r] - xr[r]) <= 1e-6 * np.linalg.norm(xr[r])
+            elif pw:
                 xs, css, _ = s.solve_rhs()
             else:
                 x1, _ = s.solve()
