@@ -360,10 +360,12 @@ def run_serving(args):
     reqs = [S.serving_request(rng) for _ in range(args.warmup + args.steps)]
     gaps = np.random.default_rng(43).exponential(1.0 / 50.0, len(reqs))
 
-    def stream(concurrent):
+    prec = 1 if args.precision == "mixed" else 0
+
+    def stream(concurrent, prec):
         with SolveServer(max_concurrent=concurrent) as srv:
             for sc in reqs[:args.warmup]:
-                srv.wait(srv.submit(sc, rhs_per_wave=True))
+                srv.wait(srv.submit(sc, rhs_per_wave=True, precision=prec))
             t0 = time.perf_counter()
             ids, t_arr = [], t0
             for sc, gap in zip(reqs[args.warmup:], gaps[args.warmup:]):
@@ -371,7 +373,7 @@ def run_serving(args):
                 dt = t_arr - time.perf_counter()
                 if dt > 0:
                     time.sleep(dt)
-                ids.append(srv.submit(sc, rhs_per_wave=True))
+                ids.append(srv.submit(sc, rhs_per_wave=True, precision=prec))
             infos = [srv.wait(i)[0] for i in ids]
             span = time.perf_counter() - t0
         ok = [i for i in infos if i["state"] == 2]
@@ -380,18 +382,23 @@ def run_serving(args):
                     done=len(ok), failed=len(infos) - len(ok), makespan_s=span,
                     rhs=int(sum(i["nrhs"] for i in ok)), iterations=int(sum(i["stats"]["iterations"] for i in ok)))
 
-    co = stream(args.concurrent)
-    one = stream(1)
+    co = stream(args.concurrent, prec)
+    # the plain FP64 path one request at a time
+    one = stream(1, 0)
     timed = reqs[args.warmup:]
     line = {
         "metric": METRIC, "value": co["solves_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": co["makespan_s"] * 1e3 / max(1, args.steps),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 translations, f64 Krylov and residuals" if prec else "f64", "data": "synthetic",
         "config": {"workload": "serving stream: 50-500 lognormal spheres per request, 1-16 right-hand sides", "requests": args.steps,
                    "arrivals": "Poisson, 50 per s", "spheres": [int(min(r.n_spheres for r in timed)),
                                                                  int(max(r.n_spheres for r in timed))],
                    "rhs_total": co["rhs"], "gmres_tolerance": 1e-6, "concurrent": args.concurrent,
-                   "admission": "FIFO by device footprint"},
+                   "admission": "FIFO by device footprint",
+                   "solve": "a request's right-hand sides as one block (foggy_solve_block), %s"
+                            % ("mixed precision" if prec else "FP64"),
+                   "one_at_a_time": "the same stream, FP64, one request at a time"},
         "latency_ms": {"p50": co["p50_ms"], "p99": co["p99_ms"]},
         "serving": co, "one_at_a_time": one,
     }
@@ -722,7 +729,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
-    if args.precision == "mixed" and args.workload not in ("operator", "block"):
+    if args.precision == "mixed" and args.workload not in ("operator", "block", "serving"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no mixed-precision solve"}),
                   flush=True)

@@ -134,6 +134,7 @@ struct foggy_handle_s {
     double last_berr = -1.0;
     int64_t launches = 0;        // kernels launched by the current solve
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm0 = nullptr, evm1 = nullptr;
+    std::vector<cudaEvent_t> ev_pool;   // operator timing events of gmres(), reused across solves
     // tree
     unsigned long long* d_keys = nullptr;
     int* d_idx = nullptr;
@@ -994,30 +995,33 @@ int gmres(foggy_handle h, foggy_stats* st) {
     double* d_beta = h->d_scal + 1;
     double* d_res = h->d_scal + 2;
     double* d_bn = h->d_scal + 3;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> mv_events;
+    // operator timing: one pair of events per application, from the handle's pool (created once,
+    // reused by later solves, destroyed with the handle)
+    size_t nmv = 0;
     // Arnoldi steps of a mixed-precision solve use the FP32 operator; the true residuals (start and
     // every restart) the FP64 one, so the restarts refine the solution to the FP64 tolerance
     const bool mixed = h->prm.precision == 1;
     auto matvec = [&](const cplx* x, cplx* y, bool arnoldi) -> int {
-        cudaEvent_t a, b;
-        cudaEventCreate(&a);
-        cudaEventCreate(&b);
-        cudaEventRecord(a, h->stream);
+        while (h->ev_pool.size() < 2 * (nmv + 1)) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, "cudaEventCreate");
+            h->ev_pool.push_back(e);
+        }
+        cudaEventRecord(h->ev_pool[2 * nmv], h->stream);
         int r = apply_operator(h, x, y, arnoldi && mixed);
-        cudaEventRecord(b, h->stream);
-        mv_events.push_back({a, b});
+        cudaEventRecord(h->ev_pool[2 * nmv + 1], h->stream);
+        ++nmv;
         st->matvecs++;
         return r;
     };
     auto cleanup = [&]() {
-        for (auto& e : mv_events) {
+        cudaStreamSynchronize(h->stream);
+        for (size_t i = 0; i < nmv; ++i) {
             float ms = 0;
-            cudaEventElapsedTime(&ms, e.first, e.second);
+            cudaEventElapsedTime(&ms, h->ev_pool[2 * i], h->ev_pool[2 * i + 1]);
             st->ms_matvec += ms;
-            cudaEventDestroy(e.first);
-            cudaEventDestroy(e.second);
         }
-        mv_events.clear();
+        nmv = 0;
     };
     TRY(norm_dev(h, h->d_b, d_bn));
     TRY(matvec(h->d_x, h->d_w, false));
@@ -1183,6 +1187,9 @@ int32_t foggy_destroy(foggy_handle h) {
     h->allocs.clear();
     if (h->h_pin) cudaFreeHost(h->h_pin);
     if (h->h_pin_flags) cudaFreeHost(h->h_pin_flags);
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : {h->ev0, h->ev1, h->evm0, h->evm1})
+        if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return FOGGY_OK;

@@ -130,6 +130,15 @@ __device__ __forceinline__ float2 f2(cplxf c) { return make_float2(c.x, c.y); }
 __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 bcast(float q) { return make_float2(q, q); }
 
+// Work unit of thread tid in the round that starts at b: rounds alternate direction, so where
+// the cost of a unit grows (or falls) with its index -- the rotation stages' items are ordered by
+// degree, the coaxial rows by order -- every thread's total evens out across rounds and the
+// stage's barrier waits less for its slowest thread.  Which thread computes a unit does not
+// change what it computes.
+__device__ __forceinline__ int snake(int b, int tid) {
+    return b + (((b / kThreads) & 1) ? kThreads - 1 - tid : tid);
+}
+
 // r += s w in two fused multiply-adds per component
 template <class C>
 __device__ __forceinline__ void cmac(real_of<C>& rx, real_of<C>& ry, C s, C w) {
@@ -421,7 +430,9 @@ __device__ inline void run_pair(const PairCtx<C>& c, int tid, int pj, int pl, co
     // ---- 2. Delta u, e^{-i s theta} ----------------------------------------------------------
     {
         const int items = pl * (pl + 3) / 2;
-        for (int t = tid; t < items; t += kThreads) {
+        for (int b_ = 0; b_ < items; b_ += kThreads) {
+            const int t = snake(b_, tid);
+            if (t >= items) continue;
             const short2 d_ = s.nk[t];
             const int nu = d_.x, s_ = d_.y;
             fwd_item(delta, s.A, s.B, SP, nu, s_, nu, eth[s_]);
@@ -431,7 +442,9 @@ __device__ inline void run_pair(const PairCtx<C>& c, int tid, int pj, int pl, co
     // ---- 3. Delta^T: x'(nu, +-k) = i^{+-k} T_{+-k}, stored times (2nu+1) ------------------
     {
         const int items = pl * (pl + 3) / 2;
-        for (int t = tid; t < items; t += kThreads) {
+        for (int b_ = 0; b_ < items; b_ += kThreads) {
+            const int t = snake(b_, tid);
+            if (t >= items) continue;
             const short2 d_ = s.nk[t];
             const int nu = d_.x, k = d_.y;
             const int fold = ((nu + k) & 1) ? nu + 1 : 0;
@@ -496,7 +509,9 @@ __device__ inline void run_pair(const PairCtx<C>& c, int tid, int pj, int pl, co
         const int rows_tot = pj + (kmax >= 1 ? kmax * pj - (kmax - 1) * kmax / 2 : 0);
         const int NW = (kmax + 1) * (pl + 2) - kmax * (kmax + 1) / 2;   // w plane stride
         const int M2 = max(pj, pl) + 2;
-        for (int t = tid; t < rows_tot; t += kThreads) {
+        for (int b_ = 0; b_ < rows_tot; b_ += kThreads) {
+            const int t = snake(b_, tid);
+            if (t >= rows_tot) continue;
             int k = 0, rem = t;
             for (;;) {
                 const int rk = pj - max(1, k) + 1;
@@ -629,7 +644,9 @@ __device__ inline void run_pair(const PairCtx<C>& c, int tid, int pj, int pl, co
     // ---- 6. Delta on the translated field, e^{-i s theta} (orders |k| <= kmax only) ----------
     {
         const int items = pj * (pj + 3) / 2;
-        for (int t = tid; t < items; t += kThreads) {
+        for (int b_ = 0; b_ < items; b_ += kThreads) {
+            const int t = snake(b_, tid);
+            if (t >= items) continue;
             const short2 d_ = s.nk[t];
             const int n = d_.x, s_ = d_.y;
             fwd_item(delta, s.A, s.B, SP, n, s_, min(n, kmax), eth[s_]);
@@ -639,7 +656,9 @@ __device__ inline void run_pair(const PairCtx<C>& c, int tid, int pj, int pl, co
     // ---- 7. Delta^T, phase, accumulate; then the next pair's tables ---------------------------
     {
         const int items = pj * (pj + 3) / 2;
-        for (int t = tid; t < items; t += kThreads) {
+        for (int b_ = 0; b_ < items; b_ += kThreads) {
+            const int t = snake(b_, tid);
+            if (t >= items) continue;
             const short2 d_ = s.nk[t];
             const int n = d_.x, m = d_.y;
             const int fold = ((n + m) & 1) ? n + 1 : 0;
@@ -1076,7 +1095,9 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     // ---- 2. Delta u, e^{-i s theta} ----------------------------------------------------------
     {
         const int items = pl * (pl + 3) / 2;
-        for (int u = tid; u < items * R; u += kThreads) {
+        for (int b_ = 0; b_ < items * R; b_ += kThreads) {
+            const int u = snake(b_, tid);
+            if (u >= items * R) continue;
             const int t = u / R, r = u % R;
             const short2 d_ = s.nk[t];
             fwd_item_r<C, R>(delta, s.A, s.B, SP, d_.x, d_.y, d_.x, eth[d_.y], r);
@@ -1086,7 +1107,9 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     // ---- 3. Delta^T: x'(nu, +-k) = i^{+-k} T_{+-k}, stored times (2nu+1) ------------------
     {
         const int items = pl * (pl + 3) / 2;
-        for (int u = tid; u < items * R; u += kThreads) {
+        for (int b_ = 0; b_ < items * R; b_ += kThreads) {
+            const int u = snake(b_, tid);
+            if (u >= items * R) continue;
             const int t = u / R, r = u % R;
             const short2 d_ = s.nk[t];
             const int nu = d_.x, k = d_.y;
@@ -1150,7 +1173,9 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     {
         const int rows_tot = pj + (kmax >= 1 ? kmax * pj - (kmax - 1) * kmax / 2 : 0);
         const int M2 = max(pj, pl) + 2;
-        for (int u = tid; u < rows_tot * R; u += kThreads) {
+        for (int b_ = 0; b_ < rows_tot * R; b_ += kThreads) {
+            const int u = snake(b_, tid);
+            if (u >= rows_tot * R) continue;
             const int t = u / R, r = u % R;
             int k = 0, rem = t;
             for (;;) {
@@ -1225,7 +1250,9 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     // ---- 6. Delta on the translated field, e^{-i s theta} (orders |k| <= kmax only) ----------
     {
         const int items = pj * (pj + 3) / 2;
-        for (int u = tid; u < items * R; u += kThreads) {
+        for (int b_ = 0; b_ < items * R; b_ += kThreads) {
+            const int u = snake(b_, tid);
+            if (u >= items * R) continue;
             const int t = u / R, r = u % R;
             const short2 d_ = s.nk[t];
             fwd_item_r<C, R>(delta, s.A, s.B, SP, d_.x, d_.y, min((int)d_.x, kmax), eth[d_.y], r);
@@ -1235,7 +1262,9 @@ __device__ inline void run_pair_block(const PairCtx<C>& c, int tid, int pj, int 
     // ---- 7. Delta^T, phase, accumulate; then the next pair's tables ---------------------------
     {
         const int items = pj * (pj + 3) / 2;
-        for (int u = tid; u < items * R; u += kThreads) {
+        for (int b_ = 0; b_ < items * R; b_ += kThreads) {
+            const int u = snake(b_, tid);
+            if (u >= items * R) continue;
             const int t = u / R, r = u % R;
             const short2 d_ = s.nk[t];
             const int n = d_.x, m = d_.y;
