@@ -894,7 +894,7 @@ def main():
                           "oracle-direct-cached), %.3f s per application of the 64-sphere cluster (cache built in "
                           "%.1f s), scaled by sum_{j!=l} P_j P_l to this scene and x %d matvecs/solve; this "
                           "scene's cache (two P_j x P_l complex blocks per ordered pair) would need "
-                          "%.0f TB" % (t_c, t_build, mv_count // args.steps, cached_bytes(sc) / 1e12)}
+                          "%.1f GB" % (t_c, t_build, mv_count // args.steps, cached_bytes(sc) / 1e9)}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

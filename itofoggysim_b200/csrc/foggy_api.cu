@@ -135,6 +135,7 @@ struct foggy_handle_s {
     int64_t launches = 0;        // kernels launched by the current solve
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm0 = nullptr, evm1 = nullptr;
     std::vector<cudaEvent_t> ev_pool;   // operator timing events of gmres(), reused across solves
+    cudaEvent_t ev_step[2] = {nullptr, nullptr};   // read-back of the Arnoldi steps in flight
     // tree
     unsigned long long* d_keys = nullptr;
     int* d_idx = nullptr;
@@ -995,6 +996,9 @@ int gmres(foggy_handle h, foggy_stats* st) {
     double* d_beta = h->d_scal + 1;
     double* d_res = h->d_scal + 2;
     double* d_bn = h->d_scal + 3;
+    for (cudaEvent_t& e : h->ev_step)
+        if (!e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return fail(h, FOGGY_ERR_CUDA, "cudaEventCreate");
     // operator timing: one pair of events per application, from the handle's pool (created once,
     // reused by later solves, destroyed with the handle)
     size_t nmv = 0;
@@ -1049,8 +1053,9 @@ int gmres(foggy_handle h, foggy_stats* st) {
         k_scale_copy<<<G, 256, 0, h->stream>>>(h->d_r, d_beta, h->d_V, n);
         k_init_cycle<<<1, 64, 0, h->stream>>>(h->d_gv, m + 1, d_beta, h->d_flags);
         h->launches += 2;
-        int k = 0;
-        for (; k < m && st->iterations < maxit; ++k) {
+        // Arnoldi step k; its residual estimate, H[k+1][k] and flags are copied into pinned slot
+        // k & 1, and the slot's event marks when they have landed
+        auto enqueue_step = [&](int k) -> int {
             cplx* vk = h->d_V + (size_t)k * n;
             cplx* vk1 = h->d_V + (size_t)(k + 1) * n;
             TRY(matvec(vk, h->d_w, true));
@@ -1066,13 +1071,29 @@ int gmres(foggy_handle h, foggy_stats* st) {
                                              h->d_flags);
             CKL(h);
             h->launches += 8;
-            CK(h, cudaMemcpyAsync(h->h_pin, h->d_scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-            CK(h, cudaMemcpyAsync(h->h_pin_flags, h->d_flags, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-            CK(h, cudaStreamSynchronize(h->stream));
+            const int sl = k & 1;
+            CK(h, cudaMemcpyAsync(h->h_pin + 4 * sl, h->d_scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaMemcpyAsync(h->h_pin_flags + sl, h->d_flags, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaEventRecord(h->ev_step[sl], h->stream));
+            return FOGGY_OK;
+        };
+        // One step of lookahead: step k + 1 is queued before step k is read back, so the GPU does
+        // not idle while the host tests convergence.  If step k ends the cycle, step k + 1 has only
+        // written column k + 1 of H and entries k + 1, k + 2 of g, which the k + 1 columns solved
+        // below never read; it costs one operator application.
+        int k = 0;
+        bool queued = false;   // step k is on the stream already
+        for (; k < m && st->iterations < maxit; ++k) {
+            if (!queued) TRY(enqueue_step(k));
+            queued = k + 1 < m && st->iterations + 1 < maxit;
+            if (queued) TRY(enqueue_step(k + 1));
+            CK(h, cudaEventSynchronize(h->ev_step[k & 1]));
             st->iterations++;
-            if (h->h_pin_flags[0] == 2) { status = FOGGY_ERR_NAN; break; }
-            if (h->h_pin_flags[0] == 1) { status = FOGGY_ERR_BREAKDOWN; break; }
-            if (h->h_pin[2] / bnorm <= tol || h->h_pin[0] == 0.0) { ++k; break; }
+            const double* pin = h->h_pin + 4 * (k & 1);
+            const int flag = h->h_pin_flags[k & 1];
+            if (flag == 2) { status = FOGGY_ERR_NAN; break; }
+            if (flag == 1) { status = FOGGY_ERR_BREAKDOWN; break; }
+            if (pin[2] / bnorm <= tol || pin[0] == 0.0) { ++k; break; }
         }
         if (status == FOGGY_ERR_NAN) break;
         if (status == FOGGY_ERR_BREAKDOWN) {
@@ -1188,7 +1209,7 @@ int32_t foggy_destroy(foggy_handle h) {
     if (h->h_pin) cudaFreeHost(h->h_pin);
     if (h->h_pin_flags) cudaFreeHost(h->h_pin_flags);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
-    for (cudaEvent_t e : {h->ev0, h->ev1, h->evm0, h->evm1})
+    for (cudaEvent_t e : {h->ev0, h->ev1, h->evm0, h->evm1, h->ev_step[0], h->ev_step[1]})
         if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;

@@ -84,7 +84,7 @@ def test_block_matvec_matches_single(native, case, pair_tables):
     for v in range(nv):
         assert _err(Yb[v], Y1[v], g) < 1e-13, "vector %d" % v
         assert _err(Yf[v], Y1[v], g) < 1e-5, "vector %d (FP32)" % v
-    assert set(tiles[:, 3].tolist()) <= {1, 2, 4}
+    assert set(tiles[:, 3].tolist()) <= {1, 2, 4, 8}
     assert np.all(tiles[:, 0] > 0) and np.all(tiles[:, 2] <= 32)
 
 
@@ -154,3 +154,29 @@ def test_block_solve_with_initial_guess_and_limits(native):
         s.set_max_iterations(2)
         x, _, its, be, st = s.solve_block(raise_on_error=False)
         assert st["status"] == -5 and np.all(its <= 2) and np.all(be > 1e-11)
+
+
+def test_block_argument_errors(native):
+    """Refusals of the block entries: right-hand-side count other than the plane waves set, restart
+    beyond the block solve's 63, the ML-FMM operator, an unknown precision."""
+    import ctypes as C
+    from itofoggysim_b200 import _native as N
+    sc = S.random_cluster(4, seed=34, p=3)
+    sc = dataclasses.replace(sc, **fibonacci_waves(2))
+    n = sc.vector_length()
+    x = np.zeros(4 * n, np.complex128)
+    st = N.FoggyStats()
+    with solver.MultiSphereSolver(sc) as s:
+        assert s.L.foggy_solve_block(s.h, 3, None, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), None, None,
+                                     None) == N.FOGGY_ERR_ARGUMENT
+        assert s.L.foggy_matvec_block(s.h, 2, 2, x.ctypes.data, x.ctypes.data, N.FOGGY_MEM_HOST) == N.FOGGY_ERR_ARGUMENT
+        s.set_restart(64)
+        assert s.L.foggy_solve_block(s.h, 4, None, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), None, None,
+                                     None) == N.FOGGY_ERR_ARGUMENT
+        s.set_restart(10)
+        s.use_ml_fmm(True)
+        assert s.L.foggy_solve_block(s.h, 4, None, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), None, None,
+                                     None) == N.FOGGY_ERR_UNSUPPORTED
+        s.use_ml_fmm(False)
+        xs, cs, its, be, st2 = s.solve_block()
+        assert st2["status"] == 0 and xs.shape == (4, n)
