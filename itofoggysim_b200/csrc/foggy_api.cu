@@ -382,14 +382,20 @@ DirectArgs direct_args(foggy_handle h, const cplx* x) {
     return a;
 }
 
+// Upper bounds of the truncation-order buckets: steps of 4 degrees up to the largest order a
+// sphere may have (kMaxDegree, the reference's cap), so every sphere is in one bucket.
+constexpr int kBucketBounds[] = {0, 4, 8, 12, 16, 20, 24, 28, 32, 36, 40, 44, 48};
+constexpr int kNumBounds = (int)(sizeof(kBucketBounds) / sizeof(kBucketBounds[0]));
+static_assert(kBucketBounds[kNumBounds - 1] >= kMaxDegree, "every order needs a bucket");
+
 // Truncation-order buckets of the spheres and the (target bucket, source bucket) launches of
 // the direct operator.  Bucket upper bounds grow in steps of 4 degrees; each launch gets enough
 // CTAs per target to fill the GPU.
 int plan_direct(foggy_handle h) {
-    const int bounds[] = {0, 4, 8, 12, 16, 20, 24, 28, 32};
+    const int* bounds = kBucketBounds;
     std::vector<std::vector<int>> members;
     std::vector<int> bp;
-    for (int bi = 1; bi < (int)(sizeof(bounds) / sizeof(bounds[0])); ++bi) {
+    for (int bi = 1; bi < kNumBounds; ++bi) {
         std::vector<int> v;
         for (int j = 0; j < h->N; ++j)
             if (h->p_s[j] > bounds[bi - 1] && h->p_s[j] <= bounds[bi]) v.push_back(j);
@@ -1368,7 +1374,6 @@ int32_t foggy_set_spheres(foggy_handle h, int32_t n_spheres, const double* centr
             if (!std::isfinite(centres[3 * (size_t)j + d])) return fail(h, FOGGY_ERR_ARGUMENT, "non-finite centre");
         pmax = std::max(pmax, std::min(n_range[2 * ip + 1], pg));
     }
-    if (pmax > 32) return fail(h, FOGGY_ERR_UNSUPPORTED, "the direct operator supports truncation orders up to 32");
     Trace tr("foggy_set_spheres");
     CK(h, cudaSetDevice(h->device));
     free_scene(h);
@@ -1703,18 +1708,18 @@ int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_in
     for (int i = 0; i < NP; ++i) pp[i] = std::max(1, std::min(n_range[2 * i + 1], pg));
     int64_t n_unk = 0;
     int pmax = 1;
-    const int bounds[] = {0, 4, 8, 12, 16, 20, 24, 28, 32};
-    std::vector<int64_t> bucket(9, 0), cnt(34, 0);
+    const int* bounds = kBucketBounds;
+    std::vector<int64_t> bucket(kNumBounds, 0), cnt(kMaxDegree + 1, 0);
     for (int j = 0; j < N; ++j) {
         const int p = pp[param_index[j]];
         n_unk += 2 * (int64_t)p * (p + 2);
         pmax = std::max(pmax, p);
-        cnt[std::min(p, 33)]++;
-        for (int b = 1; b < 9; ++b)
+        cnt[std::min(p, kMaxDegree)]++;
+        for (int b = 1; b < kNumBounds; ++b)
             if (p > bounds[b - 1] && p <= bounds[b]) bucket[b]++;
     }
     int nbuckets = 0, cmax = 1;
-    for (int b = 1; b < 9; ++b)
+    for (int b = 1; b < kNumBounds; ++b)
         if (bucket[b]) {
             ++nbuckets;
             cmax = std::max(cmax, (int)std::max<int64_t>(1, std::min<int64_t>(32, (148 * 6 + bucket[b] - 1) / bucket[b])));
@@ -1730,8 +1735,8 @@ int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_in
     bytes += 256 * q * q * q + ((int64_t)64 << 20);                                      // order tables
     int64_t tb = 0;
     if (pair_tables >= 0 && N > 1) {
-        for (int a = 1; a <= 32; ++a)
-            for (int b = a; b <= 32; ++b) {
+        for (int a = 1; a <= kMaxDegree; ++a)
+            for (int b = a; b <= kMaxDegree; ++b) {
                 if (!cnt[a] || !cnt[b]) continue;
                 const int64_t pairs = (a == b) ? cnt[a] * (cnt[a] - 1) / 2 : cnt[a] * cnt[b];
                 tb += pairs * pair_block_size(a, b) * v;
@@ -1927,7 +1932,6 @@ int32_t foggy_estimate_solve_bytes(const foggy_params* params, int32_t n_spheres
             return fail(nullptr, FOGGY_ERR_ARGUMENT, "param_index out of range");
         pmax = std::max(pmax, std::min(n_range[2 * param_index[j] + 1], params->n_range[1]));
     }
-    if (pmax > 32) return fail(nullptr, FOGGY_ERR_UNSUPPORTED, "the direct operator supports truncation orders up to 32");
     *solve_bytes = estimate_solve_bytes(*params, n_spheres, param_index, n_param, n_range, 0, table_bytes);
     return FOGGY_OK;
 }

@@ -370,7 +370,7 @@ module foggy_gpu_f
     public :: foggy_tree_parent, foggy_tree_children, foggy_tree_centre_of_box, foggy_tree_neighbours
     public :: foggy_estimate_solve_bytes, foggy_solve_block, foggy_matvec_block, foggy_block_tiles
     public :: foggy_fmm_lists
-    public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_calculate_vector_b
+    public :: foggy_ms_constructor, foggy_ms_solver_run, foggy_ms_solver_run_block, foggy_ms_calculate_vector_b
     public :: foggy_ms_get_backward_error, foggy_ms_destructor, foggy_ms_vector_length
 
     type(c_ptr), save :: m_handle = c_null_ptr
@@ -404,6 +404,17 @@ module foggy_gpu_f
             type(foggy_stats), intent(out) :: stats
             integer(c_int32_t), intent(out) :: rc
             rc = foggy_solve(m_handle, c_null_ptr, c_loc(x), FOGGY_MEM_HOST, stats)
+        end subroutine
+
+        ! lib_mie_ms_solver_run once per plane wave of the constructor, all in one block: x(:, i) receives
+        ! the solution of wave i alone, iterations(i) its Arnoldi steps (foggy_solve_block).
+        subroutine foggy_ms_solver_run_block(x, iterations, stats, rc)
+            complex(c_double_complex), intent(inout), target, contiguous :: x(:, :)
+            integer(c_int32_t), intent(out), target, contiguous :: iterations(:)
+            type(foggy_stats), intent(out) :: stats
+            integer(c_int32_t), intent(out) :: rc
+            rc = foggy_solve_block(m_handle, int(size(x, 2), c_int32_t), c_null_ptr, c_loc(x), FOGGY_MEM_HOST, &
+                                   stats, c_null_ptr, c_loc(iterations), c_null_ptr)
         end subroutine
 
         ! Mirrors lib_mie_ms_solver_calculate_vector_b(vector_x, vector_b).

@@ -244,8 +244,8 @@ def hcp_sphere_scene(sphere_radius, lattice_sphere_radius=0.0076, particle_radiu
 
 def serving_request(rng, n_lo=50, n_hi=500):
     """One request of the serving stream: sphere count log-uniform in [n_lo, n_hi], lognormal radii
-    (median uniform in 0.4-0.8 um, sigma_ln 0.3, clipped to 0.2-1.2 um so that every truncation
-    order stays within the direct operator's 32), m = 1.33 + 1e-8 i, wavelength uniform in
+    (median uniform in 0.4-0.8 um, sigma_ln 0.3, clipped to 0.2-1.2 um, orders up to 26, which
+    keeps a 30-request stream within a few minutes), m = 1.33 + 1e-8 i, wavelength uniform in
     0.45-0.65 um, volume fraction uniform in 1-5 % (cube edge (N E[V] / vf)^(1/3)), 1-16
     right-hand sides along random directions, x-polarised (TM), GMRES(30) to 1e-6."""
     n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))

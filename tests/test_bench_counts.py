@@ -78,3 +78,29 @@ def test_fibonacci_right_hand_sides():
     # distinct directions, spread over the sphere (mean direction near zero)
     assert np.min(np.linalg.norm(d[:, None] - d[None], axis=-1) + 10 * np.eye(64)) > 0.2
     assert np.linalg.norm(d.mean(0)) < 0.05
+
+
+def test_block_workload_scene():
+    """The block workload: config 4's scene shape (lognormal radii at 20,000 spheres per 90 um cube)
+    at a smaller sphere count, 128 right-hand sides, GMRES(30) to 1e-6."""
+    sc = bench.block_scene(500)
+    assert sc.n_spheres == 500 and sc.n_waves == 128
+    assert sc.gmres_tolerance == 1e-6 and sc.gmres_restart == 30
+    edge = 90.0 * (500 / 20000.0) ** (1.0 / 3.0)
+    assert np.all(sc.centres >= 0.0) and np.all(sc.centres < edge)
+    p = sc.p_of_sphere()
+    assert p.max() <= 30 and 15 <= np.median(p) <= 19
+
+
+def test_cached_operator_size_and_scale():
+    """The cached CPU operator keeps two P_j x P_l complex blocks per ordered pair; its work goes with
+    sum_{j != l} P_j P_l."""
+    a, b = Orders([3, 3, 5]), Orders([3, 5, 5, 5])
+    P = lambda o: [int(v) * (int(v) + 2) for v in o.p]
+    def pairs(o):
+        q = P(o)
+        return sum(q[i] * q[j] for i in range(len(q)) for j in range(len(q)) if i != j)
+    assert bench.cached_bytes(a) == 32 * pairs(a)
+    assert abs(bench.cached_scale(a, b) - pairs(b) / pairs(a)) < 1e-12
+    # the 64-sphere cluster's cache: 4032 pairs x 2 x 255^2 x 16 bytes
+    assert bench.cached_bytes(S.small_cluster()) == 4032 * 2 * 255 ** 2 * 16

@@ -37,9 +37,14 @@ def test_argument_errors(native):
     with pytest.raises(N.FoggyError) as e:
         solver.estimate_solve_bytes(sc)
     assert e.value.code == N.FOGGY_ERR_ARGUMENT
+    # degrees run to 45 (the reference's cap); 46 is out of range
     sc = S.random_cluster(3, seed=1, p=3)
-    sc.n_range_param = np.array([[1, 40]] * sc.n_param, np.int32)
-    sc.n_range = (1, 40)
+    sc.n_range_param = np.array([[1, 46]] * sc.n_param, np.int32)
+    sc.n_range = (1, 46)
     with pytest.raises(N.FoggyError) as e:
         solver.estimate_solve_bytes(sc)
-    assert e.value.code == N.FOGGY_ERR_UNSUPPORTED
+    assert e.value.code == N.FOGGY_ERR_ARGUMENT
+    sc.n_range_param = np.array([[1, 40]] * sc.n_param, np.int32)
+    sc.n_range = (1, 40)
+    sb, tb = solver.estimate_solve_bytes(sc)
+    assert tb > 0 and sb > 0

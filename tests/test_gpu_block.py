@@ -157,8 +157,8 @@ def test_block_solve_with_initial_guess_and_limits(native):
 
 
 def test_block_argument_errors(native):
-    """Refusals of the block entries: right-hand-side count other than the plane waves set, restart
-    beyond the block solve's 63, the ML-FMM operator, an unknown precision."""
+    """Refusals of the block entries: right-hand-side count other than the plane waves set, the ML-FMM
+    operator, an unknown precision."""
     import ctypes as C
     from itofoggysim_b200 import _native as N
     sc = S.random_cluster(4, seed=34, p=3)
@@ -170,10 +170,6 @@ def test_block_argument_errors(native):
         assert s.L.foggy_solve_block(s.h, 3, None, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), None, None,
                                      None) == N.FOGGY_ERR_ARGUMENT
         assert s.L.foggy_matvec_block(s.h, 2, 2, x.ctypes.data, x.ctypes.data, N.FOGGY_MEM_HOST) == N.FOGGY_ERR_ARGUMENT
-        s.set_restart(64)
-        assert s.L.foggy_solve_block(s.h, 4, None, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), None, None,
-                                     None) == N.FOGGY_ERR_ARGUMENT
-        s.set_restart(10)
         s.use_ml_fmm(True)
         assert s.L.foggy_solve_block(s.h, 4, None, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), None, None,
                                      None) == N.FOGGY_ERR_UNSUPPORTED

@@ -1,4 +1,5 @@
-"""Parity of the CUDA operator with the FP64 oracle at truncation orders 17-30.
+"""Parity of the CUDA operator with the FP64 oracle at truncation orders 17-30, and up to the
+reference's cap of 45.
 
 The 2000-sphere lognormal scene (radii 0.2-1.5 um at lambda = 0.55 um) has per-sphere Wiscombe
 orders up to 30, median 17.  These tests cover those degrees, every truncation-order bucket of
@@ -167,3 +168,22 @@ def test_mixed_precision_orders_17_to_30(native, pair_tables):
     assert np.linalg.norm(r / g) / np.linalg.norm(b / g) <= 1.01e-10
     rel = np.linalg.norm((x32 - x64) / g) / np.linalg.norm(x64 / g)
     assert rel < TOL_MIXED
+
+
+def test_matvec_orders_33_to_45(native, oracle):
+    """Spheres above order 32 (radius 1.8 and 2.6 um at 0.55 um: orders 34 and 45, the reference's cap,
+    lib_mie_ss_helper_functions.f90:32): they fall in the operator's upper order buckets (33-36,
+    45-48), whose CTAs use up to 216 KB of shared memory."""
+    sc = S.random_cluster(2, seed=43, radii=np.array([1.8, 2.6]), box=8.0, z_coupling=3,
+                          reference_row_rule=False)
+    assert sorted(sc.p_of_sphere().tolist()) == [34, 45]
+    g = _g_layout(sc)
+    x = _random_scaled(sc, 8, g)
+    yo = oracle.Problem(sc).matvec(x)
+    for pair_tables in (0, -1):
+        with solver.MultiSphereSolver(sc, pair_tables=pair_tables) as s:
+            y = s.calculate_vector_b(x)
+            yb = s.calculate_vector_b_block(np.stack([x, x]), precision=0)
+        assert _scaled_err(y, yo, g) < TOL_OP, pair_tables
+        assert _scaled_err(yb[1], yo, g) < TOL_OP, pair_tables
+
