@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -47,6 +48,7 @@ struct foggy_handle_s {
     foggy_params prm{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;   // the device's stream-ordered pool (device_pool)
     std::string err;
     std::vector<void*> allocs;   // every device allocation, freed in destroy
     std::map<void*, size_t> alloc_bytes;   // their sizes, returned to the budget when freed
@@ -73,6 +75,7 @@ struct foggy_handle_s {
     double* d_g = nullptr;
     // translation tables
     int tab_pmax = -1;
+    int ax_pmax = 0;   // degree of the axial (3j) tables, built on demand
     int32_t* d_axoff = nullptr;
     double* d_ga = nullptr;
     double* d_gb = nullptr;
@@ -198,9 +201,82 @@ int fail(foggy_handle h, int code, const std::string& msg) {
 // Host to device on the handle's stream, then wait.  The kernels that read dst run on that
 // non-blocking stream, which a blocking cudaMemcpy on the legacy stream does not order (from
 // pageable memory it may return before the DMA lands), and the source is often a temporary.
+static cudaError_t d2h(foggy_handle h, void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(h->stream) : e;
+}
+
 static cudaError_t h2d(foggy_handle h, void* dst, const void* src, size_t bytes) {
     cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
     return e == cudaSuccess ? cudaStreamSynchronize(h->stream) : e;
+}
+
+// Device memory of every handle comes from one stream-ordered pool per device: allocations and
+// frees are ordered on the handle's stream, so a handle that sets up or tears down while others
+// solve does not synchronise the device (cudaMalloc and cudaFree would serialise every stream of
+// co-resident solves).  Memory freed to the pool beyond kPoolKeep bytes goes back to the driver at
+// the next synchronisation; a freed block is reused by another stream only once its free has run
+// (no dependencies between handles' streams are inserted).
+constexpr uint64_t kPoolKeep = 4ull << 30;
+
+cudaMemPool_t device_pool(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = kPoolKeep;
+    int no = 0;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+    pools[device] = pool;
+    return pool;
+}
+
+// per-call device scratch, stream-ordered like dalloc (not counted in the handle's budget)
+template <class T>
+cudaError_t talloc(foggy_handle h, T** p, size_t bytes) {
+    return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), std::max<size_t>(bytes, 16), h->pool, h->stream);
+}
+inline void tfree(foggy_handle h, void* p) {
+    if (p) cudaFreeAsync(p, h->stream);
+}
+
+// The handles' small page-locked read-back buffers, 256-byte slots carved from 1 MiB blocks that
+// are allocated once and kept: cudaMallocHost per handle would serialise the device's streams.
+constexpr size_t kPinSlot = 256;
+struct PinnedSlots {
+    std::mutex mu;
+    std::vector<char*> free;
+};
+PinnedSlots& pinned_slots() {
+    static PinnedSlots P;
+    return P;
+}
+char* pinned_slot() {
+    PinnedSlots& P = pinned_slots();
+    std::lock_guard<std::mutex> lk(P.mu);
+    if (P.free.empty()) {
+        char* block = nullptr;
+        if (cudaMallocHost(reinterpret_cast<void**>(&block), 1 << 20) != cudaSuccess) return nullptr;
+        for (size_t i = 0; i < (size_t(1) << 20) / kPinSlot; ++i) P.free.push_back(block + i * kPinSlot);
+    }
+    char* q = P.free.back();
+    P.free.pop_back();
+    return q;
+}
+void pinned_release(char* q) {
+    if (!q) return;
+    PinnedSlots& P = pinned_slots();
+    std::lock_guard<std::mutex> lk(P.mu);
+    P.free.push_back(q);
 }
 
 template <class T>
@@ -210,8 +286,12 @@ int dalloc(foggy_handle h, T** p, size_t count) {
     if (h->budget && h->bytes_in_use + bytes > h->budget)
         return fail(h, FOGGY_ERR_NOMEM, "device memory budget exceeded (" + std::to_string(h->bytes_in_use + bytes) +
                                             " > " + std::to_string(h->budget) + " bytes)");
-    cudaError_t e = cudaMalloc((void**)p, bytes);
-    if (e != cudaSuccess) return fail(h, FOGGY_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, h->pool, h->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(h, FOGGY_ERR_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
+    }
     h->allocs.push_back(*p);
     h->alloc_bytes[*p] = bytes;
     h->bytes_in_use += bytes;
@@ -228,7 +308,7 @@ void dfree(foggy_handle h, T*& p) {
         h->bytes_in_use -= std::min(h->bytes_in_use, sz->second);
         h->alloc_bytes.erase(sz);
     }
-    cudaFree(p);
+    cudaFreeAsync(p, h->stream);
     p = nullptr;
 }
 
@@ -261,93 +341,107 @@ SceneView scene_view(foggy_handle h) {
     return s;
 }
 
-// 3j tables, g_nm and d-table helper tables for degrees <= pmax
-int ensure_tables(foggy_handle h, int pmax) {
-    if (h->tab_pmax >= pmax) return FOGGY_OK;
-    dfree(h, h->d_axoff);
-    dfree(h, h->d_ga);
-    dfree(h, h->d_gb);
-    dfree(h, h->d_koff);
-    dfree(h, h->d_gab);
-    dfree(h, h->d_sqrt_binom);
-    dfree(h, h->d_rs);
-    dfree(h, h->d_irs);
-    dfree(h, h->d_rj);
-    dfree(h, h->d_g);
-    dfree(h, h->d_delta);
-    dfree(h, h->d_delta32);
-    AxialTables t;
-    build_axial_tables(pmax, t);
-    TRY(dalloc(h, &h->d_axoff, t.offset.size()));
-    TRY(dalloc(h, &h->d_ga, t.ga.size()));
-    TRY(dalloc(h, &h->d_gb, t.gb.size()));
-    {
-        std::vector<int64_t> koff;
-        std::vector<double> gab;
-        build_axial_tables_qmajor(t, koff, gab);
-        TRY(dalloc(h, &h->d_koff, koff.size()));
-        TRY(dalloc(h, &h->d_gab, gab.size()));
-        CK(h, h2d(h, h->d_koff, koff.data(), koff.size() * sizeof(int64_t)));
-        CK(h, h2d(h, h->d_gab, gab.data(), gab.size() * sizeof(double)));
-    }
-    CK(h, h2d(h, h->d_axoff, t.offset.data(), t.offset.size() * sizeof(int32_t)));
-    CK(h, h2d(h, h->d_ga, t.ga.data(), t.ga.size() * sizeof(double)));
-    CK(h, h2d(h, h->d_gb, t.gb.data(), t.gb.size() * sizeof(double)));
-    int K = pmax + 1;   // the scalar-coefficient relation reads sqrt((nu+1)^2 - k^2) at nu = pmax
-    {
-        std::vector<int64_t> koff;
-        std::vector<double> gs;
-        build_scalar_gaunt_qmajor(pmax + 1, koff, gs);
-        dfree(h, h->d_koffS);
-        dfree(h, h->d_gs);
-        TRY(dalloc(h, &h->d_koffS, koff.size()));
-        TRY(dalloc(h, &h->d_gs, gs.size()));
-        CK(h, h2d(h, h->d_koffS, koff.data(), koff.size() * sizeof(int64_t)));
-        CK(h, h2d(h, h->d_gs, gs.data(), gs.size() * sizeof(double)));
-        h->gs_nm = pmax + 1;
-    }
-    std::vector<double> sb((size_t)(K + 1) * (2 * K + 1), 0.0), rs((size_t)(K + 1) * (K + 1), 0.0);
+// Host tables that depend on the truncation degree alone: the scalar Gaunt sums, d-table helper
+// tables, d^j(pi/2) and g_nm.  Built once per degree in the process and shared by every handle (a
+// solve server creates one handle per request, so they are not rebuilt per request).
+struct OrderTables {
+    int K = 0;
+    std::vector<int64_t> koffS;
+    std::vector<double> gs, sb, rs, irs, rj, delta, g;
+    std::vector<float> delta32;
+};
+
+std::shared_ptr<const OrderTables> order_tables(int pmax) {
+    static std::mutex mu;
+    static std::map<int, std::shared_ptr<const OrderTables>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(pmax);
+    if (it != cache.end()) return it->second;
+    auto t = std::make_shared<OrderTables>();
+    const int K = pmax + 1;   // the scalar-coefficient relation reads sqrt((nu+1)^2 - k^2) at nu = pmax
+    t->K = K;
+    build_scalar_gaunt_qmajor(pmax + 1, t->koffS, t->gs);
+    t->sb.assign((size_t)(K + 1) * (2 * K + 1), 0.0);
+    t->rs.assign((size_t)(K + 1) * (K + 1), 0.0);
+    t->irs.assign((size_t)(K + 1) * (K + 1), 0.0);
+    t->rj.assign(2 * (size_t)(K + 2), 0.0);
     for (int J = 0; J <= K; ++J)
         for (int m = -J; m <= J; ++m) {
             long double c = 1.0L;   // C(2J, J+m)
             int a = J + m, b = J - m;
             for (int i = 1; i <= b; ++i) c = c * (a + i) / i;
-            sb[(size_t)J * (2 * K + 1) + (m + K)] = (double)std::sqrt(c);
+            t->sb[(size_t)J * (2 * K + 1) + (m + K)] = (double)std::sqrt(c);
         }
-    std::vector<double> irs((size_t)(K + 1) * (K + 1), 0.0), rj(2 * (size_t)(K + 2), 0.0);
     for (int j = 0; j <= K; ++j)
         for (int m = 0; m <= j; ++m) {
             double v = std::sqrt((double)j * j - (double)m * m);
-            rs[(size_t)j * (K + 1) + m] = v;
-            irs[(size_t)j * (K + 1) + m] = (v > 0) ? 1.0 / v : 0.0;
+            t->rs[(size_t)j * (K + 1) + m] = v;
+            t->irs[(size_t)j * (K + 1) + m] = (v > 0) ? 1.0 / v : 0.0;
         }
     for (int j = 2; j <= K; ++j) {
-        rj[2 * j] = 1.0 / ((double)j * (j - 1));
-        rj[2 * j + 1] = 1.0 / ((double)(j - 1) * (2.0 * j - 1.0));
+        t->rj[2 * j] = 1.0 / ((double)j * (j - 1));
+        t->rj[2 * j + 1] = 1.0 / ((double)(j - 1) * (2.0 * j - 1.0));
     }
-    TRY(dalloc(h, &h->d_sqrt_binom, sb.size()));
-    TRY(dalloc(h, &h->d_rs, rs.size()));
-    TRY(dalloc(h, &h->d_irs, irs.size()));
-    TRY(dalloc(h, &h->d_rj, rj.size()));
-    CK(h, h2d(h, h->d_sqrt_binom, sb.data(), sb.size() * sizeof(double)));
-    CK(h, h2d(h, h->d_rs, rs.data(), rs.size() * sizeof(double)));
-    CK(h, h2d(h, h->d_irs, irs.data(), irs.size() * sizeof(double)));
-    CK(h, h2d(h, h->d_rj, rj.data(), rj.size() * sizeof(double)));
-    {
-        std::vector<double> dl;
-        build_delta_table(pmax, dl);
-        TRY(dalloc(h, &h->d_delta, dl.size()));
-        CK(h, h2d(h, h->d_delta, dl.data(), dl.size() * sizeof(double)));
-        std::vector<float> dl32(dl.begin(), dl.end());
-        TRY(dalloc(h, &h->d_delta32, dl32.size()));
-        CK(h, h2d(h, h->d_delta32, dl32.data(), dl32.size() * sizeof(float)));
-    }
-    std::vector<double> g;
-    build_g_table(pmax, g);
-    TRY(dalloc(h, &h->d_g, g.size()));
-    CK(h, h2d(h, h->d_g, g.data(), g.size() * sizeof(double)));
-    h->K = K;
+    build_delta_table(pmax, t->delta);
+    t->delta32.assign(t->delta.begin(), t->delta.end());
+    build_g_table(pmax, t->g);
+    cache[pmax] = t;
+    return t;
+}
+
+// the operator's order tables for degrees <= pmax on the device
+int ensure_tables(foggy_handle h, int pmax) {
+    if (h->tab_pmax >= pmax) return FOGGY_OK;
+    for (double** q : {&h->d_gs, &h->d_sqrt_binom, &h->d_rs, &h->d_irs, &h->d_rj, &h->d_g, &h->d_delta}) dfree(h, *q);
+    dfree(h, h->d_koffS);
+    dfree(h, h->d_delta32);
+    const std::shared_ptr<const OrderTables> t = order_tables(pmax);
+    auto up = [&](auto** d, const auto& v) -> int {
+        TRY(dalloc(h, d, v.size()));
+        CK(h, cudaMemcpyAsync(*d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, h->stream));
+        return FOGGY_OK;
+    };
+    TRY(up(&h->d_koffS, t->koffS));
+    TRY(up(&h->d_gs, t->gs));
+    TRY(up(&h->d_sqrt_binom, t->sb));
+    TRY(up(&h->d_rs, t->rs));
+    TRY(up(&h->d_irs, t->irs));
+    TRY(up(&h->d_rj, t->rj));
+    TRY(up(&h->d_delta, t->delta));
+    TRY(up(&h->d_delta32, t->delta32));
+    TRY(up(&h->d_g, t->g));
+    // the cached host vectors outlive the copies (the cache keeps them), so no synchronisation here
+    h->gs_nm = pmax + 1;
+    h->K = t->K;
     h->tab_pmax = pmax;
+    h->ax_pmax = 0;
+    return FOGGY_OK;
+}
+
+// 3j (axial) tables of the explicit translation coefficients, for degrees <= the order tables'
+int ensure_axial_tables(foggy_handle h) {
+    if (h->ax_pmax >= h->tab_pmax) return FOGGY_OK;
+    dfree(h, h->d_axoff);
+    dfree(h, h->d_ga);
+    dfree(h, h->d_gb);
+    dfree(h, h->d_koff);
+    dfree(h, h->d_gab);
+    AxialTables t;
+    build_axial_tables(h->tab_pmax, t);
+    std::vector<int64_t> koff;
+    std::vector<double> gab;
+    build_axial_tables_qmajor(t, koff, gab);
+    TRY(dalloc(h, &h->d_axoff, t.offset.size()));
+    TRY(dalloc(h, &h->d_ga, t.ga.size()));
+    TRY(dalloc(h, &h->d_gb, t.gb.size()));
+    TRY(dalloc(h, &h->d_koff, koff.size()));
+    TRY(dalloc(h, &h->d_gab, gab.size()));
+    CK(h, h2d(h, h->d_koff, koff.data(), koff.size() * sizeof(int64_t)));
+    CK(h, h2d(h, h->d_gab, gab.data(), gab.size() * sizeof(double)));
+    CK(h, h2d(h, h->d_axoff, t.offset.data(), t.offset.size() * sizeof(int32_t)));
+    CK(h, h2d(h, h->d_ga, t.ga.data(), t.ga.size() * sizeof(double)));
+    CK(h, h2d(h, h->d_gb, t.gb.data(), t.gb.size() * sizeof(double)));
+    h->ax_pmax = h->tab_pmax;
     return FOGGY_OK;
 }
 
@@ -488,18 +582,18 @@ int ensure_pair_tables(foggy_handle h) {
     if (!h->d_pair_off) {
         TRY(dalloc(h, &h->d_pair_off, npairs + 1));
         int64_t* d_sizes = nullptr;
-        CK(h, cudaMalloc(&d_sizes, npairs * sizeof(int64_t)));
+        CK(h, talloc(h, &d_sizes, npairs * sizeof(int64_t)));
         k_pair_sizes<<<h->N, 256, 0, h->stream>>>(scene_view(h), d_sizes);
         size_t tmp = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_sizes, h->d_pair_off, npairs, h->stream);
         void* d_tmp = nullptr;
-        cudaError_t e = cudaMalloc(&d_tmp, tmp);
+        cudaError_t e = talloc(h, &d_tmp, tmp);
         if (e == cudaSuccess) {
             cub::DeviceScan::ExclusiveSum(d_tmp, tmp, d_sizes, h->d_pair_off, npairs, h->stream);
             e = cudaStreamSynchronize(h->stream);
         }
-        cudaFree(d_tmp);
-        cudaFree(d_sizes);
+        tfree(h, d_tmp);
+        tfree(h, d_sizes);
         if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("pair offsets: ") + cudaGetErrorString(e));
     }
     Trace tr("pair tables");
@@ -535,15 +629,15 @@ int build_tree_dev(foggy_handle h) {
     }
     double* d_mm = nullptr;
     int* d_lmax = nullptr;
-    CK(h, cudaMalloc(&d_mm, 6 * sizeof(double)));
-    CK(h, cudaMalloc(&d_lmax, sizeof(int)));
+    CK(h, talloc(h, &d_mm, 6 * sizeof(double)));
+    CK(h, talloc(h, &d_lmax, sizeof(int)));
     k_minmax<<<1, 256, 0, h->stream>>>(n, h->d_centres, d_mm);
     k_morton<<<(n + 255) / 256, 256, 0, h->stream>>>(n, h->d_centres, d_mm, h->d_keys, h->d_idx);
     size_t tmp_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, h->d_keys, h->d_keys_sorted, h->d_idx, h->d_idx_sorted, n, 0,
                                     63, h->stream);
     void* d_tmp = nullptr;
-    CK(h, cudaMalloc(&d_tmp, tmp_bytes));
+    CK(h, talloc(h, &d_tmp, tmp_bytes));
     cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, h->d_keys, h->d_keys_sorted, h->d_idx, h->d_idx_sorted, n, 0,
                                     63, h->stream);
     int one = 1;
@@ -553,9 +647,9 @@ int build_tree_dev(foggy_handle h) {
     int lmax = 1;
     cudaError_t e = cudaMemcpyAsync(&lmax, d_lmax, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(d_tmp);
-    cudaFree(d_mm);
-    cudaFree(d_lmax);
+    tfree(h, d_tmp);
+    tfree(h, d_mm);
+    tfree(h, d_lmax);
     if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("tree: ") + cudaGetErrorString(e));
     CKL(h);
     // l_min = 1 + floor(log(k + 1) / log(2)) for k = 1 (lib_tree.f90:1162-1170)
@@ -594,13 +688,13 @@ int ensure_fmm(foggy_handle h) {
     std::vector<void*> scratch;
     auto sc_alloc = [&](auto** p, size_t count) -> cudaError_t {
         void* q = nullptr;
-        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(**p));
+        cudaError_t e = talloc(h, &q, std::max<size_t>(count, 1) * sizeof(**p));
         if (e == cudaSuccess) scratch.push_back(q);
         *p = static_cast<std::remove_reference_t<decltype(*p)>>(q);
         return e;
     };
     auto cleanup = [&]() {
-        for (void* q : scratch) cudaFree(q);
+        for (void* q : scratch) tfree(h, q);
         scratch.clear();
     };
     auto bad = [&](cudaError_t e, const char* what) {
@@ -871,7 +965,7 @@ int ensure_rhs(foggy_handle h) {
     const size_t nwav = (size_t)nw + nl;
     const size_t bytes = nwav * sizeof(WaveDev) + (size_t)nb * sizeof(GaussDev) + 2 * nwav * S * sizeof(double);
     void* buf = nullptr;
-    CK(h, cudaMalloc(&buf, bytes));
+    CK(h, talloc(h, &buf, bytes));
     WaveDev* d_w = static_cast<WaveDev*>(buf);
     WaveDev* d_l = d_w + nw;
     GaussDev* d_g = reinterpret_cast<GaussDev*>(d_l + nl);
@@ -895,7 +989,7 @@ int ensure_rhs(foggy_handle h) {
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(buf);
+    tfree(h, buf);
     if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("rhs: ") + cudaGetErrorString(e));
     h->rhs_ready = true;
     return FOGGY_OK;
@@ -1193,14 +1287,23 @@ int32_t foggy_create(const foggy_params* params, int32_t device, foggy_handle* o
     if (!h) return fail(nullptr, FOGGY_ERR_NOMEM, "host allocation");
     h->prm = *params;
     h->device = device;
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocHost(&h->h_pin, 8 * sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&h->h_pin_flags, 4 * sizeof(int)) != cudaSuccess) {
+    char* pin = nullptr;
+    h->pool = device_pool(device);
+    if (!h->pool || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        !(pin = pinned_slot())) {
+        if (h->stream) cudaStreamDestroy(h->stream);
         delete h;
-        return fail(nullptr, FOGGY_ERR_CUDA, "stream or pinned allocation failed");
+        return fail(nullptr, FOGGY_ERR_CUDA, "memory pool, stream or pinned allocation failed");
     }
+    h->h_pin = reinterpret_cast<double*>(pin);             // 8 doubles
+    h->h_pin_flags = reinterpret_cast<int*>(pin + 128);    // 4 ints
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
+    // memory the pool holds but no allocation uses is free for this handle too
+    uint64_t reserved = 0, used = 0;
+    cudaMemPoolGetAttribute(h->pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(h->pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    if (reserved > used) fr += (size_t)(reserved - used);
     h->budget = params->device_memory_budget > 0 ? (size_t)params->device_memory_budget : (size_t)(0.9 * fr);
     *out = h;
     return FOGGY_OK;
@@ -1209,11 +1312,10 @@ int32_t foggy_create(const foggy_params* params, int32_t device, foggy_handle* o
 int32_t foggy_destroy(foggy_handle h) {
     if (!h) return FOGGY_OK;
     cudaSetDevice(h->device);
-    if (h->stream) cudaStreamSynchronize(h->stream);
-    for (void* p : h->allocs) cudaFree(p);
+    for (void* p : h->allocs) cudaFreeAsync(p, h->stream);
     h->allocs.clear();
-    if (h->h_pin) cudaFreeHost(h->h_pin);
-    if (h->h_pin_flags) cudaFreeHost(h->h_pin_flags);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    pinned_release(reinterpret_cast<char*>(h->h_pin));
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : {h->ev0, h->ev1, h->evm0, h->evm1, h->ev_step[0], h->ev_step[1]})
         if (e) cudaEventDestroy(e);
@@ -1325,11 +1427,11 @@ static int32_t load_scene(foggy_handle h, int32_t n_spheres, const double* centr
     double *d_x = nullptr, *d_mr = nullptr, *d_mi = nullptr;
     int* d_pp = nullptr;
     int* d_pidx = nullptr;
-    CK(h, cudaMalloc(&d_x, n_param * sizeof(double)));
-    CK(h, cudaMalloc(&d_mr, n_param * sizeof(double)));
-    CK(h, cudaMalloc(&d_mi, n_param * sizeof(double)));
-    CK(h, cudaMalloc(&d_pp, n_param * sizeof(int)));
-    CK(h, cudaMalloc(&d_pidx, n_spheres * sizeof(int)));
+    CK(h, talloc(h, &d_x, n_param * sizeof(double)));
+    CK(h, talloc(h, &d_mr, n_param * sizeof(double)));
+    CK(h, talloc(h, &d_mi, n_param * sizeof(double)));
+    CK(h, talloc(h, &d_pp, n_param * sizeof(int)));
+    CK(h, talloc(h, &d_pidx, n_spheres * sizeof(int)));
     CK(h, h2d(h, d_x, xs.data(), n_param * sizeof(double)));
     CK(h, h2d(h, d_mr, h->mre.data(), n_param * sizeof(double)));
     CK(h, h2d(h, d_mi, h->mim.data(), n_param * sizeof(double)));
@@ -1338,11 +1440,11 @@ static int32_t load_scene(foggy_handle h, int32_t n_spheres, const double* centr
     k_mie_ab<<<(n_param + 63) / 64, 64, 0, h->stream>>>(n_param, d_x, d_mr, d_mi, d_pp, h->pmax, h->d_an_p, h->d_bn_p);
     k_gather_an<<<n_spheres, 64, 0, h->stream>>>(n_spheres, d_pidx, h->pmax, h->d_an_p, h->d_bn_p, h->d_an, h->d_bn);
     cudaError_t e = cudaStreamSynchronize(h->stream);
-    cudaFree(d_x);
-    cudaFree(d_mr);
-    cudaFree(d_mi);
-    cudaFree(d_pp);
-    cudaFree(d_pidx);
+    tfree(h, d_x);
+    tfree(h, d_mr);
+    tfree(h, d_mi);
+    tfree(h, d_pp);
+    tfree(h, d_pidx);
     if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("mie: ") + cudaGetErrorString(e));
     CKL(h);
     h->rhs_ready = false;
@@ -1463,8 +1565,8 @@ int32_t foggy_get_mie_coefficients(foggy_handle h, int32_t ip, double* a, double
     if (!h) return fail(nullptr, FOGGY_ERR_ARGUMENT, "handle is NULL");
     if (ip < 0 || ip >= h->NP || !a || !b) return fail(h, FOGGY_ERR_ARGUMENT, "parameter index");
     int p = h->p_param[ip];
-    CK(h, cudaMemcpy(a, h->d_an_p + (size_t)ip * h->pmax, p * sizeof(cplx), cudaMemcpyDeviceToHost));
-    CK(h, cudaMemcpy(b, h->d_bn_p + (size_t)ip * h->pmax, p * sizeof(cplx), cudaMemcpyDeviceToHost));
+    CK(h, d2h(h, a, h->d_an_p + (size_t)ip * h->pmax, p * sizeof(cplx)));
+    CK(h, d2h(h, b, h->d_bn_p + (size_t)ip * h->pmax, p * sizeof(cplx)));
     return FOGGY_OK;
 }
 
@@ -1606,7 +1708,7 @@ int32_t foggy_get_field(foggy_handle h, const double* x, int32_t mem, int32_t np
     const size_t np = (size_t)npoints;
     size_t bytes = rad.size() * sizeof(double);
     if (mem == FOGGY_MEM_HOST) bytes += len * sizeof(cplx) + 3 * np * sizeof(double) + 6 * np * sizeof(cplx);
-    CK(h, cudaMalloc(&tmp, bytes));
+    CK(h, talloc(h, &tmp, bytes));
     double* d_rad = static_cast<double*>(tmp);
     char* q = reinterpret_cast<char*>(d_rad + rad.size());
     cudaError_t e = cudaMemcpyAsync(d_rad, rad.data(), rad.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
@@ -1631,7 +1733,7 @@ int32_t foggy_get_field(foggy_handle h, const double* x, int32_t mem, int32_t np
         if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, hd, 3 * np * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(tmp);
+    tfree(h, tmp);
     if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("field: ") + cudaGetErrorString(e));
     return FOGGY_OK;
 }
@@ -1787,12 +1889,12 @@ int32_t foggy_cross_sections(foggy_handle h, const double* x, int32_t mem, doubl
     SceneView sv = scene_view(h);
     k_unpack<<<h->N, 128, 0, h->stream>>>(sv, h->pg, h->d_g, src, h->d_tmp_in);
     double* d_part = nullptr;
-    CK(h, cudaMalloc(&d_part, 2 * (size_t)h->N * sizeof(double)));
+    CK(h, talloc(h, &d_part, 2 * (size_t)h->N * sizeof(double)));
     k_cross_sections<<<h->N, 256, 0, h->stream>>>(sv, h->d_tmp_in, h->d_pq, d_part);
     std::vector<double> part(2 * (size_t)h->N);
     cudaError_t e = cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(d_part);
+    tfree(h, d_part);
     if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("cross sections: ") + cudaGetErrorString(e));
     double se = 0, sa = 0;
     for (int j = 0; j < h->N; ++j) {
@@ -1829,6 +1931,7 @@ int32_t foggy_translation_coefficients(double x, double theta, double phi, const
     int pn = n_range[1], pnu = nu_range[1];
     int pmax = std::max(pn, pnu);
     rc = ensure_tables(h, pmax);
+    if (rc == FOGGY_OK) rc = ensure_axial_tables(h);
     if (rc) {
         fail(nullptr, rc, h->err);
         foggy_destroy(h);
@@ -1838,8 +1941,8 @@ int32_t foggy_translation_coefficients(double x, double theta, double phi, const
     int Pn = pn * (pn + 2), Pnu = pnu * (pnu + 2);
     cplx *dA = nullptr, *dB = nullptr;
     std::vector<cplx> hA((size_t)Pn * Pnu), hB((size_t)Pn * Pnu);
-    cudaError_t e = cudaMalloc(&dA, hA.size() * sizeof(cplx));
-    if (e == cudaSuccess) e = cudaMalloc(&dB, hB.size() * sizeof(cplx));
+    cudaError_t e = talloc(h, &dA, hA.size() * sizeof(cplx));
+    if (e == cudaSuccess) e = talloc(h, &dB, hB.size() * sizeof(cplx));
     if (e == cudaSuccess) {
         size_t smem = translation_pair_smem_bytes(pmax);
         raise_smem_ceiling(reinterpret_cast<const void*>(k_translation_pair), smem);
@@ -1849,8 +1952,8 @@ int32_t foggy_translation_coefficients(double x, double theta, double phi, const
     if (e == cudaSuccess) e = cudaMemcpyAsync(hA.data(), dA, hA.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hB.data(), dB, hB.size() * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(dA);
-    cudaFree(dB);
+    tfree(h, dA);
+    tfree(h, dB);
     std::vector<double> g;
     build_g_table(pmax, g);
     foggy_destroy(h);
@@ -1885,8 +1988,8 @@ int32_t foggy_build_tree(foggy_handle h, int64_t* uindex_out, int32_t* order_out
     if (uindex_out || order_out) {
         std::vector<unsigned long long> ks(n);
         std::vector<int> is(n);
-        CK(h, cudaMemcpy(ks.data(), h->d_keys_sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-        CK(h, cudaMemcpy(is.data(), h->d_idx_sorted, n * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(h, d2h(h, ks.data(), h->d_keys_sorted, n * sizeof(unsigned long long)));
+        CK(h, d2h(h, is.data(), h->d_idx_sorted, n * sizeof(int)));
         int sh = 3 * (21 - h->tree_lmax);
         for (int i = 0; i < n; ++i) {
             if (order_out) order_out[i] = is[i];
@@ -1988,7 +2091,7 @@ int32_t foggy_tree_boxes(foggy_handle h, int32_t l, int64_t* boxes, int32_t* cou
     TRY(build_tree_dev(h));
     int n = h->N;
     std::vector<unsigned long long> ks(n);
-    CK(h, cudaMemcpy(ks.data(), h->d_keys_sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    CK(h, d2h(h, ks.data(), h->d_keys_sorted, n * sizeof(unsigned long long)));
     int sh = 3 * (21 - l);
     std::vector<int64_t> u;
     for (int i = 0; i < n; ++i) {
@@ -2019,8 +2122,8 @@ int32_t foggy_tree_domain(foggy_handle h, int32_t l, int64_t n, int32_t kind, in
         const int N = h->N;
         std::vector<unsigned long long> ks(N);
         std::vector<int> is(N);
-        CK(h, cudaMemcpy(ks.data(), h->d_keys_sorted, N * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-        CK(h, cudaMemcpy(is.data(), h->d_idx_sorted, N * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(h, d2h(h, ks.data(), h->d_keys_sorted, N * sizeof(unsigned long long)));
+        CK(h, d2h(h, is.data(), h->d_idx_sorted, N * sizeof(int)));
         std::vector<int64_t> boxes;
         if (kind == 1) boxes.push_back(n);
         else tree_i2(n, l, boxes);
@@ -2186,7 +2289,7 @@ int choose_tile(foggy_handle h, const BlockArgs& ba, const DirectBucket& b, bool
     if (cand.size() > 1) {
         const int nrt = std::min(ba.nrhs, 16);
         cplx* scratch = nullptr;
-        CK(h, cudaMalloc(&scratch, (size_t)nrt * h->n_unk * sizeof(cplx)));
+        CK(h, talloc(h, &scratch, (size_t)nrt * h->n_unk * sizeof(cplx)));
         BlockArgs bt = ba;
         bt.y = scratch;
         bt.nrhs = nrt;
@@ -2216,7 +2319,7 @@ int choose_tile(foggy_handle h, const BlockArgs& ba, const DirectBucket& b, bool
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        cudaFree(scratch);
+        tfree(h, scratch);
         if (err != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("block tile tuning: ") + cudaGetErrorString(err));
     }
     std::lock_guard<std::mutex> lk(g_tile_mu);
