@@ -91,3 +91,47 @@ def test_refusal_and_cancel(native):
             assert rc == N.FOGGY_ERR_STATE
         info1, x1, _ = srv.wait(first)
         assert info1["state"] == N.REQ_DONE and x1 is not None
+
+
+def test_handles_created_and_destroyed_beside_a_solve(native):
+    """Device memory comes from a stream-ordered pool shared by the handles: handles set up, applied
+    and torn down in another thread while a solve runs (their freed blocks going back to the pool and
+    out to the next handle) leave the solve's result bit-identical to the same solve alone, and each
+    churned handle's operator equals the same operator on a quiet GPU."""
+    import threading
+    big = S.random_cluster(40, seed=71, p=8)
+    small = [S.random_cluster(int(n), seed=200 + i, p=int(p)) for i, (n, p) in enumerate([(5, 4), (12, 6), (20, 7)])]
+    with solver.MultiSphereSolver(big) as s:
+        x_alone, _ = s.solve()
+    ref = []
+    for sc in small:
+        v = np.random.default_rng(3).standard_normal(sc.vector_length()) + 0j
+        with solver.MultiSphereSolver(sc) as s:
+            ref.append((v, s.calculate_vector_b(v)))
+    errors, done = [], threading.Event()
+
+    def churn():
+        try:
+            for k in range(30):
+                sc = small[k % len(small)]
+                v, y_ref = ref[k % len(small)]
+                with solver.MultiSphereSolver(sc) as s:
+                    if not np.array_equal(s.calculate_vector_b(v), y_ref):
+                        errors.append("operator of churned handle %d differs" % k)
+        except Exception as e:  # reported by the main thread
+            errors.append(repr(e))
+        finally:
+            done.set()
+
+    t = threading.Thread(target=churn)
+    t.start()
+    solves = 0
+    try:
+        while solves < 3 or not done.is_set():
+            with solver.MultiSphereSolver(big) as s:
+                x, st = s.solve()
+            assert st["status"] == 0 and np.array_equal(x, x_alone)
+            solves += 1
+    finally:
+        t.join()
+    assert not errors, errors[:3]
