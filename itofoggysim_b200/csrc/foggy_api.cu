@@ -52,6 +52,7 @@ struct foggy_handle_s {
     std::string err;
     std::vector<void*> allocs;   // every device allocation, freed in destroy
     std::map<void*, size_t> alloc_bytes;   // their sizes, returned to the budget when freed
+    std::vector<void*> direct_allocs;      // the ones made by cudaMalloc (kPoolMax and above)
     size_t bytes_in_use = 0;
     size_t budget = 0;
 
@@ -160,6 +161,7 @@ struct foggy_handle_s {
                                      // box-to-sphere, near field
     int fmm_ltotal = 0;              // entries of the twelve lists
     cplx* d_fmm_slab = nullptr;      // box-to-sphere and near-field sums, 2 x n_unk
+    cplx* d_fmm_chunks = nullptr;    // partial sums of passes split into source chunks
     // several right-hand sides in one block (foggy_solve_block, foggy_matvec_block): vectors of
     // nrhs slots, n_unk entries apart
     int blk_nrhs = 0, blk_m = 0;
@@ -218,6 +220,11 @@ static cudaError_t h2d(foggy_handle h, void* dst, const void* src, size_t bytes)
 // the next synchronisation; a freed block is reused by another stream only once its free has run
 // (no dependencies between handles' streams are inserted).
 constexpr uint64_t kPoolKeep = 4ull << 30;
+// Allocations of kPoolMax bytes and more (the pair tables and Krylov bases of large scenes, made
+// once per scene) come from cudaMalloc instead: measured on the 2000-sphere scene, the operator runs
+// 4 % faster over cudaMalloc's mapping of its 107 GB of pair tables than over the pool's, and the
+// pool takes 0.6-1.5 s longer to give them back.
+constexpr uint64_t kPoolMax = 1ull << 30;
 
 cudaMemPool_t device_pool(int device) {
     static std::mutex mu;
@@ -286,12 +293,15 @@ int dalloc(foggy_handle h, T** p, size_t count) {
     if (h->budget && h->bytes_in_use + bytes > h->budget)
         return fail(h, FOGGY_ERR_NOMEM, "device memory budget exceeded (" + std::to_string(h->bytes_in_use + bytes) +
                                             " > " + std::to_string(h->budget) + " bytes)");
-    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, h->pool, h->stream);
+    const bool direct = bytes >= kPoolMax;
+    cudaError_t e = direct ? cudaMalloc(reinterpret_cast<void**>(p), bytes)
+                           : cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, h->pool, h->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
         return fail(h, FOGGY_ERR_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
     }
+    if (direct) h->direct_allocs.push_back(*p);
     h->allocs.push_back(*p);
     h->alloc_bytes[*p] = bytes;
     h->bytes_in_use += bytes;
@@ -308,7 +318,13 @@ void dfree(foggy_handle h, T*& p) {
         h->bytes_in_use -= std::min(h->bytes_in_use, sz->second);
         h->alloc_bytes.erase(sz);
     }
-    cudaFreeAsync(p, h->stream);
+    auto d = std::find(h->direct_allocs.begin(), h->direct_allocs.end(), (void*)p);
+    if (d != h->direct_allocs.end()) {
+        h->direct_allocs.erase(d);
+        cudaFree(p);   // waits for the device, so for the stream's uses of p
+    } else {
+        cudaFreeAsync(p, h->stream);
+    }
     p = nullptr;
 }
 
@@ -668,9 +684,16 @@ void free_fmm(foggy_handle h) {
     dfree(h, h->d_fmm_D);
     dfree(h, h->d_fmm_list);
     dfree(h, h->d_fmm_slab);
+    dfree(h, h->d_fmm_chunks);
     h->fmm = FmmTree();
     h->fmm_ready = false;
 }
+
+// ML-FMM passes with fewer than kFmmFill targets run kFmmFill / targets CTAs per target (at most
+// kFmmChunks), each over every chunks-th source of the target's list, so that the upper levels'
+// few boxes still fill the GPU; their partial sums need fewer than 2 kFmmFill slabs of one target.
+constexpr int kFmmFill = 148 * 6;
+constexpr int kFmmChunks = 16;
 
 // Octree hierarchy and ML-FMM pass lists of the current scene and tree parameters, built on the
 // device from the sorted keys (k_tree.cu); the host keeps the level bounds only.
@@ -835,6 +858,7 @@ int ensure_fmm(foggy_handle h) {
     if (!rc) rc = dalloc(h, &h->d_fmm_C, (size_t)nbox * 2 * Pg);
     if (!rc) rc = dalloc(h, &h->d_fmm_D, (size_t)nbox * 2 * Pg);
     if (!rc) rc = dalloc(h, &h->d_fmm_slab, 2 * (size_t)h->n_unk);
+    if (!rc) rc = dalloc(h, &h->d_fmm_chunks, (size_t)2 * kFmmFill * 2 * Pg);
     if (rc) {
         cleanup();
         return rc;
@@ -882,7 +906,11 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
     const PointSet B{h->d_fmm_c, h->d_fmm_p, h->d_fmm_off};
     auto pass = [&](PointSet tg, PointSet sr, const cplx* in, cplx* out, int lp, int li, int tbase, int ntgt,
                     double sign, int z, int add, bool shift) {
+        // passes with few targets split each target's sources over several CTAs
+        const int chunks = ntgt > 0 ? std::max(1, std::min(kFmmChunks, (kFmmFill + ntgt - 1) / ntgt)) : 1;
         TransArgs a = base;
+        a.slab = h->d_fmm_chunks;
+        a.slab_ld = 2 * (int64_t)h->pg * (h->pg + 2);
         a.tgt = tg;
         a.src = sr;
         a.x = in;
@@ -894,8 +922,8 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
         for (int d = 0; d < 3; ++d) a.sh[d] = shift ? h->fmm_xmin[d] : 0.0;
         a.z = z;
         a.add = add;
-        launch_translate(a, ntgt, h->stream);
-        if (ntgt > 0) h->launches += 1;
+        launch_translate(a, ntgt, chunks, h->stream);
+        if (ntgt > 0) h->launches += chunks > 1 ? 2 : 1;
     };
     Trace tr("ML-FMM operator");
     // upward: aggregation at the leaves, then M2M level by level
@@ -1312,9 +1340,13 @@ int32_t foggy_create(const foggy_params* params, int32_t device, foggy_handle* o
 int32_t foggy_destroy(foggy_handle h) {
     if (!h) return FOGGY_OK;
     cudaSetDevice(h->device);
-    for (void* p : h->allocs) cudaFreeAsync(p, h->stream);
-    h->allocs.clear();
+    for (void* p : h->allocs)
+        if (std::find(h->direct_allocs.begin(), h->direct_allocs.end(), p) == h->direct_allocs.end())
+            cudaFreeAsync(p, h->stream);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->direct_allocs) cudaFree(p);
+    h->direct_allocs.clear();
+    h->allocs.clear();
     pinned_release(reinterpret_cast<char*>(h->h_pin));
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : {h->ev0, h->ev1, h->evm0, h->evm1, h->ev_step[0], h->ev_step[1]})

@@ -158,8 +158,12 @@ struct TransArgs {
     const double* delta;
     DTabs dt;
     SGaunt g;
+    cplx* slab;        // chunks > 1: partial sums, chunk c of target i at slab + (c ntargets + i) slab_ld
+    int64_t slab_ld;   // >= 2 P of every target of the pass
 };
-void launch_translate(const TransArgs& a, int ntargets, cudaStream_t s);
+// one pass: ntargets x chunks CTAs (chunks >= 1; with several, slab must hold chunks x ntargets x
+// slab_ld entries)
+void launch_translate(const TransArgs& a, int ntargets, int chunks, cudaStream_t s);
 // single-pair translation for the parity entry point: A, B blocks in the scaled basis
 __global__ void k_translation_pair(AxialView ax, DTabs dt, double x, double theta, double phi, int pn, int pnu,
                                    int z, cplx* A, cplx* B);

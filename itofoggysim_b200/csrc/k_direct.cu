@@ -859,9 +859,11 @@ void launch_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, void*
 }
 
 // ---------------------------------------------------------------------------------------------
-// ML-FMM passes: one CTA per target (sphere or box), the same seven stages per source, S summed
-// from the Gaunt table (the displacements are box geometry, so no pair tables), result written
-// to (or added onto) the target's coefficients.
+// ML-FMM passes: CTAs (target, chunk) over the target's CSR source list, chunk c taking the sources
+// c, c + chunks, ... of the list; the same seven stages per source, S summed from the Gaunt table
+// (the displacements are box geometry, so no pair tables).  With one chunk the result is written to
+// (or added onto) the target's coefficients; with several, each chunk writes its partial sum to its
+// slab and k_translate_sum adds the slabs in chunk order.
 __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     extern __shared__ __align__(16) double smem_d[];
     const int pp = a.pp;
@@ -873,8 +875,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     const int SP = pp * (pp + 3);
     const int XP = pp * (pp + 2);
     const PairCtx<cplx> ctx{s, a.delta, a.dt, a.g, a.z, pp, SP, XP, false};
-    cplx* out = a.out + a.tgt.off[t];
-    for (int e = tid; e < 2 * Pj; e += kThreads) s.acc[e] = a.add ? out[e] : mk(0, 0);
+    const int c = blockIdx.y, chunks = gridDim.y;
+    cplx* out = chunks == 1 ? a.out + a.tgt.off[t]
+                            : a.slab + ((size_t)c * gridDim.x + blockIdx.x) * a.slab_ld;
+    for (int e = tid; e < 2 * Pj; e += kThreads) s.acc[e] = (a.add && chunks == 1) ? out[e] : mk(0, 0);
     for (int e = tid; e < pp * (pp + 3) / 2; e += kThreads) {
         int n, k;
         decode_nk(e, n, k);
@@ -884,17 +888,17 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     auto disp = [&](int l) {
         return Disp{a.tgt.c + 3 * (size_t)t, a.src.c + 3 * (size_t)l, a.k, a.sign, {a.sh[0], a.sh[1], a.sh[2]}};
     };
-    if (i0 < i1) {
-        const int l = a.lidx[i0];
+    if (i0 + c < i1) {
+        const int l = a.lidx[i0 + c];
         prep_pair(s, disp(l), a.z, (const cplx*)nullptr, pj, a.src.p[l], pp, 0, tid, true);
     }
     __syncthreads();
     int cur = 0;
-    for (int i = i0; i < i1; ++i) {
+    for (int i = i0 + c; i < i1; i += chunks) {
         const int l = a.lidx[i];
         run_pair(ctx, tid, pj, a.src.p[l], a.x + a.src.off[l], (const cplx*)nullptr, cur, [&](int tt) {
-            if (i + 1 < i1) {
-                const int ln = a.lidx[i + 1];
+            if (i + chunks < i1) {
+                const int ln = a.lidx[i + chunks];
                 prep_pair(s, disp(ln), a.z, (const cplx*)nullptr, pj, a.src.p[ln], pp, cur ^ 1, tt, true);
             }
         });
@@ -903,11 +907,24 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     for (int e = tid; e < 2 * Pj; e += kThreads) out[e] = s.acc[e];
 }
 
-void launch_translate(const TransArgs& a, int ntargets, cudaStream_t s) {
+// out (+)= the sum of the chunks' slabs in chunk order, one CTA per target
+__global__ void k_translate_sum(TransArgs a, int chunks) {
+    const int t = a.tbase + blockIdx.x;
+    const int P2 = 2 * a.tgt.p[t] * (a.tgt.p[t] + 2);
+    cplx* out = a.out + a.tgt.off[t];
+    for (int e = threadIdx.x; e < P2; e += blockDim.x) {
+        cplx v = a.add ? out[e] : mk(0, 0);
+        for (int c = 0; c < chunks; ++c) v = v + a.slab[((size_t)c * gridDim.x + blockIdx.x) * a.slab_ld + e];
+        out[e] = v;
+    }
+}
+
+void launch_translate(const TransArgs& a, int ntargets, int chunks, cudaStream_t s) {
     if (ntargets <= 0) return;
     size_t smem = smem_bytes<cplx>(a.pp, false);
     raise_smem_ceiling(reinterpret_cast<const void*>(k_translate), smem);
-    k_translate<<<ntargets, kThreads, smem, s>>>(a);
+    k_translate<<<dim3(ntargets, chunks), kThreads, smem, s>>>(a);
+    if (chunks > 1) k_translate_sum<<<ntargets, 256, 0, s>>>(a, chunks);
 }
 
 // ---------------------------------------------------------------------------------------------
