@@ -12,6 +12,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -162,6 +163,10 @@ struct foggy_handle_s {
     int fmm_ltotal = 0;              // entries of the twelve lists
     cplx* d_fmm_slab = nullptr;      // box-to-sphere and near-field sums, 2 x n_unk
     cplx* d_fmm_chunks = nullptr;    // partial sums of passes split into source chunks
+    cplx* d_fmm_tab = nullptr;       // coaxial blocks of the passes' distinct translations
+    int64_t* d_fmm_taboff = nullptr; // per list entry, its block's offset in d_fmm_tab
+    bool fmm_tab_ready = false;
+    int fmm_tab_key[4] = {0, 0, 0, 0};   // (convention, z_coupling, z_translation_gt_r, on)
     // several right-hand sides in one block (foggy_solve_block, foggy_matvec_block): vectors of
     // nrhs slots, n_unk entries apart
     int blk_nrhs = 0, blk_m = 0;
@@ -685,6 +690,9 @@ void free_fmm(foggy_handle h) {
     dfree(h, h->d_fmm_list);
     dfree(h, h->d_fmm_slab);
     dfree(h, h->d_fmm_chunks);
+    dfree(h, h->d_fmm_tab);
+    dfree(h, h->d_fmm_taboff);
+    h->fmm_tab_ready = false;
     h->fmm = FmmTree();
     h->fmm_ready = false;
 }
@@ -880,6 +888,134 @@ int ensure_fmm(foggy_handle h) {
     return FOGGY_OK;
 }
 
+// One ML-FMM pass: targets tbase .. tbase + ntgt - 1 of tg over their lists (ptr list lp, index list
+// li) of sources in sr, displacement sign and shift, radial function z; in -> out (add: out +=).
+struct FmmPass {
+    PointSet tg, sr;
+    const cplx* in;
+    cplx* out;
+    int lp, li, tbase, ntgt;
+    double sign;
+    int z, add;
+    bool shift;
+};
+
+TransArgs fmm_pass_args(foggy_handle h, const TransArgs& base, const FmmPass& q) {
+    TransArgs a = base;
+    const int* L = h->d_fmm_list;
+    const int* lo = h->fmm_lofs;
+    a.slab = h->d_fmm_chunks;
+    a.slab_ld = 2 * (int64_t)h->pg * (h->pg + 2);
+    a.tgt = q.tg;
+    a.src = q.sr;
+    a.x = q.in;
+    a.out = q.out;
+    a.lptr = L + lo[q.lp] + (q.lp == 0 || q.lp >= 8 ? 0 : q.tbase);
+    a.lidx = L + lo[q.li];
+    a.tbase = q.tbase;
+    a.sign = q.sign;
+    for (int d = 0; d < 3; ++d) a.sh[d] = q.shift ? h->fmm_xmin[d] : 0.0;
+    a.z = q.z;
+    a.add = q.add;
+    return a;
+}
+
+// The coaxial blocks of the passes' translations, cached like the direct operator's pair tables
+// (pair_tables -1 = off, 0 = when they fit beside the Krylov basis, 1 = always).  Translations of
+// one index list share their radial function, displacement rule and degrees, and within a level
+// the box displacements repeat, so each list keeps one block per distinct (length, target degree,
+// source degree): the lengths come from the device (k_fmm_rho, rounded as the passes round them),
+// the host groups them, and k_fmm_tab sums each block once, as the passes would sum it per
+// translation.  The passes then read S from the blocks, with the same result bit for bit.
+int ensure_fmm_tables(foggy_handle h, const TransArgs& base, const std::vector<FmmPass>& passes) {
+    const int key[4] = {h->prm.fmm_convention, h->prm.z_coupling, h->prm.z_translation_gt_r, h->prm.pair_tables >= 0};
+    if (h->fmm_tab_ready && std::equal(key, key + 4, h->fmm_tab_key)) return FOGGY_OK;
+    dfree(h, h->d_fmm_tab);
+    dfree(h, h->d_fmm_taboff);
+    h->fmm_tab_ready = false;
+    std::copy(key, key + 4, h->fmm_tab_key);
+    if (h->prm.pair_tables < 0) {
+        h->fmm_tab_ready = true;   // off: the passes sum S from the Gaunt table
+        return FOGGY_OK;
+    }
+    const int total = h->fmm_ltotal;
+    double* d_rho = nullptr;
+    int2* d_deg = nullptr;
+    CK(h, talloc(h, &d_rho, (size_t)total * sizeof(double)));
+    CK(h, talloc(h, &d_deg, (size_t)total * sizeof(int2)));
+    CK(h, cudaMemsetAsync(d_deg, 0xff, (size_t)total * sizeof(int2), h->stream));   // -1: no pass
+    int z_of[12];
+    std::fill(z_of, z_of + 12, 0);
+    for (const FmmPass& q : passes) {
+        if (q.ntgt <= 0) continue;
+        const TransArgs a = fmm_pass_args(h, base, q);
+        k_fmm_rho<<<q.ntgt, 128, 0, h->stream>>>(a, d_rho + h->fmm_lofs[q.li], d_deg + h->fmm_lofs[q.li]);
+        h->launches += 1;
+        z_of[q.li] = q.z;
+    }
+    std::vector<double> rho(total);
+    std::vector<int2> deg(total);
+    cudaError_t e = cudaMemcpyAsync(rho.data(), d_rho, (size_t)total * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(deg.data(), d_deg, (size_t)total * sizeof(int2), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    tfree(h, d_rho);
+    tfree(h, d_deg);
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("ML-FMM tables: ") + cudaGetErrorString(e));
+    // per index list, one block per distinct (length bits, degrees)
+    std::vector<int64_t> off(total, -1);
+    std::vector<FmmTabEntry> uniq;
+    std::vector<std::pair<int, int>> list_range;   // (first unique entry, count) per index list
+    int64_t entries = 0;
+    for (int li = 1; li < 12; li += 2) {
+        const int lo = h->fmm_lofs[li], hi = li + 1 < 12 ? h->fmm_lofs[li + 1] : total;
+        std::map<std::tuple<uint64_t, int, int>, int64_t> seen;
+        const int first = (int)uniq.size();
+        for (int i = lo; i < hi; ++i) {
+            if (deg[i].x < 0) continue;
+            uint64_t bits;
+            std::memcpy(&bits, &rho[i], sizeof(bits));
+            const auto k = std::make_tuple(bits, deg[i].x, deg[i].y);
+            auto it = seen.find(k);
+            if (it == seen.end()) {
+                it = seen.emplace(k, entries).first;
+                uniq.push_back(FmmTabEntry{rho[i], deg[i].x, deg[i].y, entries});
+                entries += pair_block_size(deg[i].y, deg[i].x);
+            }
+            off[i] = it->second;
+        }
+        list_range.emplace_back(first, (int)uniq.size() - first);
+    }
+    const size_t need = (size_t)entries * sizeof(cplx) + (size_t)total * sizeof(int64_t);
+    const size_t room = h->budget > h->bytes_in_use ? h->budget - h->bytes_in_use : 0;
+    const size_t reserve = (size_t)(h->prm.gmres_restart + 4) * (size_t)h->n_unk * sizeof(cplx) + ((size_t)1 << 30);
+    if (h->prm.pair_tables == 0 && need + reserve > room) {
+        h->fmm_tab_ready = true;   // do not fit: the passes sum S from the Gaunt table
+        return FOGGY_OK;
+    }
+    Trace tr("ML-FMM tables");
+    TRY(dalloc(h, &h->d_fmm_tab, (size_t)std::max<int64_t>(entries, 1)));
+    TRY(dalloc(h, &h->d_fmm_taboff, (size_t)total));
+    FmmTabEntry* d_u = nullptr;
+    CK(h, talloc(h, &d_u, std::max<size_t>(uniq.size(), 1) * sizeof(FmmTabEntry)));
+    e = cudaMemcpyAsync(h->d_fmm_taboff, off.data(), (size_t)total * sizeof(int64_t), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && !uniq.empty())
+        e = cudaMemcpyAsync(d_u, uniq.data(), uniq.size() * sizeof(FmmTabEntry), cudaMemcpyHostToDevice, h->stream);
+    const SGaunt g{h->d_koffS, h->d_gs, h->gs_nm};
+    for (int r = 0; r < (int)list_range.size() && e == cudaSuccess; ++r) {
+        const int li = 2 * r + 1;
+        if (list_range[r].second == 0) continue;
+        k_fmm_tab<<<list_range[r].second, 256, 0, h->stream>>>(d_u + list_range[r].first, g, z_of[li], h->d_fmm_tab);
+        h->launches += 1;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);   // the host vectors go out of scope
+    tfree(h, d_u);
+    if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("ML-FMM tables: ") + cudaGetErrorString(e));
+    h->fmm_tab_ready = true;
+    return FOGGY_OK;
+}
+
 // y = A x by the ML-FMM passes (upward :387-640, downward :656-982, final summation :994-1204;
 // the Mie handles lib_mie_ms_ml_fmm_interface.f90:259-981), in the device layout.
 int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
@@ -893,8 +1029,6 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
     const int nlev = t.lmax - t.lmin + 1;
     const int nbox = t.level_base[nlev];
     const int leaf0 = t.level_base[nlev - 1];
-    const int* L = h->d_fmm_list;
-    const int* lo = h->fmm_lofs;
     SceneView sv = scene_view(h);
     TransArgs base{};
     base.delta = h->d_delta;
@@ -904,57 +1038,44 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
     base.pp = h->pg;
     const PointSet S{h->d_centres, h->d_p, h->d_off};
     const PointSet B{h->d_fmm_c, h->d_fmm_p, h->d_fmm_off};
-    auto pass = [&](PointSet tg, PointSet sr, const cplx* in, cplx* out, int lp, int li, int tbase, int ntgt,
-                    double sign, int z, int add, bool shift) {
-        // passes with few targets split each target's sources over several CTAs
-        const int chunks = ntgt > 0 ? std::max(1, std::min(kFmmChunks, (kFmmFill + ntgt - 1) / ntgt)) : 1;
-        TransArgs a = base;
-        a.slab = h->d_fmm_chunks;
-        a.slab_ld = 2 * (int64_t)h->pg * (h->pg + 2);
-        a.tgt = tg;
-        a.src = sr;
-        a.x = in;
-        a.out = out;
-        a.lptr = L + lo[lp] + (lp == 0 || lp >= 8 ? 0 : tbase);
-        a.lidx = L + lo[li];
-        a.tbase = tbase;
-        a.sign = sign;
-        for (int d = 0; d < 3; ++d) a.sh[d] = shift ? h->fmm_xmin[d] : 0.0;
-        a.z = z;
-        a.add = add;
-        launch_translate(a, ntgt, chunks, h->stream);
-        if (ntgt > 0) h->launches += chunks > 1 ? 2 : 1;
+    // the passes in order: upward (aggregation at the leaves, then M2M level by level), downward
+    // (M2L on every level, then L2L from the coarsest level down), final summation (box to
+    // sphere, near field)
+    std::vector<FmmPass> passes;
+    const char* names[6] = {"aggregation", "M2M", "M2L", "L2L", "box to sphere", "near field"};
+    std::vector<int> stage;
+    auto add = [&](int st, PointSet tg, PointSet sr, const cplx* in, cplx* out, int lp, int li, int tbase, int ntgt,
+                   double sign, int z, int addflag, bool shift) {
+        passes.push_back(FmmPass{tg, sr, in, out, lp, li, tbase, ntgt, sign, z, addflag, shift});
+        stage.push_back(st);
     };
+    add(0, B, S, x, h->d_fmm_C, 0, 1, leaf0, nbox - leaf0, sts, z_reg, 0, false);
+    for (int li = nlev - 2; li >= 0; --li)
+        add(1, B, B, h->d_fmm_C, h->d_fmm_C, 2, 3, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
+            z_reg, 0, false);
+    for (int li = 0; li < nlev; ++li)
+        add(2, B, B, h->d_fmm_C, h->d_fmm_D, 4, 5, t.level_base[li], t.level_base[li + 1] - t.level_base[li], sts, zi,
+            0, false);
+    for (int li = 1; li < nlev; ++li)
+        add(3, B, B, h->d_fmm_D, h->d_fmm_D, 6, 7, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
+            z_reg, 1, false);
+    add(4, S, B, h->d_fmm_D, h->d_fmm_slab, 8, 9, 0, h->N, sts, z_dor, 0, conv == 0);
+    add(5, S, S, x, h->d_fmm_slab + h->n_unk, 10, 11, 0, h->N, 1.0, zi, 0, false);
+    TRY(ensure_fmm_tables(h, base, passes));
+    const bool tabs = h->d_fmm_taboff != nullptr;
     Trace tr("ML-FMM operator");
-    // upward: aggregation at the leaves, then M2M level by level
-    {
-        Trace tp("aggregation");
-        pass(B, S, x, h->d_fmm_C, 0, 1, leaf0, nbox - leaf0, sts, z_reg, 0, false);
-    }
-    {
-        Trace tp("M2M");
-        for (int li = nlev - 2; li >= 0; --li)
-            pass(B, B, h->d_fmm_C, h->d_fmm_C, 2, 3, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
-                 z_reg, 0, false);
-    }
-    // downward: M2L on every level, then L2L from the coarsest level down
-    {
-        Trace tp("M2L");
-        for (int li = 0; li < nlev; ++li)
-            pass(B, B, h->d_fmm_C, h->d_fmm_D, 4, 5, t.level_base[li], t.level_base[li + 1] - t.level_base[li], sts,
-                 zi, 0, false);
-    }
-    {
-        Trace tp("L2L");
-        for (int li = 1; li < nlev; ++li)
-            pass(B, B, h->d_fmm_D, h->d_fmm_D, 6, 7, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
-                 z_reg, 1, false);
-    }
-    // final summation: box to sphere, near field, then y = x + T (both)
-    {
-        Trace tp("box to sphere, near field");
-        pass(S, B, h->d_fmm_D, h->d_fmm_slab, 8, 9, 0, h->N, sts, z_dor, 0, conv == 0);
-        pass(S, S, x, h->d_fmm_slab + h->n_unk, 10, 11, 0, h->N, 1.0, zi, 0, false);
+    for (size_t i = 0; i < passes.size(); ++i) {
+        const FmmPass& q = passes[i];
+        Trace tp(names[stage[i]]);
+        TransArgs a = fmm_pass_args(h, base, q);
+        if (tabs) {
+            a.tab = h->d_fmm_tab;
+            a.tab_off = h->d_fmm_taboff + h->fmm_lofs[q.li];
+        }
+        // passes with few targets split each target's sources over several CTAs
+        const int chunks = q.ntgt > 0 ? std::max(1, std::min(kFmmChunks, (kFmmFill + q.ntgt - 1) / q.ntgt)) : 1;
+        launch_translate(a, q.ntgt, chunks, h->stream);
+        if (q.ntgt > 0) h->launches += chunks > 1 ? 2 : 1;
     }
     CKL(h);
     k_direct_finish<<<h->N, 256, 0, h->stream>>>(sv, x, h->d_fmm_slab, 2, h->n_unk, y);

@@ -160,7 +160,17 @@ struct TransArgs {
     SGaunt g;
     cplx* slab;        // chunks > 1: partial sums, chunk c of target i at slab + (c ntargets + i) slab_ld
     int64_t slab_ld;   // >= 2 P of every target of the pass
+    const cplx* tab;         // coaxial blocks of the pass's translations (k_fmm_tab), or null:
+    const int64_t* tab_off;  // entry i's block at tab + tab_off[i] (aligned with lidx)
 };
+// a distinct translation of an ML-FMM pass: its length, degrees and block offset in the tables
+struct FmmTabEntry {
+    double rho;
+    int pt, ps;
+    int64_t off;
+};
+__global__ void k_fmm_rho(TransArgs a, double* rho, int2* deg);
+__global__ void k_fmm_tab(const FmmTabEntry* u, SGaunt g, int z, cplx* tab);
 // one pass: ntargets x chunks CTAs (chunks >= 1; with several, slab must hold chunks x ntargets x
 // slab_ld entries)
 void launch_translate(const TransArgs& a, int ntargets, int chunks, cudaStream_t s);

@@ -197,6 +197,16 @@ struct Disp {
     double sh[3];
 };
 
+// The scaled displacement d = k (sign (c_s - c_t) + sh) of a translation and its length, rounded
+// the same way wherever it is computed (the translations, and the ML-FMM table set-up that keys
+// its coaxial blocks by this length).
+__device__ __forceinline__ double disp_vec(const Disp& g, double& d0, double& d1, double& d2) {
+    d0 = __dmul_rn(g.k, __fma_rn(g.sign, __dsub_rn(g.cs[0], g.ct[0]), g.sh[0]));
+    d1 = __dmul_rn(g.k, __fma_rn(g.sign, __dsub_rn(g.cs[1], g.ct[1]), g.sh[1]));
+    d2 = __dmul_rn(g.k, __fma_rn(g.sign, __dsub_rn(g.cs[2], g.ct[2]), g.sh[2]));
+    return sqrt(__fma_rn(d0, d0, __fma_rn(d1, d1, __dmul_rn(d2, d2))));
+}
+
 // Geometry of one translation and the phase tables of buffer b, spread over fixed threads:
 // tid <= pq the azimuthal phases, 64 <= tid <= 64 + pq the polar ones, 100/101 the Bessel
 // functions (only without pair tables), the last thread the distance; with a coaxial block
@@ -226,10 +236,8 @@ __device__ inline void prep_pair(const Bufs<C>& s, const Disp& g, int z, const C
         }
     }
     if (!(e1 || e2 || e3 || e4)) return;
-    const double d0 = g.k * (g.sign * (g.cs[0] - g.ct[0]) + g.sh[0]);
-    const double d1 = g.k * (g.sign * (g.cs[1] - g.ct[1]) + g.sh[1]);
-    const double d2 = g.k * (g.sign * (g.cs[2] - g.ct[2]) + g.sh[2]);
-    const double r = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    double d0, d1, d2;
+    const double r = disp_vec(g, d0, d1, d2);
     if (e1) {
         const double ph = (d0 == 0.0 && d1 == 0.0) ? 0.0 : atan2(d1, d0);
         double sn, cs;
@@ -874,7 +882,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     const int Pj = pj * (pj + 2);
     const int SP = pp * (pp + 3);
     const int XP = pp * (pp + 2);
-    const PairCtx<cplx> ctx{s, a.delta, a.dt, a.g, a.z, pp, SP, XP, false};
+    const bool tabs = a.tab_off != nullptr;
+    const PairCtx<cplx> ctx{s, a.delta, a.dt, a.g, a.z, pp, SP, XP, tabs};
+    auto block = [&](int i) -> const cplx* { return tabs ? a.tab + a.tab_off[i] : nullptr; };
     const int c = blockIdx.y, chunks = gridDim.y;
     cplx* out = chunks == 1 ? a.out + a.tgt.off[t]
                             : a.slab + ((size_t)c * gridDim.x + blockIdx.x) * a.slab_ld;
@@ -890,21 +900,82 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     };
     if (i0 + c < i1) {
         const int l = a.lidx[i0 + c];
-        prep_pair(s, disp(l), a.z, (const cplx*)nullptr, pj, a.src.p[l], pp, 0, tid, true);
+        prep_pair(s, disp(l), a.z, block(i0 + c), pj, a.src.p[l], pp, 0, tid, !tabs);
     }
     __syncthreads();
     int cur = 0;
     for (int i = i0 + c; i < i1; i += chunks) {
         const int l = a.lidx[i];
-        run_pair(ctx, tid, pj, a.src.p[l], a.x + a.src.off[l], (const cplx*)nullptr, cur, [&](int tt) {
+        run_pair(ctx, tid, pj, a.src.p[l], a.x + a.src.off[l], block(i), cur, [&](int tt) {
             if (i + chunks < i1) {
                 const int ln = a.lidx[i + chunks];
-                prep_pair(s, disp(ln), a.z, (const cplx*)nullptr, pj, a.src.p[ln], pp, cur ^ 1, tt, true);
+                prep_pair(s, disp(ln), a.z, block(i + chunks), pj, a.src.p[ln], pp, cur ^ 1, tt, !tabs);
             }
         });
         cur ^= 1;
     }
     for (int e = tid; e < 2 * Pj; e += kThreads) out[e] = s.acc[e];
+}
+
+// The ML-FMM's coaxial blocks: for every entry i of a pass's source lists, the translation's
+// length rho (disp_vec, as the pass computes it) and degrees (target, source); one CTA per target.
+__global__ void k_fmm_rho(TransArgs a, double* rho, int2* deg) {
+    const int t = a.tbase + blockIdx.x;
+    const int i0 = a.lptr[blockIdx.x], i1 = a.lptr[blockIdx.x + 1];
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const int l = a.lidx[i];
+        const Disp g{a.tgt.c + 3 * (size_t)t, a.src.c + 3 * (size_t)l, a.k, a.sign, {a.sh[0], a.sh[1], a.sh[2]}};
+        double d0, d1, d2;
+        rho[i] = disp_vec(g, d0, d1, d2);
+        deg[i] = make_int2(a.tgt.p[t], a.src.p[l]);
+    }
+}
+
+// One coaxial block per distinct (rho, target degree, source degree) of a pass: S(k; mu, n) summed
+// from the scalar Gaunt table exactly as the translation stage sums it without tables (radial
+// functions to degree p_t + p_s + 1, the same terms in the same order), on the square layout of
+// the pair tables; entries the translation never reads (mu > p_s + 1 or n > p_t) are zero.
+__global__ void __launch_bounds__(256) k_fmm_tab(const FmmTabEntry* u, SGaunt g, int z, cplx* tab) {
+    __shared__ double jb[2 * kMaxDegree + 8], yb[2 * kMaxDegree + 8];
+    __shared__ cplx zeta[2 * kMaxDegree + 8];
+    const FmmTabEntry e = u[blockIdx.x];
+    const int M2 = max(e.pt, e.ps) + 2;
+    const int P = e.pt + e.ps + 1;
+    const int km = min(e.pt, e.ps);
+    const int64_t tot = pair_block_size(e.ps, e.pt);
+    cplx* out = tab + e.off;
+    if (e.rho == 0.0) {   // coincident centres: the translation adds its source unchanged
+        for (int64_t q = threadIdx.x; q < tot; q += blockDim.x) out[q] = mk(0, 0);
+        return;
+    }
+    if (threadIdx.x == 0) dev_sph_jn(e.rho, P, jb);
+    if (threadIdx.x == 32 && z != 1) dev_sph_yn(e.rho, P, yb);
+    __syncthreads();
+    for (int p = threadIdx.x; p <= P; p += blockDim.x) zeta[p] = zeta_of(z, p, jb, yb);
+    __syncthreads();
+    for (int64_t q = threadIdx.x; q < tot; q += blockDim.x) {
+        int k = 0;
+        while (k < km && pair_block_offset(k + 1, M2, M2) <= q) ++k;
+        const int64_t r = q - pair_block_offset(k, M2, M2);
+        const int cols = M2 - k;
+        const int mu = k + (int)(r / cols), n = k + (int)(r % cols);
+        if (mu > e.ps + 1 || n > e.pt) {
+            out[q] = mk(0, 0);
+            continue;
+        }
+        const int W = g.NM - k + 1;
+        const size_t plane = (size_t)W * W;
+        const double* gp = g.gs + g.koff[k] + (size_t)(mu - k) * W + (n - k);
+        const int qm = min(n, mu);
+        int p = n + mu;
+        double sx = 0.0, sy = 0.0;
+        for (int qq = 0; qq <= qm; ++qq, p -= 2) {
+            const double gq = __ldg(gp + qq * plane);
+            sx += gq * zeta[p].x;
+            sy += gq * zeta[p].y;
+        }
+        out[q] = mk(sx, sy);
+    }
 }
 
 // out (+)= the sum of the chunks' slabs in chunk order, one CTA per target

@@ -142,6 +142,29 @@ def test_fmm_matvec_matches_oracle(native, oracle, n, p, z, conv, rule, lmax):
     assert np.array_equal(y, y2), "FMM operator is not bit-reproducible"
 
 
+@pytest.mark.parametrize("n,p,z,conv,rule,lmax", CASES)
+def test_fmm_tables_equal_gaunt_sums(native, n, p, z, conv, rule, lmax):
+    """The passes' cached coaxial blocks (one per distinct translation length and degrees of each
+    pass list) against S summed from the Gaunt table per translation (pair_tables = -1): the same
+    operator bit for bit, in both conventions (the reference's shifted box-to-sphere step
+    included), and the same again after the radial function changes (the blocks are rebuilt)."""
+    sc = S.random_cluster(n, seed=n + (p or 0), p=p, z_coupling=z, reference_row_rule=rule)
+    sc.tree_l_max = lmax
+    x = _x(sc, 4)
+    out = {}
+    for pt in (0, -1):
+        with solver.MultiSphereSolver(sc, use_ml_fmm=True, fmm_convention=conv, z_translation_gt_r=3,
+                                      pair_tables=pt) as s:
+            y1 = s.calculate_vector_b(x)
+            s.params.z_coupling = 4 if z != 4 else 3
+            s._set()
+            y2 = s.calculate_vector_b(x)
+        out[pt] = (y1, y2)
+    assert np.array_equal(out[0][0], out[-1][0])
+    assert np.array_equal(out[0][1], out[-1][1])
+    assert not np.array_equal(out[0][0], out[0][1])
+
+
 def test_consistent_fmm_close_to_direct(native, oracle):
     sc = long_wave_scene(8)
     x = _x(sc, 5)
