@@ -88,12 +88,12 @@ typedef struct foggy_params {
                                     tends to the direct operator as the order grows        */
     int32_t z_translation_gt_r;  /* radial function of the box-to-sphere step in convention 0
                                     (the reference's tests set 3)                          */
-    int32_t precision;           /* 0: FP64 throughout; 1: mixed (direct operator only): the
-                                    Arnoldi steps apply the operator in FP32 (single-precision
-                                    pair tables, rotations and coaxial sums; FP64 vectors), the
-                                    true residual at the start and at every restart in FP64, so
-                                    the restarts refine to gmres_tolerance.  foggy_matvec stays
-                                    FP64.                                                   */
+    int32_t precision;           /* 0: FP64 throughout; 1: mixed: the Arnoldi steps apply the
+                                    operator (direct or ML-FMM) in FP32 (single-precision
+                                    coaxial blocks, rotations and coaxial sums; FP64 vectors
+                                    and box coefficients), the true residual at the start and
+                                    at every restart in FP64, so the restarts refine to
+                                    gmres_tolerance.  foggy_matvec stays FP64.               */
 } foggy_params;
 
 /* Per-solve statistics (the reference prints these; here they are returned). */

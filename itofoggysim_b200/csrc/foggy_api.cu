@@ -165,8 +165,9 @@ struct foggy_handle_s {
     cplx* d_fmm_chunks = nullptr;    // partial sums of passes split into source chunks
     cplx* d_fmm_tab = nullptr;       // coaxial blocks of the passes' distinct translations
     int64_t* d_fmm_taboff = nullptr; // per list entry, its block's offset in d_fmm_tab
+    cplxf* d_fmm_tab32 = nullptr;    // the blocks in single precision (mixed-precision solves)
     bool fmm_tab_ready = false;
-    int fmm_tab_key[4] = {0, 0, 0, 0};   // (convention, z_coupling, z_translation_gt_r, on)
+    int fmm_tab_key[5] = {0, 0, 0, 0, 0};   // (convention, z_coupling, z_translation_gt_r, on, precision)
     // several right-hand sides in one block (foggy_solve_block, foggy_matvec_block): vectors of
     // nrhs slots, n_unk entries apart
     int blk_nrhs = 0, blk_m = 0;
@@ -692,6 +693,7 @@ void free_fmm(foggy_handle h) {
     dfree(h, h->d_fmm_chunks);
     dfree(h, h->d_fmm_tab);
     dfree(h, h->d_fmm_taboff);
+    dfree(h, h->d_fmm_tab32);
     h->fmm_tab_ready = false;
     h->fmm = FmmTree();
     h->fmm_ready = false;
@@ -928,12 +930,14 @@ TransArgs fmm_pass_args(foggy_handle h, const TransArgs& base, const FmmPass& q)
 // the host groups them, and k_fmm_tab sums each block once, as the passes would sum it per
 // translation.  The passes then read S from the blocks, with the same result bit for bit.
 int ensure_fmm_tables(foggy_handle h, const TransArgs& base, const std::vector<FmmPass>& passes) {
-    const int key[4] = {h->prm.fmm_convention, h->prm.z_coupling, h->prm.z_translation_gt_r, h->prm.pair_tables >= 0};
-    if (h->fmm_tab_ready && std::equal(key, key + 4, h->fmm_tab_key)) return FOGGY_OK;
+    const int key[5] = {h->prm.fmm_convention, h->prm.z_coupling, h->prm.z_translation_gt_r, h->prm.pair_tables >= 0,
+                        h->prm.precision};
+    if (h->fmm_tab_ready && std::equal(key, key + 5, h->fmm_tab_key)) return FOGGY_OK;
     dfree(h, h->d_fmm_tab);
     dfree(h, h->d_fmm_taboff);
+    dfree(h, h->d_fmm_tab32);
     h->fmm_tab_ready = false;
-    std::copy(key, key + 4, h->fmm_tab_key);
+    std::copy(key, key + 5, h->fmm_tab_key);
     if (h->prm.pair_tables < 0) {
         h->fmm_tab_ready = true;   // off: the passes sum S from the Gaunt table
         return FOGGY_OK;
@@ -986,7 +990,8 @@ int ensure_fmm_tables(foggy_handle h, const TransArgs& base, const std::vector<F
         }
         list_range.emplace_back(first, (int)uniq.size() - first);
     }
-    const size_t need = (size_t)entries * sizeof(cplx) + (size_t)total * sizeof(int64_t);
+    const bool mixed = h->prm.precision == 1;
+    const size_t need = (size_t)entries * (sizeof(cplx) + (mixed ? sizeof(cplxf) : 0)) + (size_t)total * sizeof(int64_t);
     const size_t room = h->budget > h->bytes_in_use ? h->budget - h->bytes_in_use : 0;
     const size_t reserve = (size_t)(h->prm.gmres_restart + 4) * (size_t)h->n_unk * sizeof(cplx) + ((size_t)1 << 30);
     if (h->prm.pair_tables == 0 && need + reserve > room) {
@@ -1009,6 +1014,17 @@ int ensure_fmm_tables(foggy_handle h, const TransArgs& base, const std::vector<F
         h->launches += 1;
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess && mixed) {
+        const int rc = dalloc(h, &h->d_fmm_tab32, (size_t)std::max<int64_t>(entries, 1));
+        if (rc) {
+            tfree(h, d_u);
+            return rc;
+        }
+        k_narrow<<<(unsigned)std::min<int64_t>((entries + 255) / 256 + 1, 148 * 8), 256, 0, h->stream>>>(
+            h->d_fmm_tab, h->d_fmm_tab32, entries);
+        h->launches += 1;
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);   // the host vectors go out of scope
     tfree(h, d_u);
     if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("ML-FMM tables: ") + cudaGetErrorString(e));
@@ -1018,7 +1034,9 @@ int ensure_fmm_tables(foggy_handle h, const TransArgs& base, const std::vector<F
 
 // y = A x by the ML-FMM passes (upward :387-640, downward :656-982, final summation :994-1204;
 // the Mie handles lib_mie_ms_ml_fmm_interface.f90:259-981), in the device layout.
-int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
+// fp32: translations in single precision (the Arnoldi steps of a mixed-precision solve); the box
+// coefficients, the chunks' partial sums and y stay FP64.
+int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y, bool fp32 = false) {
     TRY(ensure_fmm(h));
     const FmmTree& t = h->fmm;
     const int conv = h->prm.fmm_convention;
@@ -1036,6 +1054,8 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
     base.g = SGaunt{h->d_koffS, h->d_gs, h->gs_nm};
     base.k = sv.k;
     base.pp = h->pg;
+    base.fp32 = fp32 ? 1 : 0;
+    base.delta32 = h->d_delta32;
     const PointSet S{h->d_centres, h->d_p, h->d_off};
     const PointSet B{h->d_fmm_c, h->d_fmm_p, h->d_fmm_off};
     // the passes in order: upward (aggregation at the leaves, then M2M level by level), downward
@@ -1062,14 +1082,15 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
     add(4, S, B, h->d_fmm_D, h->d_fmm_slab, 8, 9, 0, h->N, sts, z_dor, 0, conv == 0);
     add(5, S, S, x, h->d_fmm_slab + h->n_unk, 10, 11, 0, h->N, 1.0, zi, 0, false);
     TRY(ensure_fmm_tables(h, base, passes));
-    const bool tabs = h->d_fmm_taboff != nullptr;
-    Trace tr("ML-FMM operator");
+    const bool tabs = h->d_fmm_taboff != nullptr && (!fp32 || h->d_fmm_tab32 != nullptr);
+    Trace tr(fp32 ? "ML-FMM operator (FP32)" : "ML-FMM operator");
     for (size_t i = 0; i < passes.size(); ++i) {
         const FmmPass& q = passes[i];
         Trace tp(names[stage[i]]);
         TransArgs a = fmm_pass_args(h, base, q);
         if (tabs) {
             a.tab = h->d_fmm_tab;
+            a.tab32 = h->d_fmm_tab32;
             a.tab_off = h->d_fmm_taboff + h->fmm_lofs[q.li];
         }
         // passes with few targets split each target's sources over several CTAs
@@ -1087,7 +1108,7 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y) {
 // y = A x in the device layout
 // fp32: the single-precision operator (mixed-precision solves' Arnoldi steps), when its tables exist
 int apply_operator(foggy_handle h, const cplx* x, cplx* y, bool fp32 = false) {
-    if (h->prm.matvec_mode == FOGGY_MATVEC_MLFMM) return apply_operator_fmm(h, x, y);
+    if (h->prm.matvec_mode == FOGGY_MATVEC_MLFMM) return apply_operator_fmm(h, x, y, fp32);
     TRY(ensure_pair_tables(h));
     DirectArgs a = direct_args(h, x);
     a.fp32 = (fp32 && h->stab32_ready) ? 1 : 0;
@@ -1415,8 +1436,6 @@ static int check_params(foggy_handle h, const foggy_params* p) {
     if (p->z_translation_gt_r < 1 || p->z_translation_gt_r > 4)
         return fail(h, FOGGY_ERR_ARGUMENT, "z_translation_gt_r must be 1..4");
     if (p->precision != 0 && p->precision != 1) return fail(h, FOGGY_ERR_ARGUMENT, "precision must be 0 (FP64) or 1 (mixed)");
-    if (p->precision == 1 && p->matvec_mode == FOGGY_MATVEC_MLFMM)
-        return fail(h, FOGGY_ERR_UNSUPPORTED, "mixed precision is built for the direct operator only");
     return FOGGY_OK;
 }
 

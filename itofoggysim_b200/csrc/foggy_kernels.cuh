@@ -162,7 +162,11 @@ struct TransArgs {
     int64_t slab_ld;   // >= 2 P of every target of the pass
     const cplx* tab;         // coaxial blocks of the pass's translations (k_fmm_tab), or null:
     const int64_t* tab_off;  // entry i's block at tab + tab_off[i] (aligned with lidx)
+    int fp32;                // translation arithmetic in single precision (mixed-precision Arnoldi
+    const float* delta32;    // steps): d^j(pi/2) and the blocks in FP32, coefficients kept in FP64
+    const cplxf* tab32;
 };
+__global__ void k_narrow(const cplx* in, cplxf* out, int64_t n);
 // a distinct translation of an ML-FMM pass: its length, degrees and block offset in the tables
 struct FmmTabEntry {
     double rho;

@@ -872,10 +872,11 @@ void launch_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, void*
 // (the displacements are box geometry, so no pair tables).  With one chunk the result is written to
 // (or added onto) the target's coefficients; with several, each chunk writes its partial sum to its
 // slab and k_translate_sum adds the slabs in chunk order.
+template <class C>
 __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     extern __shared__ __align__(16) double smem_d[];
     const int pp = a.pp;
-    const Bufs<cplx> s = carve<cplx>(smem_d, pp, false);
+    const Bufs<C> s = carve<C>(smem_d, pp, false);
     const int t = a.tbase + blockIdx.x;
     const int tid = threadIdx.x;
     const int pj = a.tgt.p[t];
@@ -883,12 +884,21 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
     const int SP = pp * (pp + 3);
     const int XP = pp * (pp + 2);
     const bool tabs = a.tab_off != nullptr;
-    const PairCtx<cplx> ctx{s, a.delta, a.dt, a.g, a.z, pp, SP, XP, tabs};
-    auto block = [&](int i) -> const cplx* { return tabs ? a.tab + a.tab_off[i] : nullptr; };
+    const C* tab;
+    const real_of<C>* delta;
+    if constexpr (sizeof(C) == 8) {
+        tab = a.tab32;
+        delta = a.delta32;
+    } else {
+        tab = a.tab;
+        delta = a.delta;
+    }
+    const PairCtx<C> ctx{s, delta, a.dt, a.g, a.z, pp, SP, XP, tabs};
+    auto block = [&](int i) -> const C* { return tabs ? tab + a.tab_off[i] : nullptr; };
     const int c = blockIdx.y, chunks = gridDim.y;
     cplx* out = chunks == 1 ? a.out + a.tgt.off[t]
                             : a.slab + ((size_t)c * gridDim.x + blockIdx.x) * a.slab_ld;
-    for (int e = tid; e < 2 * Pj; e += kThreads) s.acc[e] = (a.add && chunks == 1) ? out[e] : mk(0, 0);
+    for (int e = tid; e < 2 * Pj; e += kThreads) s.acc[e] = (a.add && chunks == 1) ? cm<C>(out[e].x, out[e].y) : C{0, 0};
     for (int e = tid; e < pp * (pp + 3) / 2; e += kThreads) {
         int n, k;
         decode_nk(e, n, k);
@@ -914,7 +924,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_translate(TransArgs a) {
         });
         cur ^= 1;
     }
-    for (int e = tid; e < 2 * Pj; e += kThreads) out[e] = s.acc[e];
+    for (int e = tid; e < 2 * Pj; e += kThreads) out[e] = mk(s.acc[e].x, s.acc[e].y);
 }
 
 // The ML-FMM's coaxial blocks: for every entry i of a pass's source lists, the translation's
@@ -978,6 +988,12 @@ __global__ void __launch_bounds__(256) k_fmm_tab(const FmmTabEntry* u, SGaunt g,
     }
 }
 
+// single-precision copy of tables
+__global__ void k_narrow(const cplx* in, cplxf* out, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = cplxf{(float)in[i].x, (float)in[i].y};
+}
+
 // out (+)= the sum of the chunks' slabs in chunk order, one CTA per target
 __global__ void k_translate_sum(TransArgs a, int chunks) {
     const int t = a.tbase + blockIdx.x;
@@ -992,9 +1008,15 @@ __global__ void k_translate_sum(TransArgs a, int chunks) {
 
 void launch_translate(const TransArgs& a, int ntargets, int chunks, cudaStream_t s) {
     if (ntargets <= 0) return;
-    size_t smem = smem_bytes<cplx>(a.pp, false);
-    raise_smem_ceiling(reinterpret_cast<const void*>(k_translate), smem);
-    k_translate<<<dim3(ntargets, chunks), kThreads, smem, s>>>(a);
+    if (a.fp32) {
+        const size_t smem = smem_bytes<cplxf>(a.pp, false);
+        raise_smem_ceiling(reinterpret_cast<const void*>(k_translate<cplxf>), smem);
+        k_translate<cplxf><<<dim3(ntargets, chunks), kThreads, smem, s>>>(a);
+    } else {
+        const size_t smem = smem_bytes<cplx>(a.pp, false);
+        raise_smem_ceiling(reinterpret_cast<const void*>(k_translate<cplx>), smem);
+        k_translate<cplx><<<dim3(ntargets, chunks), kThreads, smem, s>>>(a);
+    }
     if (chunks > 1) k_translate_sum<<<ntargets, 256, 0, s>>>(a, chunks);
 }
 

@@ -33,8 +33,21 @@ def test_mixed_solve_matches_fp64(native, case, tables):
     assert st32["restarts"] >= 1
 
 
-def test_mixed_with_mlfmm_is_unsupported(native):
-    sc = S.random_cluster(8, seed=2, p=4)
-    with pytest.raises(N.FoggyError) as e:
-        solver.MultiSphereSolver(sc, use_ml_fmm=True, precision=1)
-    assert e.value.code == N.FOGGY_ERR_UNSUPPORTED
+@pytest.mark.parametrize("tables", [0, -1])
+def test_mixed_mlfmm_solve_matches_fp64(native, tables):
+    """The ML-FMM passes in FP32 in the Arnoldi steps (consistent convention, a scene whose boxes
+    are small against the wavelength): FP64 backward error met, solution within 1e-6 and C_ext within
+    1e-7 of the FP64 ML-FMM solve, with the cached translation blocks and without."""
+    rng = np.random.default_rng(7)
+    sc = S.make_scene(rng.uniform(0.1, 0.3, 40), 10.0, 5, lambda_0=6.0, n_max=8, z_coupling=3,
+                      reference_row_rule=False, tree_l_max=3, gmres_tolerance=1e-8)
+    with solver.MultiSphereSolver(sc, use_ml_fmm=True, fmm_convention=1, pair_tables=tables) as s:
+        x64, st64 = s.solve()
+        c64 = s.cross_sections(x64)
+    with solver.MultiSphereSolver(sc, use_ml_fmm=True, fmm_convention=1, pair_tables=tables, precision=1) as s:
+        x32, st32 = s.solve()
+        c32 = s.cross_sections(x32)
+    assert st64["status"] == 0 and st32["status"] == 0
+    assert st32["backward_error"] <= sc.gmres_tolerance
+    assert np.linalg.norm(x32 - x64) <= 1e-6 * np.linalg.norm(x64)
+    assert abs(c32[1] - c64[1]) <= 1e-7 * abs(c64[1])
