@@ -271,7 +271,7 @@ def cpu_sample(sc, budget_s=15.0, seed=0):
 
 
 def cpu_cached_sample():
-    """BASELINE.md's oracle-direct-cached mode: the oracle's operator with the translation blocks of
+    """The cached CPU mode of the reference algorithm: the oracle's operator with the translation blocks of
     every ordered pair built once and kept (bit-identical to recomputing them), timed on all host cores
     for the 64-sphere cluster, where the cache fits (4032 pairs x 2 blocks of 255^2 complex, 8.4 GB).  Returns seconds per cached application and the seconds the cache took to build."""
     from oracle import oracle as O
@@ -450,8 +450,8 @@ def run_multi_rhs(args):
 
 
 def block_scene(n_spheres):
-    """SURVEY config 4's scene shape at n_spheres: lognormal water spheres (median 0.6 um, sigma_ln 0.3,
-    clipped to 0.2-1.5 um) at config 4's number density (20,000 spheres in a 90 um cube), 64 Fibonacci
+    """The 20,000-sphere 128-right-hand-side scene's shape at n_spheres: lognormal water spheres (median 0.6 um, sigma_ln 0.3,
+    clipped to 0.2-1.5 um) at the number density of 20,000 spheres in a 90 um cube, 64 Fibonacci
     directions x TM/TE = 128 right-hand sides, GMRES(30) to 1e-6."""
     from itofoggysim_b200 import scene as S
     box = 90.0 * (n_spheres / 20000.0) ** (1.0 / 3.0)
@@ -720,6 +720,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-cached", action="store_true",
                     help="also time the oracle with cached translation blocks (about a minute of CPU)")
+    ap.add_argument("--cpu-mlfmm", action="store_true",
+                    help="with --operator mlfmm: also time one application of the oracle's ML-FMM (the "
+                         "reference's passes, translations recomputed exactly; minutes of CPU)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 Arnoldi operator, FP64 true residuals (its own JSON line, with errors "
                          "against an FP64 solve)")
@@ -890,11 +893,24 @@ def main():
             per_solve_c = t_c * cached_scale(sc_small, sc) * (mv_count / args.steps)
             result["cpu_baseline_cached"] = {
                 "value": 1.0 / per_solve_c, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
-                "sample": "oracle operator with every pair's translation blocks cached (BASELINE.md "
-                          "oracle-direct-cached), %.3f s per application of the 64-sphere cluster (cache built in "
+                "sample": "oracle operator with every pair's translation blocks cached "
+                          "(oracle-direct-cached), %.3f s per application of the 64-sphere cluster (cache built in "
                           "%.1f s), scaled by sum_{j!=l} P_j P_l to this scene and x %d matvecs/solve; this "
                           "scene's cache (two P_j x P_l complex blocks per ordered pair) would need "
                           "%.1f GB" % (t_c, t_build, mv_count // args.steps, cached_bytes(sc) / 1e9)}
+        if fmm and args.cpu_mlfmm:
+            from oracle import oracle as O
+            P = O.Problem(sc)
+            xo = P.vector_b()
+            t0 = time.perf_counter()
+            P.fmm_matvec(xo, l_max=sc.tree_l_max, convention=args.fmm_convention, z_gt_r=3)
+            t_f = time.perf_counter() - t0
+            result["cpu_baseline_mlfmm"] = {
+                "value": 1.0 / (t_f * (mv_count / args.steps)), "unit": "solves/s", "cores": os.cpu_count(),
+                "kind": "port",
+                "sample": "one whole application of the oracle's ML-FMM (oracle-mlfmm: the reference's "
+                          "passes and lists, every translation's coefficients recomputed exactly), %.1f s, x %d "
+                          "matvecs/solve" % (t_f, mv_count // args.steps)}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -81,7 +81,7 @@ def test_fibonacci_right_hand_sides():
 
 
 def test_block_workload_scene():
-    """The block workload: config 4's scene shape (lognormal radii at 20,000 spheres per 90 um cube)
+    """The block workload: the 20,000-sphere scene's shape (lognormal radii at 20,000 spheres per 90 um cube)
     at a smaller sphere count, 128 right-hand sides, GMRES(30) to 1e-6."""
     sc = bench.block_scene(500)
     assert sc.n_spheres == 500 and sc.n_waves == 128
