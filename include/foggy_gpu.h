@@ -71,8 +71,11 @@ typedef struct foggy_params {
     double  gmres_tolerance;     /* stop when ||b - A x|| / ||b|| <= tolerance              */
     int32_t tree_l_max;          /* 0: reference rule from tree_s_opt; > 0: fixed deepest level */
     int32_t tree_s_opt;          /* elements per leaf for the reference l_max rule (10)     */
-    double  fmm_digits;          /* not used: the ML-FMM expands every box to the global order,
-                                    as the reference does                                  */
+    double  fmm_digits;          /* ML-FMM box orders: 0 = the global order n_range(2) on every
+                                    level, as the reference does; d > 0 = per level the
+                                    excess-bandwidth order kd + 1.8 d^(2/3) (kd)^(1/3) of the
+                                    box diagonal d, rounded up, never below the global order,
+                                    at most 45 (not in the reference)                      */
     int64_t device_memory_budget;/* bytes the handle may allocate; 0 = 90% of free memory  */
     int32_t pair_tables;         /* geometry-only scalar translation coefficients of every sphere
                                     pair kept in device memory for the solve: 0 = when they fit

@@ -167,6 +167,7 @@ struct foggy_handle_s {
     int64_t* d_fmm_taboff = nullptr; // per list entry, its block's offset in d_fmm_tab
     cplxf* d_fmm_tab32 = nullptr;    // the blocks in single precision (mixed-precision solves)
     bool fmm_tab_ready = false;
+    int fmm_pmax = 0;                // largest box order (the global order, or per-level orders)
     int fmm_tab_key[5] = {0, 0, 0, 0, 0};   // (convention, z_coupling, z_translation_gt_r, on, precision)
     // several right-hand sides in one block (foggy_solve_block, foggy_matvec_block): vectors of
     // nrhs slots, n_unk entries apart
@@ -695,6 +696,7 @@ void free_fmm(foggy_handle h) {
     dfree(h, h->d_fmm_taboff);
     dfree(h, h->d_fmm_tab32);
     h->fmm_tab_ready = false;
+    h->fmm_pmax = 0;
     h->fmm = FmmTree();
     h->fmm_ready = false;
 }
@@ -704,6 +706,17 @@ void free_fmm(foggy_handle h) {
 // few boxes still fill the GPU; their partial sums need fewer than 2 kFmmFill slabs of one target.
 constexpr int kFmmFill = 148 * 6;
 constexpr int kFmmChunks = 16;
+
+// Expansion order of the boxes of level l.  The reference expands every box to its global order
+// p_g (digits = 0).  With digits > 0: the excess-bandwidth order L = kd + 1.8 digits^(2/3) (kd)^(1/3)
+// of the level's box diagonal d = sqrt(3) D 2^-l (D the scaled domain's edge), rounded up, never
+// below p_g, at most kMaxDegree.
+int fmm_level_order(double k, double D, int l, double digits, int pg) {
+    if (!(digits > 0.0)) return pg;
+    const double kd = k * std::sqrt(3.0) * std::ldexp(D, -l);
+    const double L = std::ceil(std::fma(1.8 * std::pow(digits, 2.0 / 3.0), std::cbrt(kd), kd));
+    return (int)std::min<double>(kMaxDegree, std::max<double>(pg, L));
+}
 
 // Octree hierarchy and ML-FMM pass lists of the current scene and tree parameters, built on the
 // device from the sorted keys (k_tree.cu); the host keeps the level bounds only.
@@ -859,21 +872,36 @@ int ensure_fmm(foggy_handle h) {
     la.list = h->d_fmm_list;
     k_fmm_lists<<<blocks((size_t)std::max(n, nbox) + 1), 256, 0, h->stream>>>(la);
     h->launches += 4;
-    // box centres, orders and coefficient offsets; the boxes' expansions
-    const int Pg = h->pg * (h->pg + 2);
-    int rc = FOGGY_OK;
+    // box centres, orders and coefficient offsets; the boxes' expansions, level by level
+    FmmLevels lv{};
+    lv.lmin = lmin;
+    double Dm = 0.0;   // the scaled domain's edge, as k_fmm_boxes computes it
+    for (int d = 0; d < 3; ++d) Dm = std::max(Dm, (mmh[3 + d] - mmh[d]) * (1.0 + 2.220446049250313e-16));
+    int pmax = h->pg;
+    int64_t box_entries = 0;
+    for (int li = 0; li < nlev; ++li) {
+        const int L = fmm_level_order(wavenumber(h->prm), Dm, lmin + li, h->prm.fmm_digits, h->pg);
+        lv.order[li] = L;
+        lv.base[li] = lb[li];
+        lv.off[li] = box_entries;
+        box_entries += (int64_t)(lb[li + 1] - lb[li]) * 2 * L * (L + 2);
+        pmax = std::max(pmax, L);
+    }
+    h->fmm_pmax = pmax;
+    const int Pm = pmax * (pmax + 2);
+    int rc = ensure_tables(h, pmax);
     if (!rc) rc = dalloc(h, &h->d_fmm_c, 3 * (size_t)nbox);
     if (!rc) rc = dalloc(h, &h->d_fmm_p, (size_t)nbox);
     if (!rc) rc = dalloc(h, &h->d_fmm_off, (size_t)nbox);
-    if (!rc) rc = dalloc(h, &h->d_fmm_C, (size_t)nbox * 2 * Pg);
-    if (!rc) rc = dalloc(h, &h->d_fmm_D, (size_t)nbox * 2 * Pg);
+    if (!rc) rc = dalloc(h, &h->d_fmm_C, (size_t)box_entries);
+    if (!rc) rc = dalloc(h, &h->d_fmm_D, (size_t)box_entries);
     if (!rc) rc = dalloc(h, &h->d_fmm_slab, 2 * (size_t)h->n_unk);
-    if (!rc) rc = dalloc(h, &h->d_fmm_chunks, (size_t)2 * kFmmFill * 2 * Pg);
+    if (!rc) rc = dalloc(h, &h->d_fmm_chunks, (size_t)2 * kFmmFill * 2 * Pm);
     if (rc) {
         cleanup();
         return rc;
     }
-    k_fmm_boxes<<<blocks(nbox), 256, 0, h->stream>>>(nbox, box_n, box_level, mm, h->pg, h->d_fmm_c, h->d_fmm_p,
+    k_fmm_boxes<<<blocks(nbox), 256, 0, h->stream>>>(nbox, box_n, box_level, mm, lv, h->d_fmm_c, h->d_fmm_p,
                                                      h->d_fmm_off);
     h->launches += 1;
     e = cudaGetLastError();
@@ -907,7 +935,7 @@ TransArgs fmm_pass_args(foggy_handle h, const TransArgs& base, const FmmPass& q)
     const int* L = h->d_fmm_list;
     const int* lo = h->fmm_lofs;
     a.slab = h->d_fmm_chunks;
-    a.slab_ld = 2 * (int64_t)h->pg * (h->pg + 2);
+    a.slab_ld = 2 * (int64_t)h->fmm_pmax * (h->fmm_pmax + 2);
     a.tgt = q.tg;
     a.src = q.sr;
     a.x = q.in;
@@ -1053,7 +1081,7 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y, bool fp32 = false
     base.dt = dtabs(h);
     base.g = SGaunt{h->d_koffS, h->d_gs, h->gs_nm};
     base.k = sv.k;
-    base.pp = h->pg;
+    base.pp = std::max(h->pg, h->fmm_pmax);
     base.fp32 = fp32 ? 1 : 0;
     base.delta32 = h->d_delta32;
     const PointSet S{h->d_centres, h->d_p, h->d_off};
@@ -1412,7 +1440,7 @@ void foggy_default_params(foggy_params* p) {
     p->gmres_tolerance = 1e-6;
     p->tree_l_max = 0;
     p->tree_s_opt = 10;
-    p->fmm_digits = 3.0;
+    p->fmm_digits = 0.0;
     p->device_memory_budget = 0;
     p->pair_tables = 0;
     p->fmm_convention = 0;
@@ -1428,6 +1456,8 @@ static int check_params(foggy_handle h, const foggy_params* p) {
     if (p->z_coupling < 1 || p->z_coupling > 4) return fail(h, FOGGY_ERR_ARGUMENT, "z_coupling must be 1..4");
     if (p->gmres_restart < 1 || p->gmres_restart > 60) return fail(h, FOGGY_ERR_ARGUMENT, "gmres_restart must be 1..60");
     if (p->gmres_max_iterations < 1) return fail(h, FOGGY_ERR_ARGUMENT, "gmres_max_iterations must be >= 1");
+    if (!(p->fmm_digits >= 0.0) || p->fmm_digits > 16.0)
+        return fail(h, FOGGY_ERR_ARGUMENT, "fmm_digits must be in [0, 16] (0: the global order on every level)");
     if (!(p->gmres_tolerance > 0)) return fail(h, FOGGY_ERR_ARGUMENT, "gmres_tolerance must be > 0");
     if (p->matvec_mode != FOGGY_MATVEC_DIRECT && p->matvec_mode != FOGGY_MATVEC_MLFMM)
         return fail(h, FOGGY_ERR_ARGUMENT, "matvec_mode");
@@ -1514,7 +1544,8 @@ int32_t foggy_set_params(foggy_handle h, const foggy_params* params) {
         h->stab_ready = false;
         h->stab32_ready = false;
     }
-    if (params->tree_l_max != old.tree_l_max || params->tree_s_opt != old.tree_s_opt) {
+    if (params->tree_l_max != old.tree_l_max || params->tree_s_opt != old.tree_s_opt ||
+        params->fmm_digits != old.fmm_digits) {
         h->tree_ready = false;
         free_fmm(h);
     }

@@ -251,7 +251,14 @@ __global__ void k_fmm_lists(FmmListArgs a);
 __global__ void k_fmm_child_ptr(int nbox, int lb1, const int* parent, int* out);
 __global__ void k_fmm_counts(int n, int nleaf, int leaf0, const int* order, const int* couple, const int* incl_leaf,
                              const int* run_start, const int* run_end, const int* e2_cnt, int* near_cnt, int* agg_cnt);
-__global__ void k_fmm_boxes(int nbox, const long long* box_n, const int* box_level, const double* mm, int pg,
+// expansion order, coefficient offset and first box id per level (index l - lmin)
+struct FmmLevels {
+    int lmin;
+    int order[22];
+    int base[22];
+    int64_t off[22];
+};
+__global__ void k_fmm_boxes(int nbox, const long long* box_n, const int* box_level, const double* mm, FmmLevels lv,
                             double* bc, int* bp, int64_t* bo);
 
 }  // namespace foggy

@@ -310,7 +310,7 @@ __global__ void k_fmm_counts(int n, int nleaf, int leaf0, const int* order, cons
 
 // box centres in the scene's units (lib_tree_get_centre_of_box, lib_tree.f90:1292-1300, unscaled by
 // lib_tree_get_unscaled_point with D = max_d (x_max,d - x_min,d)(1 + 2^-52)), orders and offsets
-__global__ void k_fmm_boxes(int nbox, const long long* box_n, const int* box_level, const double* mm, int pg,
+__global__ void k_fmm_boxes(int nbox, const long long* box_n, const int* box_level, const double* mm, FmmLevels lv,
                             double* bc, int* bp, int64_t* bo) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nbox) return;
@@ -321,8 +321,10 @@ __global__ void k_fmm_boxes(int nbox, const long long* box_n, const int* box_lev
     deinterleave(box_n[b], l, c);
     const double h = ldexp(1.0, -l);
     for (int d = 0; d < 3; ++d) bc[3 * (size_t)b + d] = __dadd_rn(__dmul_rn(__dmul_rn(h, __dadd_rn((double)c[d], 0.5)), D), mm[d]);
-    bp[b] = pg;
-    bo[b] = (int64_t)b * 2 * pg * (pg + 2);
+    const int li = l - lv.lmin;
+    const int L = lv.order[li];
+    bp[b] = L;
+    bo[b] = lv.off[li] + (int64_t)(b - lv.base[li]) * 2 * L * (L + 2);
 }
 
 }  // namespace foggy

@@ -23,7 +23,7 @@ from . import _native as N
 
 
 def _params(scene, use_ml_fmm=False, init_with_single_sphere=False, memory_budget=0, pair_tables=0,
-            fmm_convention=0, z_translation_gt_r=3, precision=0):
+            fmm_convention=0, z_translation_gt_r=3, precision=0, fmm_digits=0.0):
     L = N.load()
     p = N.FoggyParams()
     L.foggy_default_params(C.byref(p))
@@ -44,6 +44,7 @@ def _params(scene, use_ml_fmm=False, init_with_single_sphere=False, memory_budge
     p.fmm_convention = int(fmm_convention)
     p.z_translation_gt_r = int(z_translation_gt_r)
     p.precision = int(precision)
+    p.fmm_digits = float(fmm_digits)
     return p
 
 
@@ -51,13 +52,14 @@ class MultiSphereSolver:
     """lib_mie_ms_constructor + the solver interface, on one GPU."""
 
     def __init__(self, scene, use_ml_fmm=False, init_with_single_sphere=False, device=0, memory_budget=0,
-                 pair_tables=0, fmm_convention=0, z_translation_gt_r=3, precision=0):
+                 pair_tables=0, fmm_convention=0, z_translation_gt_r=3, precision=0, fmm_digits=0.0):
         """fmm_convention 0 runs the ML-FMM as the reference writes it, 1 the consistent
-        expansion (see foggy_params.fmm_convention)."""
+        expansion (see foggy_params.fmm_convention); fmm_digits > 0 expands each level's boxes to
+        the excess-bandwidth order of that many digits instead of the global order."""
         self.L = N.load()
         self.scene = scene
         self.params = _params(scene, use_ml_fmm, init_with_single_sphere, memory_budget, pair_tables,
-                              fmm_convention, z_translation_gt_r, precision)
+                              fmm_convention, z_translation_gt_r, precision, fmm_digits)
         h = C.c_void_p()
         N.check(self.L.foggy_create(C.byref(self.params), int(device), C.byref(h)))
         self.h = h

@@ -1230,19 +1230,42 @@ Tree build(int N, const double* centres, int s, int l_max_fixed) {
     return t;
 }
 
-typedef std::vector<cd> Vec;   // reference layout, global range, [a | b]
+typedef std::vector<cd> Vec;   // reference layout from degree n1, [a | b]
+
+// Per-level expansion orders, not in the reference (which expands every box to its global order):
+// with digits > 0, the excess-bandwidth order L = kd + 1.8 digits^(2/3) (kd)^(1/3) of the level's
+// box diagonal d = sqrt(3) D 2^-l, rounded up, never below the global order p_g, at most 45;
+// digits = 0 gives p_g on every level.
+int level_order(double k, double D, int l, double digits, int pg) {
+    if (!(digits > 0.0)) return pg;
+    const double kd = k * std::sqrt(3.0) * std::ldexp(D, -l);
+    const double L = std::ceil(std::fma(1.8 * std::pow(digits, 2.0 / 3.0), std::cbrt(kd), kd));
+    return (int)std::min(45.0, std::max((double)pg, L));
+}
 
 struct Fmm {
     Problem& P;
     int conv, zgt;
     Tree t;
+    std::vector<int> Lv;   // expansion order per level (index l - lmin)
+    int Cb;                // entries per part of a box vector (degrees n1..max Lv)
     std::map<std::array<double, 8>, std::pair<std::vector<cd>, std::vector<cd>>> cache;
-    Fmm(Problem& p, int c, int z, const Tree& tr) : P(p), conv(c), zgt(z), t(tr) {}
+    Fmm(Problem& p, int c, int z, const Tree& tr, double digits = 0.0) : P(p), conv(c), zgt(z), t(tr) {
+        int lm = P.n2;
+        for (int l = t.lmin; l <= t.lmax; ++l) {
+            Lv.push_back(level_order(P.k, t.D, l, digits, P.n2));
+            lm = std::max(lm, Lv.back());
+        }
+        Cb = (lm + 1) * (lm + 1) - P.n1 * P.n1;
+    }
 
-    // out(rows r1..r2) += T(kd; z) in(cols c1..c2), both in the global layout
+    // out(rows r1..r2) += T(kd; z) in(cols c1..c2); in and out in the layout from degree n1 with
+    // Cin / Cout entries per part (-1: the spheres' global layout)
     void apply(const double kd[3], int z, int r1, int r2, int c1, int c2, const cd* in, cd* out,
-               const std::vector<cd>* scale_a = nullptr, const std::vector<cd>* scale_b = nullptr, int a0 = 0) {
-        int C = P.cnt();
+               const std::vector<cd>* scale_a = nullptr, const std::vector<cd>* scale_b = nullptr, int a0 = 0,
+               int Cin = -1, int Cout = -1) {
+        if (Cin < 0) Cin = P.cnt();
+        if (Cout < 0) Cout = P.cnt();
         double rho, th, ph;
         to_spherical(kd, &rho, &th, &ph);
         if (rho == 0.0) {   // coincident centres: the reference passes the coefficients through
@@ -1250,7 +1273,7 @@ struct Fmm {
                 for (int m = -n; m <= n; ++m) {
                     int o = blk(P.n1, n, m);
                     out[o] += in[o];
-                    out[C + o] += in[C + o];
+                    out[Cout + o] += in[Cin + o];
                 }
             return;
         }
@@ -1259,7 +1282,7 @@ struct Fmm {
         if (it == cache.end()) {
             int cr = (r2 + 1) * (r2 + 1) - r1 * r1, cc = (c2 + 1) * (c2 + 1) - c1 * c1;
             std::vector<cd> A((size_t)cr * cc), B((size_t)cr * cc);
-            wig_thread_temp_init(2 * (4 * P.n2 + 8));
+            wig_thread_temp_init(2 * (4 * std::max(std::max(r2, c2), P.n2) + 8));
             translation_xu(rho, th, ph, r1, r2, c1, c2, z, A.data(), B.data());
             it = cache.emplace(key, std::make_pair(std::move(A), std::move(B))).first;
         }
@@ -1274,8 +1297,8 @@ struct Fmm {
                     for (int mu = -nu; mu <= nu; ++mu) {
                         int col = blk(c1, nu, mu), xo = blk(P.n1, nu, mu);
                         cd a = A[(size_t)row * cc + col], b = B[(size_t)row * cc + col];
-                        s1 += a * in[xo] + b * in[C + xo];
-                        s2 += b * in[xo] + a * in[C + xo];
+                        s1 += a * in[xo] + b * in[Cin + xo];
+                        s2 += b * in[xo] + a * in[Cin + xo];
                     }
                 int o = blk(P.n1, n, m);
                 if (scale_a) {
@@ -1283,7 +1306,7 @@ struct Fmm {
                     s2 *= (*scale_b)[n - a0];
                 }
                 out[o] += s1;
-                out[C + o] += s2;
+                out[Cout + o] += s2;
             }
     }
 
@@ -1295,8 +1318,8 @@ struct Fmm {
         const int nlev = t.lmax - t.lmin + 1;
         std::vector<std::vector<Vec>> Cc(nlev), Dd(nlev);
         for (int li = 0; li < nlev; ++li) {
-            Cc[li].assign(t.boxes[li].size(), Vec(2 * (size_t)C, cd(0, 0)));
-            Dd[li].assign(t.boxes[li].size(), Vec(2 * (size_t)C, cd(0, 0)));
+            Cc[li].assign(t.boxes[li].size(), Vec(2 * (size_t)Cb, cd(0, 0)));
+            Dd[li].assign(t.boxes[li].size(), Vec(2 * (size_t)Cb, cd(0, 0)));
         }
         auto rows_of = [&](int j, int* a, int* b) {
             sphere_range(P, j, a, b);
@@ -1313,7 +1336,7 @@ struct Fmm {
                 if (!rows_of(i, &ia, &ib)) continue;
                 double kd[3];
                 for (int d = 0; d < 3; ++d) kd[d] = k * sts * (P.centres[3 * i + d] - cb[d]);
-                apply(kd, z_reg, n1, n2, ia, ib, x + (size_t)2 * C * i, Cc[L][q].data());
+                apply(kd, z_reg, n1, Lv[L], ia, ib, x + (size_t)2 * C * i, Cc[L][q].data(), nullptr, nullptr, 0, C, Cb);
             }
         }
         // upward step 2: M2M
@@ -1330,7 +1353,8 @@ struct Fmm {
                     double cc[3], kd[3];
                     t.unscaled_centre(ch, l + 1, cc);
                     for (int d = 0; d < 3; ++d) kd[d] = k * (cc[d] - cp[d]);
-                    apply(kd, z_reg, n1, n2, n1, n2, Cc[li + 1][it->second].data(), Cc[li][q].data());
+                    apply(kd, z_reg, n1, Lv[li], n1, Lv[li + 1], Cc[li + 1][it->second].data(), Cc[li][q].data(),
+                          nullptr, nullptr, 0, Cb, Cb);
                 }
             }
         }
@@ -1347,7 +1371,8 @@ struct Fmm {
                     double cs[3], kd[3];
                     t.unscaled_centre(s, l, cs);
                     for (int d = 0; d < 3; ++d) kd[d] = k * sts * (cs[d] - cb[d]);
-                    apply(kd, z_m2l, n1, n2, n1, n2, Cc[li][it->second].data(), Dd[li][q].data());
+                    apply(kd, z_m2l, n1, Lv[li], n1, Lv[li], Cc[li][it->second].data(), Dd[li][q].data(), nullptr,
+                          nullptr, 0, Cb, Cb);
                 }
             }
         }
@@ -1361,7 +1386,8 @@ struct Fmm {
                 t.unscaled_centre(nb, l, cb);
                 t.unscaled_centre(nb >> 3, l - 1, cp);
                 for (int d = 0; d < 3; ++d) kd[d] = k * (cp[d] - cb[d]);
-                apply(kd, z_reg, n1, n2, n1, n2, Dd[li - 1][pi].data(), Dd[li][q].data());
+                apply(kd, z_reg, n1, Lv[li], n1, Lv[li - 1], Dd[li - 1][pi].data(), Dd[li][q].data(), nullptr,
+                      nullptr, 0, Cb, Cb);
             }
         }
         // final summation: box-to-sphere and near field, y = x + a/b (...)
@@ -1384,9 +1410,12 @@ struct Fmm {
                 if (rows) {
                     double r = std::sqrt(kd[0] * kd[0] + kd[1] * kd[1] + kd[2] * kd[2]);
                     if (r == 0.0) {
-                        for (int i = 0; i < 2 * C; ++i) yj[i] += Dd[L][q][i];
+                        for (int i = 0; i < C; ++i) {
+                            yj[i] += Dd[L][q][i];
+                            yj[C + i] += Dd[L][q][Cb + i];
+                        }
                     } else {
-                        apply(kd, z_dor, ja, jb, n1, n2, Dd[L][q].data(), yj, &P.an[ip], &P.bn[ip], a0);
+                        apply(kd, z_dor, ja, jb, n1, Lv[L], Dd[L][q].data(), yj, &P.an[ip], &P.bn[ip], a0, Cb, C);
                     }
                 }
                 for (int l : near) {
@@ -1607,10 +1636,11 @@ int orc_cross_sections(void* p, const double* xin, double* out) {
 
 // ML-FMM operator (convention 0: the reference as written; 1: consistent expansion) with
 // l_max fixed (> 0) or from s_opt; x, y in the reference layout.
-int orc_fmm_matvec(void* p, int l_max_fixed, int s_opt, int convention, int z_gt_r, const double* x, double* y) {
+int orc_fmm_matvec(void* p, int l_max_fixed, int s_opt, int convention, int z_gt_r, double digits, const double* x,
+                   double* y) {
     Problem* P = static_cast<Problem*>(p);
     fmmo::Tree t = fmmo::build(P->N, P->centres.data(), s_opt, l_max_fixed);
-    fmmo::Fmm f(*P, convention, z_gt_r, t);
+    fmmo::Fmm f(*P, convention, z_gt_r, t, digits);
     f.run(reinterpret_cast<const cd*>(x), reinterpret_cast<cd*>(y));
     return 0;
 }

@@ -263,15 +263,17 @@ def _pairs_apply(self, x, targets, sources):
 Problem.pairs_apply = _pairs_apply
 
 
-def _fmm_matvec(self, x, l_max=0, s_opt=10, convention=0, z_gt_r=3):
+def _fmm_matvec(self, x, l_max=0, s_opt=10, convention=0, z_gt_r=3, digits=0.0):
     """The reference's ML-FMM operator y = A x (convention 0, as the Fortran does it) or the
-    consistent expansion (convention 1); l_max > 0 fixes the leaf level."""
+    consistent expansion (convention 1); l_max > 0 fixes the leaf level; digits > 0 expands each
+    level's boxes to the excess-bandwidth order of that many digits (not in the reference, which
+    uses its global order everywhere; digits = 0)."""
     L = lib()
     if not getattr(L, "_fmm_sig", False):
-        L.orc_fmm_matvec.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, dp, dp]
+        L.orc_fmm_matvec.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, dp, dp]
         L._fmm_sig = True
     y = np.zeros(2 * self.n)
-    L.orc_fmm_matvec(self.h, int(l_max), int(s_opt), int(convention), int(z_gt_r), _c(x), y)
+    L.orc_fmm_matvec(self.h, int(l_max), int(s_opt), int(convention), int(z_gt_r), float(digits), _c(x), y)
     return y.view(np.complex128)
 
 

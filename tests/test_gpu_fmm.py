@@ -165,6 +165,34 @@ def test_fmm_tables_equal_gaunt_sums(native, n, p, z, conv, rule, lmax):
     assert not np.array_equal(out[0][0], out[0][1])
 
 
+LEVEL_CASES = [
+    # n, p, convention, digits (boxes of an 8 um cube at lambda = 6 um: per-level orders 5..9)
+    (16, 3, 1, 2.0),
+    (16, 3, 0, 2.0),
+    (20, 4, 1, 1.0),
+]
+
+
+@pytest.mark.parametrize("n,p,conv,digits", LEVEL_CASES)
+def test_per_level_orders_match_oracle(native, oracle, n, p, conv, digits):
+    """Boxes expanded to per-level orders (fmm_digits > 0: the excess-bandwidth order of the level's
+    box diagonal, never below the global order): the device passes against the oracle's restatement
+    at 1e-12, with the cached translation blocks bit-identical to the per-translation sums."""
+    sc = long_wave_scene(p, n=n)
+    x = _x(sc, 6)
+    ref = oracle.Problem(sc).fmm_matvec(x, l_max=3, convention=conv, z_gt_r=3, digits=digits)
+    ys = []
+    for pt in (0, -1):
+        with solver.MultiSphereSolver(sc, use_ml_fmm=True, fmm_convention=conv, z_translation_gt_r=3,
+                                      pair_tables=pt, fmm_digits=digits) as s:
+            ys.append(s.calculate_vector_b(x))
+    assert _err(ys[0], ref, _g(sc)) < 1e-12
+    assert np.array_equal(ys[0], ys[1])
+    with solver.MultiSphereSolver(sc, use_ml_fmm=True, fmm_convention=conv, z_translation_gt_r=3) as s:
+        y_global = s.calculate_vector_b(x)
+    assert not np.array_equal(y_global, ys[0])
+
+
 def test_consistent_fmm_close_to_direct(native, oracle):
     sc = long_wave_scene(8)
     x = _x(sc, 5)
