@@ -168,6 +168,7 @@ struct foggy_handle_s {
     cplxf* d_fmm_tab32 = nullptr;    // the blocks in single precision (mixed-precision solves)
     bool fmm_tab_ready = false;
     int fmm_pmax = 0;                // largest box order (the global order, or per-level orders)
+    std::vector<int> fmm_list_host;  // the twelve pass lists, read back once (chunk counts)
     int fmm_tab_key[5] = {0, 0, 0, 0, 0};   // (convention, z_coupling, z_translation_gt_r, on, precision)
     // several right-hand sides in one block (foggy_solve_block, foggy_matvec_block): vectors of
     // nrhs slots, n_unk entries apart
@@ -697,6 +698,7 @@ void free_fmm(foggy_handle h) {
     dfree(h, h->d_fmm_tab32);
     h->fmm_tab_ready = false;
     h->fmm_pmax = 0;
+    h->fmm_list_host.clear();
     h->fmm = FmmTree();
     h->fmm_ready = false;
 }
@@ -905,6 +907,10 @@ int ensure_fmm(foggy_handle h) {
                                                      h->d_fmm_off);
     h->launches += 1;
     e = cudaGetLastError();
+    h->fmm_list_host.assign((size_t)h->fmm_ltotal + 1, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h->fmm_list_host.data(), h->d_fmm_list, ((size_t)h->fmm_ltotal + 1) * sizeof(int),
+                            cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     cleanup();
     if (e != cudaSuccess) return fail(h, FOGGY_ERR_CUDA, std::string("ML-FMM lists: ") + cudaGetErrorString(e));
@@ -1121,8 +1127,15 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y, bool fp32 = false
             a.tab32 = h->d_fmm_tab32;
             a.tab_off = h->d_fmm_taboff + h->fmm_lofs[q.li];
         }
-        // passes with few targets split each target's sources over several CTAs
-        const int chunks = q.ntgt > 0 ? std::max(1, std::min(kFmmChunks, (kFmmFill + q.ntgt - 1) / q.ntgt)) : 1;
+        // passes with few targets split each target's sources over several CTAs, no more than the
+        // longest of its source lists
+        int longest = 0;
+        if (q.ntgt > 0) {
+            const int* ptr = h->fmm_list_host.data() + h->fmm_lofs[q.lp] + (q.lp == 0 || q.lp >= 8 ? 0 : q.tbase);
+            for (int b = 0; b < q.ntgt; ++b) longest = std::max(longest, ptr[b + 1] - ptr[b]);
+        }
+        const int chunks =
+            q.ntgt > 0 ? std::max(1, std::min({kFmmChunks, (kFmmFill + q.ntgt - 1) / q.ntgt, longest})) : 1;
         launch_translate(a, q.ntgt, chunks, h->stream);
         if (q.ntgt > 0) h->launches += chunks > 1 ? 2 : 1;
     }

@@ -999,9 +999,19 @@ __global__ void k_translate_sum(TransArgs a, int chunks) {
     const int t = a.tbase + blockIdx.x;
     const int P2 = 2 * a.tgt.p[t] * (a.tgt.p[t] + 2);
     cplx* out = a.out + a.tgt.off[t];
+    const size_t cs = (size_t)gridDim.x * a.slab_ld;   // stride between a target's chunks
     for (int e = threadIdx.x; e < P2; e += blockDim.x) {
+        const cplx* q = a.slab + (size_t)blockIdx.x * a.slab_ld + e;
         cplx v = a.add ? out[e] : mk(0, 0);
-        for (int c = 0; c < chunks; ++c) v = v + a.slab[((size_t)c * gridDim.x + blockIdx.x) * a.slab_ld + e];
+        int c = 0;
+        for (; c + 4 <= chunks; c += 4) {   // four loads in flight, added in chunk order
+            const cplx q0 = q[c * cs], q1 = q[(c + 1) * cs], q2 = q[(c + 2) * cs], q3 = q[(c + 3) * cs];
+            v = v + q0;
+            v = v + q1;
+            v = v + q2;
+            v = v + q3;
+        }
+        for (; c < chunks; ++c) v = v + q[c * cs];
         out[e] = v;
     }
 }
