@@ -347,7 +347,8 @@ int32_t foggy_matvec_rhs(foggy_handle h, int32_t nrhs, const double* x, double* 
  * (lib_mie_ms_solver_run, lib_mie_ms_solver_interface.f90:143-154, around lib_solver_GMRES.f90:116-316);
  * here every operator application serves the whole block: each CTA of the operator applies the
  * translations of one target sphere to a tile of right-hand sides, whose width the library picks per
- * launch shape by timing (foggy_block_tiles).  Each right-hand side keeps its own GMRES(m) recurrence
+ * launch shape by timing (foggy_block_tiles); with matvec_mode = FOGGY_MATVEC_MLFMM the passes run
+ * vector after vector inside each block application.  Each right-hand side keeps its own GMRES(m) recurrence
  * (gmres_restart 1..63, gmres_tolerance, gmres_max_iterations apply to each) and leaves the block when
  * its true residual meets the tolerance at a restart.  With params.precision = 1 the Arnoldi steps
  * apply the operator with FP32 translation arithmetic and the restart residuals in FP64.  x (and x0, if
@@ -360,7 +361,8 @@ int32_t foggy_solve_block(foggy_handle h, int32_t nrhs, const double* x0, double
 
 /* y_v = A x_v for nrhs vectors in one block operator application (the direct operator,
  * lib_mie_ms_solver_calculate_vector_b, lib_mie_ms_solver_interface.f90:739-783, applied to several
- * vectors at once); precision 0 = FP64 translations, 1 = FP32 translations (FP64 vectors). */
+ * vectors at once; the ML-FMM passes vector after vector); precision 0 = FP64 translations, 1 = FP32
+ * translations (FP64 vectors). */
 int32_t foggy_matvec_block(foggy_handle h, int32_t nrhs, int32_t precision, const double* x, double* y, int32_t mem);
 
 /* The block operator's tile width per launch for a block of nrhs vectors, tuned on first use:

@@ -2557,8 +2557,12 @@ BlockArgs block_args(foggy_handle h, const cplx* X, cplx* Y, int nrhs, bool fp32
 
 // Y_r = A X_r for r < nrhs (device layout, n_unk apart), FP64 or FP32 translation arithmetic
 int apply_operator_block(foggy_handle h, const cplx* X, cplx* Y, int nrhs, bool fp32) {
-    if (h->prm.matvec_mode != FOGGY_MATVEC_DIRECT)
-        return fail(h, FOGGY_ERR_UNSUPPORTED, "several right-hand sides in one block: direct operator only");
+    if (h->prm.matvec_mode == FOGGY_MATVEC_MLFMM) {
+        // the ML-FMM passes one vector after another (their translations are per box, not per pair)
+        for (int r = 0; r < nrhs; ++r)
+            TRY(apply_operator_fmm(h, X + (size_t)r * h->n_unk, Y + (size_t)r * h->n_unk, fp32));
+        return FOGGY_OK;
+    }
     TRY(ensure_pair_tables(h));
     const BlockArgs ba = block_args(h, X, Y, nrhs, fp32);
     const bool tabs = fp32 ? ba.d.pt.stab32 != nullptr : ba.d.pt.stab != nullptr;
@@ -2843,8 +2847,6 @@ int32_t foggy_solve_block(foggy_handle h, int32_t nrhs, const double* x0, double
     if (nrhs < 1 || nrhs != (int)h->waves.size())
         return fail(h, FOGGY_ERR_ARGUMENT, "nrhs must equal the number of plane waves set (one right-hand side each)");
     if (!h->beams.empty()) return fail(h, FOGGY_ERR_ARGUMENT, "one right-hand side per plane wave excludes Gaussian beams");
-    if (h->prm.matvec_mode != FOGGY_MATVEC_DIRECT)
-        return fail(h, FOGGY_ERR_UNSUPPORTED, "several right-hand sides in one block: direct operator only");
     if (h->prm.gmres_restart < 1 || h->prm.gmres_restart > 63)
         return fail(h, FOGGY_ERR_ARGUMENT, "gmres_restart must be 1..63 for the block solve");
     Trace tr("foggy_solve_block");

@@ -156,9 +156,31 @@ def test_block_solve_with_initial_guess_and_limits(native):
         assert st["status"] == -5 and np.all(its <= 2) and np.all(be > 1e-11)
 
 
+def test_block_solve_through_the_mlfmm(native):
+    """A block over the ML-FMM operator (consistent passes, boxes small against the wavelength; its
+    passes run vector after vector inside each block application): each right-hand side within 1e-10
+    of its own ML-FMM solve, FP64 and mixed precision (1e-6)."""
+    rng = np.random.default_rng(7)
+    sc = S.make_scene(rng.uniform(0.1, 0.3, 30), 9.0, 5, lambda_0=6.0, n_max=6, z_coupling=3,
+                      reference_row_rule=False, tree_l_max=3, waves=fibonacci_waves(3), gmres_tolerance=1e-12)
+    g = _g_layout(sc)
+    with solver.MultiSphereSolver(sc, use_ml_fmm=True, fmm_convention=1) as s:
+        xs, _, _ = s.solve_rhs()
+        x, cs, its, be, st = s.solve_block()
+        assert st["status"] == 0 and np.all(be <= 1e-12)
+        for r in range(sc.n_waves):
+            assert _err(x[r], xs[r], g) < 1e-10, "right-hand side %d" % r
+    sc2 = dataclasses.replace(sc, gmres_tolerance=1e-8)
+    with solver.MultiSphereSolver(sc2, use_ml_fmm=True, fmm_convention=1, precision=1) as s:
+        x32, _, _, be32, st32 = s.solve_block()
+    assert st32["status"] == 0 and np.all(be32 <= 1e-8)
+    for r in range(sc.n_waves):
+        assert np.linalg.norm((x32[r] - xs[r]) / g) <= 1e-6 * np.linalg.norm(xs[r] / g)
+
+
 def test_block_argument_errors(native):
-    """Refusals of the block entries: right-hand-side count other than the plane waves set, the ML-FMM
-    operator, an unknown precision."""
+    """Refusals of the block entries: right-hand-side count other than the plane waves set, an
+    unknown precision."""
     import ctypes as C
     from itofoggysim_b200 import _native as N
     sc = S.random_cluster(4, seed=34, p=3)
@@ -170,9 +192,5 @@ def test_block_argument_errors(native):
         assert s.L.foggy_solve_block(s.h, 3, None, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), None, None,
                                      None) == N.FOGGY_ERR_ARGUMENT
         assert s.L.foggy_matvec_block(s.h, 2, 2, x.ctypes.data, x.ctypes.data, N.FOGGY_MEM_HOST) == N.FOGGY_ERR_ARGUMENT
-        s.use_ml_fmm(True)
-        assert s.L.foggy_solve_block(s.h, 4, None, x.ctypes.data, N.FOGGY_MEM_HOST, C.byref(st), None, None,
-                                     None) == N.FOGGY_ERR_UNSUPPORTED
-        s.use_ml_fmm(False)
         xs, cs, its, be, st2 = s.solve_block()
         assert st2["status"] == 0 and xs.shape == (4, n)
