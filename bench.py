@@ -606,6 +606,50 @@ def run_operator(args):
                       "tflops": flops / (float(np.mean(out)) * 1e-3) / 1e12}), flush=True)
 
 
+def long_wave_scene(n):
+    """n water spheres of radius 0.1-0.3 um at lambda = 6 um, 0.04 spheres per um^3 (boxes a fraction
+    of a wavelength to a few wavelengths), global order 8: the regime where the reference's ML-FMM
+    expansion is accurate."""
+    from itofoggysim_b200 import scene as S
+    rng = np.random.default_rng(7)
+    box = (n / 0.04) ** (1.0 / 3.0)
+    return S.make_scene(rng.uniform(0.1, 0.3, n), box, 5, lambda_0=6.0, n_max=8, z_coupling=3,
+                        reference_row_rule=False, name="long_wave_%d" % n)
+
+
+def run_fmm_scale(args):
+    """The direct operator against the ML-FMM (consistent convention, --fmm-digits per-level orders or
+    the global order) on long_wave_scene(--spheres): device time per application (median of
+    --applications after one untimed one) and the relative difference of the two results."""
+    import torch
+    from itofoggysim_b200 import solver
+    dev = torch.device("cuda", 0)
+    sc = long_wave_scene(args.spheres)
+    out = {"workload": "fmm_scale", "spheres": args.spheres, "fmm_digits": args.fmm_digits}
+    ys = {}
+    for name, kw in (("direct", {}), ("mlfmm", dict(use_ml_fmm=True, fmm_convention=1, fmm_digits=args.fmm_digits))):
+        with solver.MultiSphereSolver(sc, **kw) as s:
+            b = s.get_vector_b()
+            xd = torch.from_numpy(b.view(np.float64).copy()).to(dev)
+            yd = torch.empty_like(xd)
+            s.matvec_device(xd.data_ptr(), yd.data_ptr())
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(max(1, args.applications)):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                s.matvec_device(xd.data_ptr(), yd.data_ptr())
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            ys[name] = yd.cpu().numpy().view(np.complex128)
+            out[name + "_ms"] = float(np.median(ts))
+    out["speedup"] = out["direct_ms"] / out["mlfmm_ms"]
+    out["rel_diff"] = float(np.linalg.norm(ys["mlfmm"] - ys["direct"]) / np.linalg.norm(ys["direct"]))
+    print(json.dumps(out), flush=True)
+
+
 def g_layout(sc):
     g = np.array([math.sqrt(math.factorial(n + m) / math.factorial(n - m))
                   for n in range(1, sc.n_range[1] + 1) for m in range(-n, n + 1)])
@@ -704,7 +748,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="medium", choices=["medium", "small", "serving", "multi_rhs", "block",
-                                                             "operator"],
+                                                             "operator", "fmm_scale"],
                     help="serving: a request stream through the solve server; block: 128 right-hand sides of "
                          "one lognormal scene as one mixed-precision block (their own JSON lines)")
     ap.add_argument("--spheres", type=int, default=500, help="spheres of the block and operator workloads' scenes")
@@ -715,6 +759,8 @@ def main():
     ap.add_argument("--operator", default="direct", choices=["direct", "mlfmm"],
                     help="mlfmm: the ML-FMM passes (fmm_convention below) instead of all pairs")
     ap.add_argument("--fmm-convention", type=int, default=0, choices=[0, 1])
+    ap.add_argument("--fmm-digits", type=float, default=0.0,
+                    help="fmm_scale workload: per-level ML-FMM orders for this many digits (0: the global order)")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU sampling")
     ap.add_argument("--matvecs-per-solve", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -746,6 +792,14 @@ def main():
                   flush=True)
         elif rank == 0:
             run_multi_rhs(args)
+        return
+
+    if args.workload == "fmm_scale":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "operator comparison mode of the GPU arm"}),
+                  flush=True)
+        elif rank == 0:
+            run_fmm_scale(args)
         return
 
     if args.workload == "operator":

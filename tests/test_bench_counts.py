@@ -104,3 +104,14 @@ def test_cached_operator_size_and_scale():
     assert abs(bench.cached_scale(a, b) - pairs(b) / pairs(a)) < 1e-12
     # the 64-sphere cluster's cache: 4032 pairs x 2 x 255^2 x 16 bytes
     assert bench.cached_bytes(S.small_cluster()) == 4032 * 2 * 255 ** 2 * 16
+
+
+def test_long_wave_scene():
+    """The ML-FMM comparison scene: spheres of radius 0.1-0.3 um at lambda = 6 um, 0.04 per um^3,
+    global order 8."""
+    sc = bench.long_wave_scene(500)
+    assert sc.n_spheres == 500 and sc.lambda_0 == 6.0
+    assert np.all(sc.p_of_sphere() == 8)
+    edge = (500 / 0.04) ** (1.0 / 3.0)
+    assert np.all(sc.centres >= 0.0) and np.all(sc.centres < edge)
+    assert np.all((sc.radius >= 0.1) & (sc.radius <= 0.3))
