@@ -1107,9 +1107,9 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y, bool fp32 = false
     for (int li = nlev - 2; li >= 0; --li)
         add(1, B, B, h->d_fmm_C, h->d_fmm_C, 2, 3, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
             z_reg, 0, false);
-    for (int li = 0; li < nlev; ++li)
-        add(2, B, B, h->d_fmm_C, h->d_fmm_D, 4, 5, t.level_base[li], t.level_base[li + 1] - t.level_base[li], sts, zi,
-            0, false);
+    // M2L of every level in one launch: each box's incoming sum depends only on the outgoing
+    // expansions of its own level
+    add(2, B, B, h->d_fmm_C, h->d_fmm_D, 4, 5, 0, nbox, sts, zi, 0, false);
     for (int li = 1; li < nlev; ++li)
         add(3, B, B, h->d_fmm_D, h->d_fmm_D, 6, 7, t.level_base[li], t.level_base[li + 1] - t.level_base[li], 1.0,
             z_reg, 1, false);
