@@ -163,6 +163,9 @@ struct foggy_handle_s {
     int fmm_ltotal = 0;              // entries of the twelve lists
     cplx* d_fmm_slab = nullptr;      // box-to-sphere and near-field sums, 2 x n_unk
     cplx* d_fmm_chunks = nullptr;    // partial sums of passes split into source chunks
+    cplx* d_fmm_chunks2 = nullptr;   // the same for the near-field pass, which runs beside the others
+    cudaStream_t side = nullptr;     // the near-field pass's stream, joined before the sum
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cplx* d_fmm_tab = nullptr;       // coaxial blocks of the passes' distinct translations
     int64_t* d_fmm_taboff = nullptr; // per list entry, its block's offset in d_fmm_tab
     cplxf* d_fmm_tab32 = nullptr;    // the blocks in single precision (mixed-precision solves)
@@ -693,6 +696,7 @@ void free_fmm(foggy_handle h) {
     dfree(h, h->d_fmm_list);
     dfree(h, h->d_fmm_slab);
     dfree(h, h->d_fmm_chunks);
+    dfree(h, h->d_fmm_chunks2);
     dfree(h, h->d_fmm_tab);
     dfree(h, h->d_fmm_taboff);
     dfree(h, h->d_fmm_tab32);
@@ -899,6 +903,7 @@ int ensure_fmm(foggy_handle h) {
     if (!rc) rc = dalloc(h, &h->d_fmm_D, (size_t)box_entries);
     if (!rc) rc = dalloc(h, &h->d_fmm_slab, 2 * (size_t)h->n_unk);
     if (!rc) rc = dalloc(h, &h->d_fmm_chunks, (size_t)2 * kFmmFill * 2 * Pm);
+    if (!rc) rc = dalloc(h, &h->d_fmm_chunks2, (size_t)2 * kFmmFill * 2 * Pm);
     if (rc) {
         cleanup();
         return rc;
@@ -1117,11 +1122,22 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y, bool fp32 = false
     add(5, S, S, x, h->d_fmm_slab + h->n_unk, 10, 11, 0, h->N, 1.0, zi, 0, false);
     TRY(ensure_fmm_tables(h, base, passes));
     const bool tabs = h->d_fmm_taboff != nullptr && (!fp32 || h->d_fmm_tab32 != nullptr);
+    // the near field needs only x: it runs on a second stream beside the box passes
+    if (!h->side) {
+        if (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess)
+            return fail(h, FOGGY_ERR_CUDA, "ML-FMM side stream");
+    }
+    CK(h, cudaEventRecord(h->ev_fork, h->stream));
+    CK(h, cudaStreamWaitEvent(h->side, h->ev_fork, 0));
     Trace tr(fp32 ? "ML-FMM operator (FP32)" : "ML-FMM operator");
     for (size_t i = 0; i < passes.size(); ++i) {
         const FmmPass& q = passes[i];
+        const bool near = stage[i] == 5;
         Trace tp(names[stage[i]]);
         TransArgs a = fmm_pass_args(h, base, q);
+        if (near) a.slab = h->d_fmm_chunks2;
         if (tabs) {
             a.tab = h->d_fmm_tab;
             a.tab32 = h->d_fmm_tab32;
@@ -1136,9 +1152,12 @@ int apply_operator_fmm(foggy_handle h, const cplx* x, cplx* y, bool fp32 = false
         }
         const int chunks =
             q.ntgt > 0 ? std::max(1, std::min({kFmmChunks, (kFmmFill + q.ntgt - 1) / q.ntgt, longest})) : 1;
-        launch_translate(a, q.ntgt, chunks, h->stream);
+        launch_translate(a, q.ntgt, chunks, near ? h->side : h->stream);
         if (q.ntgt > 0) h->launches += chunks > 1 ? 2 : 1;
     }
+    // join first, so that whatever follows on the handle's stream (frees included) comes after the side
+    cudaEventRecord(h->ev_join, h->side);
+    cudaStreamWaitEvent(h->stream, h->ev_join, 0);
     CKL(h);
     k_direct_finish<<<h->N, 256, 0, h->stream>>>(sv, x, h->d_fmm_slab, 2, h->n_unk, y);
     h->launches += 1;
@@ -1532,8 +1551,10 @@ int32_t foggy_destroy(foggy_handle h) {
     h->allocs.clear();
     pinned_release(reinterpret_cast<char*>(h->h_pin));
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
-    for (cudaEvent_t e : {h->ev0, h->ev1, h->evm0, h->evm1, h->ev_step[0], h->ev_step[1]})
+    if (h->side) cudaStreamSynchronize(h->side);
+    for (cudaEvent_t e : {h->ev0, h->ev1, h->evm0, h->evm1, h->ev_step[0], h->ev_step[1], h->ev_fork, h->ev_join})
         if (e) cudaEventDestroy(e);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return FOGGY_OK;
