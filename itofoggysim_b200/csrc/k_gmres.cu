@@ -10,33 +10,34 @@ constexpr int kT = 256;
 constexpr int kMaxDots = 64;   // Krylov vectors handled per dots launch
 }
 
-// part[i * kRedBlocks + block] = partial sum of conj(V_i) . w over the block's slice
+// conj(v) . w over [lo, hi) by one warp: lanes stride the slice, then a fixed butterfly of shuffles
+__device__ __forceinline__ cplx warp_dot(const cplx* __restrict__ v, const cplx* __restrict__ w, int64_t lo, int64_t hi,
+                                         int lane) {
+    double sx = 0.0, sy = 0.0;
+    for (int64_t t = lo + lane; t < hi; t += 32) {
+        const cplx a = v[t], b = w[t];
+        sx += a.x * b.x + a.y * b.y;
+        sy += a.x * b.y - a.y * b.x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    return mk(sx, sy);
+}
+
+// part[i * kRedBlocks + block] = partial sum of conj(V_i) . w over the block's slice; warp q of the
+// block takes the vectors i = q, q + 8, ... (no block-wide barrier per vector)
 __global__ void __launch_bounds__(kT) k_dots_partial(const cplx* V, int64_t ld, int nv, const cplx* w, int64_t n,
                                                      cplx* part) {
-    __shared__ double red_x[kT], red_y[kT];
-    int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-    int64_t lo = (int64_t)blockIdx.x * chunk;
-    int64_t hi = min(n, lo + chunk);
-    for (int i = 0; i < nv; ++i) {
-        const cplx* v = V + (size_t)i * ld;
-        double sx = 0.0, sy = 0.0;
-        for (int64_t t = lo + threadIdx.x; t < hi; t += blockDim.x) {
-            cplx a = v[t], b = w[t];
-            sx += a.x * b.x + a.y * b.y;
-            sy += a.x * b.y - a.y * b.x;
-        }
-        red_x[threadIdx.x] = sx;
-        red_y[threadIdx.x] = sy;
-        __syncthreads();
-        for (int s = kT / 2; s > 0; s >>= 1) {
-            if (threadIdx.x < s) {
-                red_x[threadIdx.x] += red_x[threadIdx.x + s];
-                red_y[threadIdx.x] += red_y[threadIdx.x + s];
-            }
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) part[(size_t)i * gridDim.x + blockIdx.x] = mk(red_x[0], red_y[0]);
-        __syncthreads();
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = (int64_t)blockIdx.x * chunk;
+    const int64_t hi = min(n, lo + chunk);
+    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    for (int i = q; i < nv; i += kT / 32) {
+        const cplx d = warp_dot(V + (size_t)i * ld, w, lo, hi, lane);
+        if (lane == 0) part[(size_t)i * gridDim.x + blockIdx.x] = d;
     }
 }
 
@@ -191,33 +192,16 @@ __global__ void k_update_x(cplx* x, const cplx* V, int64_t ld, const cplx* y, in
 // part[(b nv + i) kRedBlocks + block] = partial sum of conj(V_i) . w_b
 __global__ void __launch_bounds__(kT) k_dots_partial_b(const cplx* V, int64_t ldi, int64_t ld, int nv,
                                                        const cplx* W, int64_t n, const int* live, cplx* part) {
-    __shared__ double red_x[kT], red_y[kT];
     const int b = blockIdx.y;
     if (!live[b]) return;
     const cplx* w = W + (size_t)b * ld;
-    int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-    int64_t lo = (int64_t)blockIdx.x * chunk;
-    int64_t hi = min(n, lo + chunk);
-    for (int i = 0; i < nv; ++i) {
-        const cplx* v = V + (size_t)i * ldi + (size_t)b * ld;
-        double sx = 0.0, sy = 0.0;
-        for (int64_t t = lo + threadIdx.x; t < hi; t += blockDim.x) {
-            cplx a = v[t], c = w[t];
-            sx += a.x * c.x + a.y * c.y;
-            sy += a.x * c.y - a.y * c.x;
-        }
-        red_x[threadIdx.x] = sx;
-        red_y[threadIdx.x] = sy;
-        __syncthreads();
-        for (int s = kT / 2; s > 0; s >>= 1) {
-            if (threadIdx.x < s) {
-                red_x[threadIdx.x] += red_x[threadIdx.x + s];
-                red_y[threadIdx.x] += red_y[threadIdx.x + s];
-            }
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) part[((size_t)b * nv + i) * gridDim.x + blockIdx.x] = mk(red_x[0], red_y[0]);
-        __syncthreads();
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = (int64_t)blockIdx.x * chunk;
+    const int64_t hi = min(n, lo + chunk);
+    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    for (int i = q; i < nv; i += kT / 32) {
+        const cplx d = warp_dot(V + (size_t)i * ldi + (size_t)b * ld, w, lo, hi, lane);
+        if (lane == 0) part[((size_t)b * nv + i) * gridDim.x + blockIdx.x] = d;
     }
 }
 
