@@ -2072,6 +2072,17 @@ int64_t estimate_solve_bytes(const foggy_params& prm, int N, const int* param_in
     bytes += 2 * len * v;                                                                 // host staging
     const int64_t q = 2 * pmax + 2;
     bytes += 256 * q * q * q + ((int64_t)64 << 20);                                      // order tables
+    if (prm.matvec_mode == FOGGY_MATVEC_MLFMM) {
+        // the ML-FMM's box expansions (every sphere's box on every level, at most), the partial sums of
+        // its chunked passes on both streams, and its lists; its cached translation blocks are kept only
+        // when they fit beside all this
+        const int depth = prm.tree_l_max > 0 ? prm.tree_l_max
+                                             : std::min(21, 3 + (int)std::ceil(std::log((double)std::max(N, 2)) /
+                                                                                std::log(8.0)));
+        const int Lb = prm.fmm_digits > 0.0 ? kMaxDegree : pg;
+        const int64_t Pb = (int64_t)Lb * (Lb + 2), nbox = (int64_t)N * depth;
+        bytes += 2 * nbox * 2 * Pb * v + 2 * (int64_t)2 * kFmmFill * 2 * Pb * v + nbox * 220 * 4 + (int64_t)N * 256;
+    }
     int64_t tb = 0;
     if (pair_tables >= 0 && N > 1) {
         for (int a = 1; a <= kMaxDegree; ++a)

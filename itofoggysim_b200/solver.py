@@ -395,10 +395,10 @@ def universal_index(points, level):
     return out
 
 
-def estimate_solve_bytes(scene, precision=0):
-    """(solve bytes, pair-table bytes) a direct-operator solve of scene holds on the device at its
-    peak (foggy_estimate_solve_bytes; host only, no GPU)."""
-    p = _params(scene, precision=precision)
+def estimate_solve_bytes(scene, precision=0, use_ml_fmm=False, fmm_digits=0.0):
+    """(solve bytes, pair-table bytes) a solve of scene holds on the device at its peak
+    (foggy_estimate_solve_bytes; host only, no GPU); use_ml_fmm adds the ML-FMM's buffers."""
+    p = _params(scene, use_ml_fmm=use_ml_fmm, precision=precision, fmm_digits=fmm_digits)
     sb, tb = C.c_int64(), C.c_int64()
     N.check(N.load().foggy_estimate_solve_bytes(C.byref(p), scene.n_spheres, N.ptr(N.as_i32(scene.param_index), C.c_int32),
                                                scene.n_param, N.ptr(N.as_i32(scene.n_range_param).reshape(-1), C.c_int32),

@@ -48,3 +48,13 @@ def test_argument_errors(native):
     sc.n_range = (1, 40)
     sb, tb = solver.estimate_solve_bytes(sc)
     assert tb > 0 and sb > 0
+
+
+def test_mlfmm_adds_its_box_expansions(native):
+    """An ML-FMM solve also holds its box expansions and chunk partial sums: more bytes than the
+    direct solve, and more again with per-level orders (bounded by the largest order)."""
+    sc = S.small_cluster()
+    d, _ = solver.estimate_solve_bytes(sc)
+    f, _ = solver.estimate_solve_bytes(sc, use_ml_fmm=True)
+    f3, _ = solver.estimate_solve_bytes(sc, use_ml_fmm=True, fmm_digits=3.0)
+    assert d < f < f3
