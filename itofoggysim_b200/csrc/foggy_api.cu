@@ -562,9 +562,90 @@ int plan_direct(foggy_handle h) {
     return FOGGY_OK;
 }
 
+// The single-precision pair tables as tensor-core products (k_pair_tc.cu).  The pairs are grouped
+// by M2 = max(p_s, p_t) + 2 (the groups share the Gaunt operand) and, within a group, ordered by
+// min(p_s, p_t) from the largest down, so that the np pairs of a tile have blocks of similar size;
+// a tile computes the 128-row tiles of its largest block.
+int build_pair_tables_tc(foggy_handle h, const SGaunt& g) {
+    const int n = h->N;
+    const int nm = h->pmax + 3;   // M2 = 3..pmax + 2, min order 1..pmax
+    std::vector<int64_t> start((size_t)nm * nm + 1, 0);
+    auto bucket = [&](int ps, int pt) { return (size_t)(std::max(ps, pt) + 2) * nm + (nm - 1 - std::min(ps, pt)); };
+    for (int s = 0; s < n; ++s)
+        for (int t = s + 1; t < n; ++t) start[bucket(h->p_s[s], h->p_s[t]) + 1]++;
+    for (size_t b = 0; b < (size_t)nm * nm; ++b) start[b + 1] += start[b];
+    const int64_t npairs = start[(size_t)nm * nm];
+    std::vector<int2> pairs((size_t)npairs);
+    {
+        std::vector<int64_t> fill(start.begin(), start.end() - 1);
+        for (int s = 0; s < n; ++s)
+            for (int t = s + 1; t < n; ++t) pairs[(size_t)fill[bucket(h->p_s[s], h->p_s[t])]++] = make_int2(s, t);
+    }
+    std::vector<TcGroup> groups;
+    std::vector<TcTile> tiles;
+    std::vector<int> group_tile0;
+    int64_t a_floats = 0;
+    for (int M2 = 3; M2 < nm; ++M2) {
+        const int64_t g0 = start[(size_t)M2 * nm], g1 = start[(size_t)(M2 + 1) * nm];
+        if (g0 == g1) continue;
+        TcGroup gr;
+        gr.M2 = M2;
+        gr.K = tc_group_k(M2);
+        gr.np = tc_group_pairs(gr.K);
+        auto tiles_of = [&](int64_t first) {
+            const int2 st = pairs[(size_t)first];
+            return (int)((pair_block_size(h->p_s[st.x], h->p_s[st.y]) + 127) / 128);
+        };
+        gr.mtiles = tiles_of(g0);
+        gr.a_off = a_floats;
+        a_floats += (int64_t)gr.mtiles * 2 * 128 * gr.K;
+        group_tile0.push_back((int)tiles.size());
+        for (int64_t f = g0; f < g1; f += gr.np)
+            tiles.push_back(TcTile{(int)groups.size(), (int)f, (int)std::min<int64_t>(gr.np, g1 - f), tiles_of(f)});
+        groups.push_back(gr);
+    }
+    group_tile0.push_back((int)tiles.size());
+    int2* d_pairs = nullptr;
+    TcTile* d_tiles = nullptr;
+    TcGroup* d_groups = nullptr;
+    float* d_a = nullptr;
+    int* d_err = nullptr;
+    auto fin = [&](int rc) {
+        tfree(h, d_pairs);
+        tfree(h, d_tiles);
+        tfree(h, d_groups);
+        tfree(h, d_a);
+        tfree(h, d_err);
+        return rc;
+    };
+    if (talloc(h, &d_pairs, pairs.size() * sizeof(int2)) != cudaSuccess ||
+        talloc(h, &d_tiles, tiles.size() * sizeof(TcTile)) != cudaSuccess ||
+        talloc(h, &d_groups, groups.size() * sizeof(TcGroup)) != cudaSuccess ||
+        talloc(h, &d_a, (size_t)a_floats * sizeof(float)) != cudaSuccess || talloc(h, &d_err, sizeof(int)) != cudaSuccess)
+        return fin(fail(h, FOGGY_ERR_NOMEM, "tensor-core pair tables: device scratch"));
+    cudaError_t e = h2d(h, d_pairs, pairs.data(), pairs.size() * sizeof(int2));
+    if (e == cudaSuccess) e = h2d(h, d_tiles, tiles.data(), tiles.size() * sizeof(TcTile));
+    if (e == cudaSuccess) e = h2d(h, d_groups, groups.data(), groups.size() * sizeof(TcGroup));
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, sizeof(int), h->stream);
+    if (e != cudaSuccess) return fin(fail(h, FOGGY_ERR_CUDA, std::string("tensor-core pair tables: ") + cudaGetErrorString(e)));
+    TcArgs ta{scene_view(h), h->prm.z_coupling, d_pairs, d_tiles, d_groups, d_a, h->d_pair_off, h->d_stab32, d_err};
+    for (size_t i = 0; i < groups.size(); ++i) {
+        launch_tc_pack_a(g, groups[i], d_a, h->stream);
+        launch_pair_tc(ta, group_tile0[i], group_tile0[i + 1] - group_tile0[i], groups[i].K, groups[i].np, h->stream);
+        h->launches += 2;
+    }
+    e = cudaGetLastError();
+    int err = 0;
+    if (e == cudaSuccess) e = d2h(h, &err, d_err, sizeof(int));
+    if (e != cudaSuccess) return fin(fail(h, FOGGY_ERR_CUDA, std::string("tensor-core pair tables: ") + cudaGetErrorString(e)));
+    if (err) return fin(fail(h, FOGGY_ERR_CUDA, "tensor-core pair tables: a wait for a copy or the tensor core timed out"));
+    return fin(FOGGY_OK);
+}
+
 // Scalar coaxial coefficients of all unordered sphere pairs (geometry and z only), built once
 // and read by every operator application.  Skipped when they do not fit (pair_tables = 0) or
-// when switched off (pair_tables = -1).
+// when switched off (pair_tables = -1).  The double-precision tables are FP64 sums (k_pair_s); the
+// single-precision ones are tensor-core products in 3xTF32 (build_pair_tables_tc).
 int ensure_pair_tables(foggy_handle h) {
     const bool mixed = h->prm.precision == 1;
     if (h->prm.pair_tables < 0 || h->N < 2) {
@@ -635,8 +716,7 @@ int ensure_pair_tables(foggy_handle h) {
     }
     if (want32) {
         if (!h->d_stab32) TRY(dalloc(h, &h->d_stab32, (size_t)tot));
-        launch_pair_s(scene_view(h), g, h->prm.z_coupling, h->d_pair_off, h->d_stab32, true, grid, chunks, h->stream);
-        h->launches += 1;
+        TRY(build_pair_tables_tc(h, g));
         h->stab32_ready = true;
     }
     CKL(h);

@@ -133,6 +133,35 @@ void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s);
 // scalar coaxial tables of every pair, in FP64 (stab: cplx*) or FP32 (cplxf*)
 void launch_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, void* stab, bool fp32, dim3 grid,
                    int chunks, cudaStream_t s);
+
+// k_pair_tc.cu -- the FP32 tables as tensor-core products (tcgen05 kind::tf32, 3xTF32).  The pairs
+// of one M2 = max order + 2 share the Gaunt operand; a tile is up to np pairs of one group.
+struct TcGroup {
+    int M2, K, np;        // K: degrees p = 0..2 M2 - 2 padded to 8; np: pairs per tile (64, or 16 for K > 72)
+    int mtiles;           // 128-row tiles of the packed Gaunt operand (the group's largest block)
+    int64_t a_off;        // float offset of the group's packed operand
+};
+struct TcTile {
+    int group, first, count;   // pairs first..first + count - 1 of the sorted pair list
+    int mtiles;                // 128-row tiles of the tile's largest block
+};
+struct TcArgs {
+    SceneView sc;
+    int z;
+    const int2* pairs;         // (s, t), s < t, by group, largest block first within a group
+    const TcTile* tiles;
+    const TcGroup* groups;
+    const float* a;            // packed Gaunt operands
+    const int64_t* pair_off;
+    cplxf* stab;
+    int* err;                  // set when a wait for a copy or the tensor core timed out
+};
+int64_t tc_group_rows(int M2);
+int tc_group_k(int M2);
+int tc_group_pairs(int K);
+size_t tc_smem_bytes(int K, int np);
+void launch_tc_pack_a(SGaunt g, const TcGroup& gr, float* out, cudaStream_t s);
+void launch_pair_tc(const TcArgs& a, int tile0, int ntiles, int K, int np, cudaStream_t s);
 // y = x + T (sum of the slab partials) for coupled spheres, y = x otherwise
 __global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial, int slabs, int64_t n_unk,
                                 cplx* y);
