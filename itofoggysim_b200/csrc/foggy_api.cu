@@ -565,7 +565,7 @@ int plan_direct(foggy_handle h) {
 // The single-precision pair tables as tensor-core products (k_pair_tc.cu).  The pairs are grouped
 // by M2 = max(p_s, p_t) + 2 (the groups share the Gaunt operand) and, within a group, ordered by
 // min(p_s, p_t) from the largest down, so that the np pairs of a tile have blocks of similar size;
-// a tile computes the 128-row tiles of its largest block.
+// the 128-row tiles of a tile's largest block are split into runs of 8, one CTA each.
 int build_pair_tables_tc(foggy_handle h, const SGaunt& g) {
     const int n = h->N;
     const int nm = h->pmax + 3;   // M2 = 3..pmax + 2, min order 1..pmax
@@ -600,8 +600,12 @@ int build_pair_tables_tc(foggy_handle h, const SGaunt& g) {
         gr.a_off = a_floats;
         a_floats += (int64_t)gr.mtiles * 2 * 128 * gr.K;
         group_tile0.push_back((int)tiles.size());
-        for (int64_t f = g0; f < g1; f += gr.np)
-            tiles.push_back(TcTile{(int)groups.size(), (int)f, (int)std::min<int64_t>(gr.np, g1 - f), tiles_of(f)});
+        // runs of at most 8 row tiles per CTA, so that groups of few pairs still fill the GPU
+        for (int64_t f = g0; f < g1; f += gr.np) {
+            const int mt = tiles_of(f), cnt = (int)std::min<int64_t>(gr.np, g1 - f);
+            for (int m = 0; m < mt; m += 8)
+                tiles.push_back(TcTile{(int)groups.size(), (int)f, cnt, m, std::min(mt, m + 8)});
+        }
         groups.push_back(gr);
     }
     group_tile0.push_back((int)tiles.size());

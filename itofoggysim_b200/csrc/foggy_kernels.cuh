@@ -143,7 +143,7 @@ struct TcGroup {
 };
 struct TcTile {
     int group, first, count;   // pairs first..first + count - 1 of the sorted pair list
-    int mtiles;                // 128-row tiles of the tile's largest block
+    int m0, m1;                // the 128-row tiles m0..m1 - 1 of their blocks (at most 8)
 };
 struct TcArgs {
     SceneView sc;

@@ -11,9 +11,10 @@
 //     T[e][n] = sum_p G[e][p] Z[n][p],   column n = (pair, re | im),
 // M = 128 rows e per MMA, N = 2 x the pairs of a CTA, K = the degrees p = 0..2 M2 - 2 padded to 8.
 // G is packed once per handle in the operand layout of the MMA (k_tc_pack_a, split in FP64); each
-// CTA computes the Bessel functions of its pairs, splits their zeta into the B operand, and walks
-// the 128-row tiles of its group: a bulk copy brings tile m + 2 while the MMAs of tile m + 1 run and
-// the epilogue warps read tile m out of tensor memory (two accumulators) into the tables.
+// CTA computes the Bessel functions of its pairs, splits their zeta into the B operand, and walks a
+// run of up to 8 of the 128-row tiles of its group: a bulk copy brings tile m + 2 while the MMAs of
+// tile m + 1 run and eight epilogue warps (two per TMEM lane quarter, one per half of the columns)
+// read tile m out of tensor memory (two accumulators) into the tables.
 #include <algorithm>
 #include <cstdint>
 
@@ -26,7 +27,8 @@ namespace foggy {
 namespace {
 
 constexpr int kTcRows = 128;            // rows e per tile (M of one MMA)
-constexpr int kTcThreads = 160;         // warps 0-3: epilogue (TMEM lanes 0-127); warp 4: copies + MMAs
+constexpr int kTcEpiWarps = 8;          // warps 0-7: epilogue (warp w: TMEM lanes 32 (w % 4).., column half w / 4)
+constexpr int kTcThreads = 32 * (kTcEpiWarps + 1);   // + warp 8: bulk copies and MMAs
 constexpr uint32_t kTcCols = 256;       // TMEM columns: two accumulators of up to 128 columns
 constexpr long long kTcSpin = 4000000000LL;   // clock cycles a wait may take before it gives up (~2 s)
 
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(kTcThreads) k_pair_tc(TcArgs a, int tile0) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TcTile tl = a.tiles[tile0 + blockIdx.x];
     const TcGroup gr = a.groups[tl.group];
-    const int K = gr.K, np = gr.np, N = 2 * np, P = 2 * gr.M2 - 2, mt = tl.mtiles;
+    const int K = gr.K, np = gr.np, N = 2 * np, P = 2 * gr.M2 - 2, m0 = tl.m0, mt = tl.m1 - tl.m0;
 
     const uint32_t raw = smem_u32(tc_smem_raw);
     unsigned char* base = tc_smem_raw + (((raw + 127u) & ~127u) - raw);
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(kTcThreads) k_pair_tc(TcArgs a, int tile0) {
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&bar_full[b]), 1);
             mbar_init(smem_u32(&bar_mma[b]), 1);
-            mbar_init(smem_u32(&bar_empty[b]), 4 * 32);
+            mbar_init(smem_u32(&bar_empty[b]), kTcEpiWarps * 32);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_abort = 0;
@@ -255,7 +257,7 @@ __global__ void __launch_bounds__(kTcThreads) k_pair_tc(TcArgs a, int tile0) {
     tc_fence_after();
     const uint32_t tmem = s_tmem;
 
-    if (warp == 4) {
+    if (warp == kTcEpiWarps) {
         if (lane == 0) {
             const uint32_t abytes = (uint32_t)(2 * kTcRows * K * 4);
             const float* ga = a.a + gr.a_off;
@@ -266,10 +268,11 @@ __global__ void __launch_bounds__(kTcThreads) k_pair_tc(TcArgs a, int tile0) {
             const uint32_t step_a = 32 * kTcRows, step_b = 32 * N;  // bytes per K slice of 8
             const uint32_t lo_a = (uint32_t)(kTcRows * K * 4);
             int loaded = 0, consumed = 0, issued = 0;
-            auto load = [&](int m) {
-                const int b = m & 1;
+            // j: the CTA's own tile count (buffers and phases), m0 + j: the tile of the group
+            auto load = [&](int j) {
+                const int b = j & 1;
                 mbar_expect_tx(smem_u32(&bar_full[b]), abytes);
-                bulk_g2s(sa[b], ga + (size_t)m * 2 * kTcRows * K, abytes, smem_u32(&bar_full[b]));
+                bulk_g2s(sa[b], ga + (size_t)(m0 + j) * 2 * kTcRows * K, abytes, smem_u32(&bar_full[b]));
                 ++loaded;
             };
             load(0);
@@ -305,14 +308,15 @@ __global__ void __launch_bounds__(kTcThreads) k_pair_tc(TcArgs a, int tile0) {
         }
         __syncwarp();
     } else {
-        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+        const int quarter = warp & 3, half = warp >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         for (int m = 0; m < mt; ++m) {
             const int b = m & 1;
             const bool ok = mbar_wait(smem_u32(&bar_mma[b]), (m >> 1) & 1, &s_abort);
             if (!__all_sync(0xffffffffu, ok)) break;
             tc_fence_after();
-            const int64_t e = (int64_t)m * kTcRows + warp * 32 + lane;
-            for (int c = 0; c < N; c += 16) {
+            const int64_t e = (int64_t)(m0 + m) * kTcRows + quarter * 32 + lane;
+            for (int c = half * np; c < (half + 1) * np; c += 16) {
                 uint32_t v[16];
                 tmem_ld16(tmem + lane_base + (uint32_t)(b * 128 + c), v);
                 tmem_wait_ld();
