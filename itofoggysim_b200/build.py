@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libfoggy_b200.so")
-SOURCES = ["foggy_api.cu", "k_direct.cu", "k_pair_tc.cu", "k_translation.cu", "k_scene.cu", "k_gmres.cu", "k_tree.cu", "gaunt.cpp", "fmm_tree.cpp", "server.cpp"]
+SOURCES = ["foggy_api.cu", "k_direct.cu", "k_pair_tables.cu", "k_translation.cu", "k_scene.cu", "k_gmres.cu", "k_tree.cu", "gaunt.cpp", "fmm_tree.cpp", "server.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

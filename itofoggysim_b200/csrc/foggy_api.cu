@@ -562,11 +562,13 @@ int plan_direct(foggy_handle h) {
     return FOGGY_OK;
 }
 
-// The single-precision pair tables as tensor-core products (k_pair_tc.cu).  The pairs are grouped
-// by M2 = max(p_s, p_t) + 2 (the groups share the Gaunt operand) and, within a group, ordered by
-// min(p_s, p_t) from the largest down, so that the np pairs of a tile have blocks of similar size;
-// the 128-row tiles of a tile's largest block are split into runs of 8, one CTA each.
-int build_pair_tables_tc(foggy_handle h, const SGaunt& g) {
+// The pair tables over groups of pairs (k_pair_tables.cu).  The pairs are grouped by
+// M2 = max(p_s, p_t) + 2 (a group shares its Gaunt coefficients) and, within a group, ordered by
+// min(p_s, p_t) from the largest down, so that the pairs of a tile have blocks of similar size.
+// FP64 tables (fp64): tiles of kPairs64 pairs, their row tiles in runs of 16, summed on the CUDA
+// cores.  FP32 tables (fp32): tiles of 64 pairs (16 above order 34), runs of 8 row tiles, as
+// tensor-core products.  One CTA per run.
+int build_pair_tables(foggy_handle h, const SGaunt& g, bool fp64, bool fp32) {
     const int n = h->N;
     const int nm = h->pmax + 3;   // M2 = 3..pmax + 2, min order 1..pmax
     std::vector<int64_t> start((size_t)nm * nm + 1, 0);
@@ -581,9 +583,12 @@ int build_pair_tables_tc(foggy_handle h, const SGaunt& g) {
         for (int s = 0; s < n; ++s)
             for (int t = s + 1; t < n; ++t) pairs[(size_t)fill[bucket(h->p_s[s], h->p_s[t])]++] = make_int2(s, t);
     }
+    auto tiles_of = [&](int64_t first) {
+        const int2 st = pairs[(size_t)first];
+        return (int)((pair_block_size(h->p_s[st.x], h->p_s[st.y]) + 127) / 128);
+    };
     std::vector<TcGroup> groups;
-    std::vector<TcTile> tiles;
-    std::vector<int> group_tile0;
+    std::vector<int64_t> gbeg, gend;
     int64_t a_floats = 0;
     for (int M2 = 3; M2 < nm; ++M2) {
         const int64_t g0 = start[(size_t)M2 * nm], g1 = start[(size_t)(M2 + 1) * nm];
@@ -592,64 +597,84 @@ int build_pair_tables_tc(foggy_handle h, const SGaunt& g) {
         gr.M2 = M2;
         gr.K = tc_group_k(M2);
         gr.np = tc_group_pairs(gr.K);
-        auto tiles_of = [&](int64_t first) {
-            const int2 st = pairs[(size_t)first];
-            return (int)((pair_block_size(h->p_s[st.x], h->p_s[st.y]) + 127) / 128);
-        };
         gr.mtiles = tiles_of(g0);
         gr.a_off = a_floats;
-        a_floats += (int64_t)gr.mtiles * 2 * 128 * gr.K;
-        group_tile0.push_back((int)tiles.size());
-        // runs of at most 8 row tiles per CTA, so that groups of few pairs still fill the GPU
-        for (int64_t f = g0; f < g1; f += gr.np) {
-            const int mt = tiles_of(f), cnt = (int)std::min<int64_t>(gr.np, g1 - f);
-            for (int m = 0; m < mt; m += 8)
-                tiles.push_back(TcTile{(int)groups.size(), (int)f, cnt, m, std::min(mt, m + 8)});
-        }
+        if (fp32) a_floats += (int64_t)gr.mtiles * 2 * 128 * gr.K;
         groups.push_back(gr);
+        gbeg.push_back(g0);
+        gend.push_back(g1);
     }
-    group_tile0.push_back((int)tiles.size());
+    // tiles of np pairs per group, their row tiles in runs of `run`; tile0[i] = first tile of group i
+    auto make_tiles = [&](bool tc, int run, std::vector<TcTile>& tiles, std::vector<int>& tile0) {
+        for (size_t i = 0; i < groups.size(); ++i) {
+            tile0.push_back((int)tiles.size());
+            const int np = tc ? groups[i].np : kPairs64;
+            for (int64_t f = gbeg[i]; f < gend[i]; f += np) {
+                const int mt = tiles_of(f), cnt = (int)std::min<int64_t>(np, gend[i] - f);
+                for (int m = 0; m < mt; m += run) tiles.push_back(TcTile{(int)i, (int)f, cnt, m, std::min(mt, m + run)});
+            }
+        }
+        tile0.push_back((int)tiles.size());
+    };
+    std::vector<TcTile> t64, t32;
+    std::vector<int> t64_0, t32_0;
+    if (fp64) make_tiles(false, 16, t64, t64_0);
+    if (fp32) make_tiles(true, 8, t32, t32_0);
     int2* d_pairs = nullptr;
-    TcTile* d_tiles = nullptr;
+    TcTile* d_t64 = nullptr;
+    TcTile* d_t32 = nullptr;
     TcGroup* d_groups = nullptr;
     float* d_a = nullptr;
     int* d_err = nullptr;
     auto fin = [&](int rc) {
         tfree(h, d_pairs);
-        tfree(h, d_tiles);
+        tfree(h, d_t64);
+        tfree(h, d_t32);
         tfree(h, d_groups);
         tfree(h, d_a);
         tfree(h, d_err);
         return rc;
     };
     if (talloc(h, &d_pairs, pairs.size() * sizeof(int2)) != cudaSuccess ||
-        talloc(h, &d_tiles, tiles.size() * sizeof(TcTile)) != cudaSuccess ||
+        talloc(h, &d_t64, std::max<size_t>(t64.size(), 1) * sizeof(TcTile)) != cudaSuccess ||
+        talloc(h, &d_t32, std::max<size_t>(t32.size(), 1) * sizeof(TcTile)) != cudaSuccess ||
         talloc(h, &d_groups, groups.size() * sizeof(TcGroup)) != cudaSuccess ||
-        talloc(h, &d_a, (size_t)a_floats * sizeof(float)) != cudaSuccess || talloc(h, &d_err, sizeof(int)) != cudaSuccess)
-        return fin(fail(h, FOGGY_ERR_NOMEM, "tensor-core pair tables: device scratch"));
+        talloc(h, &d_a, (size_t)std::max<int64_t>(a_floats, 1) * sizeof(float)) != cudaSuccess ||
+        talloc(h, &d_err, sizeof(int)) != cudaSuccess)
+        return fin(fail(h, FOGGY_ERR_NOMEM, "pair tables: device scratch"));
     cudaError_t e = h2d(h, d_pairs, pairs.data(), pairs.size() * sizeof(int2));
-    if (e == cudaSuccess) e = h2d(h, d_tiles, tiles.data(), tiles.size() * sizeof(TcTile));
+    if (e == cudaSuccess && fp64) e = h2d(h, d_t64, t64.data(), t64.size() * sizeof(TcTile));
+    if (e == cudaSuccess && fp32) e = h2d(h, d_t32, t32.data(), t32.size() * sizeof(TcTile));
     if (e == cudaSuccess) e = h2d(h, d_groups, groups.data(), groups.size() * sizeof(TcGroup));
     if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, sizeof(int), h->stream);
-    if (e != cudaSuccess) return fin(fail(h, FOGGY_ERR_CUDA, std::string("tensor-core pair tables: ") + cudaGetErrorString(e)));
-    TcArgs ta{scene_view(h), h->prm.z_coupling, d_pairs, d_tiles, d_groups, d_a, h->d_pair_off, h->d_stab32, d_err};
-    for (size_t i = 0; i < groups.size(); ++i) {
-        launch_tc_pack_a(g, groups[i], d_a, h->stream);
-        launch_pair_tc(ta, group_tile0[i], group_tile0[i + 1] - group_tile0[i], groups[i].K, groups[i].np, h->stream);
-        h->launches += 2;
+    if (e != cudaSuccess) return fin(fail(h, FOGGY_ERR_CUDA, std::string("pair tables: ") + cudaGetErrorString(e)));
+    if (fp64) {
+        PairArgs pa{scene_view(h), h->prm.z_coupling, d_pairs, d_t64, d_groups, g, h->d_pair_off, h->d_stab};
+        for (size_t i = 0; i < groups.size(); ++i) {
+            launch_pair_s_group(pa, t64_0[i], t64_0[i + 1] - t64_0[i], groups[i].M2, h->stream);
+            h->launches += 1;
+        }
+    }
+    if (fp32) {
+        TcArgs ta{scene_view(h), h->prm.z_coupling, d_pairs, d_t32, d_groups, d_a, h->d_pair_off, h->d_stab32, d_err};
+        for (size_t i = 0; i < groups.size(); ++i) {
+            launch_tc_pack_a(g, groups[i], d_a, h->stream);
+            launch_pair_tc(ta, t32_0[i], t32_0[i + 1] - t32_0[i], groups[i].K, groups[i].np, h->stream);
+            h->launches += 2;
+        }
     }
     e = cudaGetLastError();
     int err = 0;
     if (e == cudaSuccess) e = d2h(h, &err, d_err, sizeof(int));
-    if (e != cudaSuccess) return fin(fail(h, FOGGY_ERR_CUDA, std::string("tensor-core pair tables: ") + cudaGetErrorString(e)));
+    if (e != cudaSuccess) return fin(fail(h, FOGGY_ERR_CUDA, std::string("pair tables: ") + cudaGetErrorString(e)));
     if (err) return fin(fail(h, FOGGY_ERR_CUDA, "tensor-core pair tables: a wait for a copy or the tensor core timed out"));
     return fin(FOGGY_OK);
 }
 
 // Scalar coaxial coefficients of all unordered sphere pairs (geometry and z only), built once
 // and read by every operator application.  Skipped when they do not fit (pair_tables = 0) or
-// when switched off (pair_tables = -1).  The double-precision tables are FP64 sums (k_pair_s); the
-// single-precision ones are tensor-core products in 3xTF32 (build_pair_tables_tc).
+// when switched off (pair_tables = -1).  The double-precision tables are FP64 sums on the CUDA
+// cores, the single-precision ones tensor-core products in 3xTF32 (build_pair_tables).
 int ensure_pair_tables(foggy_handle h) {
     const bool mixed = h->prm.precision == 1;
     if (h->prm.pair_tables < 0 || h->N < 2) {
@@ -710,19 +735,11 @@ int ensure_pair_tables(foggy_handle h) {
     }
     Trace tr("pair tables");
     SGaunt g{h->d_koffS, h->d_gs, h->gs_nm};
-    int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, (148 * 8 + h->N - 1) / h->N));
-    dim3 grid(h->N, chunks);
-    if (want64) {
-        if (!h->d_stab) TRY(dalloc(h, &h->d_stab, (size_t)tot));
-        launch_pair_s(scene_view(h), g, h->prm.z_coupling, h->d_pair_off, h->d_stab, false, grid, chunks, h->stream);
-        h->launches += 1;
-        h->stab_ready = true;
-    }
-    if (want32) {
-        if (!h->d_stab32) TRY(dalloc(h, &h->d_stab32, (size_t)tot));
-        TRY(build_pair_tables_tc(h, g));
-        h->stab32_ready = true;
-    }
+    if (want64 && !h->d_stab) TRY(dalloc(h, &h->d_stab, (size_t)tot));
+    if (want32 && !h->d_stab32) TRY(dalloc(h, &h->d_stab32, (size_t)tot));
+    TRY(build_pair_tables(h, g, want64, want32));
+    if (want64) h->stab_ready = true;
+    if (want32) h->stab32_ready = true;
     CKL(h);
     h->stab_z = h->prm.z_coupling;
     return FOGGY_OK;

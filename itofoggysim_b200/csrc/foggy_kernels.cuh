@@ -130,12 +130,10 @@ size_t block_smem_bytes(int pp, bool tabs, bool fp32, int R);
 bool launch_direct_block(const BlockArgs& a, const DirectBucket& b, int R, cudaStream_t s);
 size_t translation_pair_smem_bytes(int pmax);
 void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s);
-// scalar coaxial tables of every pair, in FP64 (stab: cplx*) or FP32 (cplxf*)
-void launch_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, void* stab, bool fp32, dim3 grid,
-                   int chunks, cudaStream_t s);
 
-// k_pair_tc.cu -- the FP32 tables as tensor-core products (tcgen05 kind::tf32, 3xTF32).  The pairs
-// of one M2 = max order + 2 share the Gaunt operand; a tile is up to np pairs of one group.
+// k_pair_tables.cu -- the pair tables over groups of pairs with one M2 = max order + 2: FP32 as
+// tensor-core products (tcgen05 kind::tf32, 3xTF32; the group's pairs share the Gaunt operand, a
+// tile is up to np pairs), FP64 summed on the CUDA cores (tiles of up to kPairs64 pairs).
 struct TcGroup {
     int M2, K, np;        // K: degrees p = 0..2 M2 - 2 padded to 8; np: pairs per tile (64, or 16 for K > 72)
     int mtiles;           // 128-row tiles of the packed Gaunt operand (the group's largest block)
@@ -162,6 +160,19 @@ int tc_group_pairs(int K);
 size_t tc_smem_bytes(int K, int np);
 void launch_tc_pack_a(SGaunt g, const TcGroup& gr, float* out, cudaStream_t s);
 void launch_pair_tc(const TcArgs& a, int tile0, int ntiles, int K, int np, cudaStream_t s);
+constexpr int kPairs64 = 32;   // pairs per tile of the FP64 tables
+struct PairArgs {
+    SceneView sc;
+    int z;
+    const int2* pairs;
+    const TcTile* tiles;       // tiles of up to kPairs64 pairs, runs of up to 16 row tiles
+    const TcGroup* groups;
+    SGaunt g;
+    const int64_t* pair_off;
+    cplx* stab;
+};
+size_t pair_s_group_smem_bytes(int M2);
+void launch_pair_s_group(const PairArgs& a, int tile0, int ntiles, int M2, cudaStream_t s);
 // y = x + T (sum of the slab partials) for coupled spheres, y = x otherwise
 __global__ void k_direct_finish(SceneView sc, const cplx* x, const cplx* partial, int slabs, int64_t n_unk,
                                 cplx* y);

@@ -699,62 +699,6 @@ __global__ void k_pair_sizes(SceneView sc, int64_t* sizes) {
         sizes[pair_index(s, t, sc.n)] = pair_block_size(ps, sc.p[t]);
 }
 
-// One CTA per (sphere s, chunk c) walks t = s + 1 + c, s + 1 + c + chunks, ...:
-//   S(k; a, b) = sum_q (2p+1)(a b p; -k k 0)(a b p; 0 0 0) i^p z_p(k |d_t - d_s|),  p = a + b - 2q
-// for k = 0..min(p_s, p_t) on the square a, b = k..M+1, M = max(p_s, p_t) (S is symmetric in a, b;
-// the square lets either sphere of the pair read it with its own degree as the fast index).
-template <class C>
-__global__ void __launch_bounds__(256) k_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, C* stab,
-                                                int chunks) {
-    __shared__ double jb[2 * kMaxDegree + 8], yb[2 * kMaxDegree + 8];
-    __shared__ cplx zeta[2 * kMaxDegree + 8];
-    __shared__ double rho_s;
-    const int s = blockIdx.x;
-    const int ps = sc.p[s];
-    const double* cs = sc.centres + 3 * (size_t)s;
-    for (int t = s + 1 + blockIdx.y; t < sc.n; t += chunks) {
-        const int pt = sc.p[t];
-        const int M2 = max(ps, pt) + 2;
-        const int P = 2 * M2 - 2;
-        if (threadIdx.x == 0) {
-            const double* ct = sc.centres + 3 * (size_t)t;
-            double d0 = sc.k * (ct[0] - cs[0]);
-            double d1 = sc.k * (ct[1] - cs[1]);
-            double d2 = sc.k * (ct[2] - cs[2]);
-            rho_s = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) dev_sph_jn(rho_s, P, jb);
-        if (threadIdx.x == 32 && z != 1) dev_sph_yn(rho_s, P, yb);
-        __syncthreads();
-        for (int p = threadIdx.x; p <= P; p += blockDim.x) zeta[p] = zeta_of(z, p, jb, yb);
-        __syncthreads();
-        C* out = stab + pair_off[pair_index(s, t, sc.n)];
-        const int km = min(ps, pt);
-        const int64_t tot = pair_block_size(ps, pt);
-        for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
-            int k = 0;
-            while (k < km && pair_block_offset(k + 1, M2, M2) <= e) ++k;
-            int64_t r = e - pair_block_offset(k, M2, M2);
-            int cols = M2 - k;
-            int aa = k + (int)(r / cols), bb = k + (int)(r % cols);
-            const int W = g.NM - k + 1;
-            const size_t plane = (size_t)W * W;
-            const double* gp = g.gs + g.koff[k] + (size_t)(aa - k) * W + (bb - k);
-            int qm = min(aa, bb);
-            int p = aa + bb;
-            double sx = 0.0, sy = 0.0;
-            for (int q = 0; q <= qm; ++q, p -= 2) {
-                double c = __ldg(gp + q * plane);
-                sx += c * zeta[p].x;
-                sy += c * zeta[p].y;
-            }
-            out[e] = cm<C>(sx, sy);
-        }
-        __syncthreads();
-    }
-}
-
 // ---------------------------------------------------------------------------------------------
 // the pair tables and the d(pi/2) table of an operator precision
 __device__ __forceinline__ const cplx* stab_of(const DirectArgs& a, cplx*) { return a.pt.stab; }
@@ -858,13 +802,6 @@ void launch_direct(const DirectArgs& a, const DirectBucket& b, cudaStream_t s) {
     }
 }
 
-void launch_pair_s(SceneView sc, SGaunt g, int z, const int64_t* pair_off, void* stab, bool fp32, dim3 grid,
-                   int chunks, cudaStream_t s) {
-    if (fp32)
-        k_pair_s<cplxf><<<grid, 256, 0, s>>>(sc, g, z, pair_off, static_cast<cplxf*>(stab), chunks);
-    else
-        k_pair_s<cplx><<<grid, 256, 0, s>>>(sc, g, z, pair_off, static_cast<cplx*>(stab), chunks);
-}
 
 // ---------------------------------------------------------------------------------------------
 // ML-FMM passes: CTAs (target, chunk) over the target's CSR source list, chunk c taking the sources

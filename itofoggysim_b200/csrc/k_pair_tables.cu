@@ -1,6 +1,7 @@
-// Single-precision pair tables of the mixed-precision operator as tensor-core products:
-// tcgen05.mma kind::tf32 with every operand split into a TF32 high and low part (3xTF32:
-// hi*hi + hi*lo + lo*hi, FP32 accumulation in tensor memory).
+// Pair tables of every sphere pair, kept in HBM for the operator: the single-precision ones (the
+// mixed-precision operator) as tensor-core products, tcgen05.mma kind::tf32 with every operand split
+// into a TF32 high and low part (3xTF32: hi*hi + hi*lo + lo*hi, FP32 accumulation in tensor memory);
+// the double-precision ones summed in FP64 on the CUDA cores over the same groups of pairs.
 //
 // Row e of the block of an unordered sphere pair (s, t) is the scalar coaxial coefficient
 // S(k; a, b) that k_pair_s sums (k = 0..min(p_s, p_t), a, b = k..M+1, M = max(p_s, p_t)):
@@ -338,6 +339,91 @@ __global__ void __launch_bounds__(kTcThreads) k_pair_tc(TcArgs a, int tile0) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols));
     }
     if (tid == 0 && s_abort) atomicExch(a.err, 1);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Double-precision tables on the CUDA cores, over the same groups (one M2 = max order + 2): one CTA
+// per run of up to 16 row tiles of up to 32 pairs.  The pairs' zeta_p sit in shared memory; each
+// thread takes one row e = (k, a, b), keeps its Gaunt coefficients in registers and sums
+// S = sum_q G_q zeta_{a+b-2q} for every second pair of the tile.  The sum runs over q ascending with
+// one FMA per term, as the per-pair sum it replaces did, so the tables are bit-identical to it.
+template <int QMAX>
+__global__ void __launch_bounds__(256) k_pair_s_group(PairArgs a, int tile0) {
+    extern __shared__ __align__(16) unsigned char ps_smem[];
+    __shared__ int64_t s_off[kPairs64], s_tot[kPairs64];
+    const int tid = threadIdx.x;
+    const TcTile tl = a.tiles[tile0 + blockIdx.x];
+    const int M2 = a.groups[tl.group].M2, P = 2 * M2 - 2, km = M2 - 2;
+    cplx* zeta = reinterpret_cast<cplx*>(ps_smem);                              // [kPairs64][P + 1]
+    double* scr = reinterpret_cast<double*>(zeta + (size_t)kPairs64 * (P + 1));  // [kPairs64][2 (P + 1)]
+    for (int i = tid; i < tl.count; i += 256) {
+        const int2 st = a.pairs[tl.first + i];
+        const double* cs = a.sc.centres + 3 * (size_t)st.x;
+        const double* ct = a.sc.centres + 3 * (size_t)st.y;
+        double d0 = a.sc.k * (ct[0] - cs[0]);
+        double d1 = a.sc.k * (ct[1] - cs[1]);
+        double d2 = a.sc.k * (ct[2] - cs[2]);
+        const double rho = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        double* jb = scr + (size_t)2 * (P + 1) * i;
+        dev_sph_jn(rho, P, jb);
+        if (a.z != 1) dev_sph_yn(rho, P, jb + P + 1);
+        s_off[i] = a.pair_off[pair_index(st.x, st.y, a.sc.n)];
+        s_tot[i] = pair_block_size(a.sc.p[st.x], a.sc.p[st.y]);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < tl.count * (P + 1); idx += 256) {
+        const int i = idx / (P + 1), p = idx - i * (P + 1);
+        const double* jb = scr + (size_t)2 * (P + 1) * i;
+        zeta[idx] = zeta_of(a.z, p, jb, jb + P + 1);
+    }
+    __syncthreads();
+    const int r = tid & 127, half = tid >> 7;
+    for (int m = tl.m0; m < tl.m1; ++m) {
+        const int64_t e = (int64_t)m * 128 + r;
+        if (e >= s_tot[0]) break;   // the tile's first pair has its largest block
+        int k = 0;
+        while (k < km && pair_block_offset(k + 1, M2, M2) <= e) ++k;
+        const int64_t rr = e - pair_block_offset(k, M2, M2);
+        const int cols = M2 - k;
+        const int aa = k + (int)(rr / cols), bb = k + (int)(rr % cols);
+        const int W = a.g.NM - k + 1;
+        const size_t plane = (size_t)W * W;
+        const double* gp = a.g.gs + a.g.koff[k] + (size_t)(aa - k) * W + (bb - k);
+        const int qm = min(aa, bb), p0 = aa + bb;
+        double c[QMAX];
+#pragma unroll
+        for (int q = 0; q < QMAX; ++q) c[q] = q <= qm ? __ldg(gp + q * plane) : 0.0;
+        for (int i = half; i < tl.count; i += 2) {
+            if (e >= s_tot[i]) break;   // blocks shrink along the tile
+            const cplx* zi = zeta + (size_t)(P + 1) * i + p0;
+            double sx = 0.0, sy = 0.0;
+#pragma unroll
+            for (int q = 0; q < QMAX; ++q) {
+                if (q <= qm) {
+                    const cplx zz = zi[-2 * q];
+                    sx += c[q] * zz.x;
+                    sy += c[q] * zz.y;
+                }
+            }
+            a.stab[s_off[i] + e] = cplx{sx, sy};
+        }
+    }
+}
+
+size_t pair_s_group_smem_bytes(int M2) { return (size_t)kPairs64 * (2 * M2 - 1) * 32; }
+
+void launch_pair_s_group(const PairArgs& a, int tile0, int ntiles, int M2, cudaStream_t s) {
+    const size_t smem = pair_s_group_smem_bytes(M2);
+    if (M2 <= 16) {
+        raise_smem_ceiling(reinterpret_cast<const void*>(k_pair_s_group<16>), smem);
+        k_pair_s_group<16><<<ntiles, 256, smem, s>>>(a, tile0);
+    } else if (M2 <= 32) {
+        raise_smem_ceiling(reinterpret_cast<const void*>(k_pair_s_group<32>), smem);
+        k_pair_s_group<32><<<ntiles, 256, smem, s>>>(a, tile0);
+    } else {
+        raise_smem_ceiling(reinterpret_cast<const void*>(k_pair_s_group<48>), smem);
+        k_pair_s_group<48><<<ntiles, 256, smem, s>>>(a, tile0);
+    }
 }
 
 void launch_pair_tc(const TcArgs& a, int tile0, int ntiles, int K, int np, cudaStream_t s) {
