@@ -3,7 +3,7 @@
 A handle in mixed precision (precision = 1) keeps its FP32 pair tables, the scalar coaxial
 coefficients S(k; a, b) of every sphere pair, as the product of the Gaunt coefficients and the
 pairs' i^p z_p(kd) on the tensor cores, each operand split into a TF32 high and low part
-(k_pair_tc.cu).  The FP32 operator that reads those tables must agree with
+(k_pair_tables.cu).  The FP32 operator that reads those tables must agree with
 
   * the FP64 operator of the same handle (FP64 tables summed in FP64, pinned to the oracle at 1e-12
     by test_gpu_parity.py and test_gpu_high_order.py): 1e-5, the tolerance of every FP32 operator
