@@ -29,9 +29,21 @@
 
 extern "C" {
 void wig_table_init(int max_two_j, int wigner_type);
-void wig_temp_init(int max_two_j);
 void wig_thread_temp_init(int max_two_j);
+void wig_temp_free(void);
 double wig3jj(int two_j1, int two_j2, int two_j3, int two_m1, int two_m2, int two_m3);
+}
+
+// wigxjpf keeps one scratch array per thread (wig_thread_temp_init allocates a new one each call).
+// Grow the calling thread's array when it is smaller than asked, never shrink it: the main thread
+// also runs in the OpenMP regions below, and a smaller array left there would make a later 3j call
+// of higher degree on that thread fail.
+static void ensure_wig_temp(int max_two_j) {
+    static thread_local int have = -1;
+    if (have >= max_two_j) return;
+    if (have >= 0) wig_temp_free();
+    wig_thread_temp_init(max_two_j);
+    have = max_two_j;
 }
 
 typedef std::complex<double> cd;
@@ -298,7 +310,7 @@ void translation_xu(double x, double theta, double phi, int n1, int n2, int nu1,
     int cnt_nu = (nu2 + 1) * (nu2 + 1) - nu1 * nu1;
 #pragma omp parallel
     {
-        wig_thread_temp_init(2 * (2 * pmax + 2));
+        ensure_wig_temp(2 * (2 * pmax + 2));
 #pragma omp for schedule(dynamic)
         for (int n = n1; n <= n2; ++n) {
             for (int m = -n; m <= n; ++m) {
@@ -777,7 +789,7 @@ void matvec_direct(Problem& P, const cd* x, cd* y, int j0 = 0, int j1 = -1, bool
     for (int w = 0; w < (int)work.size(); ++w) {
         int j = work[w].first;
         std::vector<cd> lA, lB;
-        wig_thread_temp_init(2 * (4 * P.n2 + 8));
+        ensure_wig_temp(2 * (4 * P.n2 + 8));
         int ip = P.pidx[j];
         int a0 = P.nr[2 * ip];
         cd* yj = y + (size_t)2 * C * j;
@@ -937,7 +949,7 @@ extern "C" {
 void orc_init(int max_n) {
     int two_j = 2 * (4 * max_n + 8);
     wig_table_init(two_j, 3);
-    wig_temp_init(two_j);
+    ensure_wig_temp(two_j);
 }
 
 int orc_sph_jn(double x, int nmax, double* out) { sph_jn(x, nmax, out); return 0; }
@@ -1282,7 +1294,7 @@ struct Fmm {
         if (it == cache.end()) {
             int cr = (r2 + 1) * (r2 + 1) - r1 * r1, cc = (c2 + 1) * (c2 + 1) - c1 * c1;
             std::vector<cd> A((size_t)cr * cc), B((size_t)cr * cc);
-            wig_thread_temp_init(2 * (4 * std::max(std::max(r2, c2), P.n2) + 8));
+            ensure_wig_temp(2 * (4 * std::max(std::max(r2, c2), P.n2) + 8));
             translation_xu(rho, th, ph, r1, r2, c1, c2, z, A.data(), B.data());
             it = cache.emplace(key, std::make_pair(std::move(A), std::move(B))).first;
         }
@@ -1525,7 +1537,7 @@ int orc_pairs_apply(void* p, const double* xin, int npairs, const int* pj, const
     int C = P->cnt();
 #pragma omp parallel for schedule(dynamic)
     for (int w = 0; w < npairs; ++w) {
-        wig_thread_temp_init(2 * (4 * P->n2 + 8));
+        ensure_wig_temp(2 * (4 * P->n2 + 8));
         int j = pj[w], l = pl[w];
         if (j == l) continue;
         int ja, jb, la, lb;
